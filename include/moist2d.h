@@ -1,0 +1,213 @@
+/*
+ * moist2d.h - C-ABI of libmoist2d_sm100a.so, the B200 (sm_100a) implementation of
+ * moist2d's large time step.
+ *
+ * The entry points replace the Julia methods of moist.jl (seiya/moist2d):
+ *   rk3_step!(s::State, p::Params{T})               moist.jl:1589-1683  -> moist_rk3_step
+ *   compute_step!(d_phys x6, s, s0, p, dt, ns)       moist.jl:1039-1580  -> moist_compute_step
+ *   cloud_microphysics!(...)                         moist.jl:554-671    -> moist_cloud_microphysics
+ *   rain_sedimentation!(...)                         moist.jl:674-707    -> moist_rain_sedimentation
+ *   implicit_correction!(rho_w, drho_w, theta, rt2pres, dt, p)
+ *                                                    moist.jl:974-1030   -> moist_implicit_correction
+ *   device(x)  (the CuArray hook)                    moist.jl:227-228    -> moist_ctx_create + moist_upload_state
+ * A Julia caller binds them with ccall; Python binds them with ctypes
+ * (moist2d_b200/_lib.py).
+ *
+ * Conventions
+ *  - Every call returns an int status (MOIST_OK = 0). Errors the reference raises as Julia
+ *    exceptions (error("NaN detected in rho"), moist.jl:1543-1577) become MOIST_ERR_NAN, with
+ *    the field index from moist_nan_field() and the text from moist_last_error().
+ *  - Precision is chosen per context (MOIST_F32 / MOIST_F64), the counterpart of Params{T}
+ *    and the global FT (moist.jl:22-24). Every host array passed to a context holds elements
+ *    of that type.
+ *  - Host state arrays use the reference layout: 2-D fields are Julia column-major (ka, ia)
+ *    arrays, z (k) fastest, ka = nz, ia = nx + 2*halo, with `halo` periodic columns on each
+ *    side (moist.jl:82-88, 319-345). 1-D x fields have length ia, theta_ref has length ka.
+ *  - Device buffers belong to the context. One context = one CUDA stream. Calls on one
+ *    context are not thread-safe; different contexts may be driven from different threads.
+ *    Calls return after the work they queued has finished, unless stated otherwise.
+ */
+#ifndef MOIST2D_H
+#define MOIST2D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MOIST2D_ABI_VERSION 1
+
+/* precision of a context (Params{Float32} / Params{Float64}) */
+enum { MOIST_F32 = 0, MOIST_F64 = 1 };
+
+/* status codes */
+enum {
+    MOIST_OK = 0,
+    MOIST_ERR_NAN = 1,          /* a NaN was found by the end-of-stage check (moist.jl:1542-1578) */
+    MOIST_ERR_ARG = 2,          /* invalid argument (null pointer, nz < 2, nx < 2, ns < 1, ...) */
+    MOIST_ERR_CUDA = 3,         /* a CUDA runtime call failed; text in moist_last_error */
+    MOIST_ERR_TIMEOUT = 4,      /* a bounded device-side wait ran out */
+    MOIST_ERR_UNSUPPORTED = 5,  /* valid in the reference but not provided by this library */
+    MOIST_ERR_NOMEM = 6         /* device allocation failed */
+};
+
+/* field indices reported by moist_nan_field(), in the order compute_step! checks them */
+enum {
+    MOIST_FIELD_RHO = 0,
+    MOIST_FIELD_RHO_U = 1,
+    MOIST_FIELD_RHO_W = 2,
+    MOIST_FIELD_RHO_THETA = 3,
+    MOIST_FIELD_RHO_QV = 4,
+    MOIST_FIELD_RHO_QC = 5,
+    MOIST_FIELD_RHO_QR = 6,
+    MOIST_FIELD_D_RHO_U_PHYS = 7,
+    MOIST_FIELD_D_RHO_THETA_PHYS = 8,
+    MOIST_FIELD_D_RHO_QV_PHYS = 9,
+    MOIST_FIELD_D_RHO_QC_PHYS = 10,
+    MOIST_FIELD_D_RHO_QR_PHYS = 11
+};
+
+/* context creation flags */
+enum {
+    /* In a MOIST_F32 context the w-p tridiagonal elimination runs in FP64 by default; this flag
+     * selects the reference's literal Float32 elimination (moist.jl:952-971) instead. */
+    MOIST_FLAG_TRI_NATIVE = 1
+};
+
+/*
+ * Params{T} (moist.jl:70-222) plus the global physical constants of set_constants!
+ * (moist.jl:26-60). Scalars are passed as double and converted to the context precision
+ * (exact for values that are already of type T, which is how the Julia and Python mirrors
+ * fill them). The grid vectors are arrays of the context type T, length nz, as produced by
+ * the Params constructor (moist.jl:198-216); they are copied at context creation.
+ */
+typedef struct moist_params {
+    /* grid */
+    int32_t nx, nz, halo;      /* Nx, Nz, halo; ia = nx + 2*halo, ka = nz */
+    int32_t ns;                /* acoustic substeps of the last RK stage (Params.ns) */
+    double lx, h, dx;          /* Lx, H, dx */
+    const void* zf;            /* face heights zf[k]   (T, nz) */
+    const void* dz;            /* layer depths dz[k]   (T, nz) */
+    const void* z;             /* centre heights z[k]  (T, nz) */
+    double dt;                 /* large time step */
+    /* dynamics */
+    double nu, kappa, gamma_d, beta_offcenter, zf_sponge;
+    /* process switches (moist.jl:107-120) */
+    int32_t do_mp, do_auto, do_accr, do_revap, do_sed, do_rd, do_sf;
+    /* surface-flux and radiation coefficients (moist.jl:121-135) */
+    double cd, ch, ce, uabs_min, temp_surf;
+    double k_abs_qv, k_abs_qc, k_abs_qr, surf_emissivity, tau_cooling, z_tropopause;
+    /* physical constants (moist.jl:30-59) */
+    double grav, rd, rv, cpd, cpv, cpl, cvd, p0, lv, sigma, epsvap;
+    double k_auto, qc_threshold, k_accr, k_evap, a_term, b_term;
+    double t0, es0, a_sat, b_sat, eps;
+} moist_params;
+
+/*
+ * Host view of State (moist.jl:294-317). Every pointer may be NULL, which means "skip this
+ * field" on upload and download. Element type = context precision.
+ */
+typedef struct moist_state_host {
+    void* rho;            /* (ka, ia) */
+    void* rho_u;          /* (ka, ia)  at (k, i+1/2) */
+    void* rho_w;          /* (ka, ia)  at (k+1/2, i); rho_w[ke] is the rigid lid */
+    void* rho_theta;      /* (ka, ia) */
+    void* rho_qv;         /* (ka, ia) */
+    void* rho_qc;         /* (ka, ia) */
+    void* rho_qr;         /* (ka, ia) */
+    void* prec;           /* (ia) accumulated precipitation */
+    void* mflux;          /* (ia) */
+    void* shflux;         /* (ia) */
+    void* lhflux;         /* (ia) */
+    void* theta_ref;      /* (ka) */
+    void* d_rho_theta_mp; /* (ka, ia) */
+    void* d_rho_qv_mp;    /* (ka, ia) */
+    void* d_rho_qc_mp;    /* (ka, ia) */
+    void* d_rho_qr_mp;    /* (ka, ia) */
+    void* d_rho_qr_sed;   /* (ka, ia) */
+    void* d_rho_u_sf;     /* (ia) */
+    void* d_rho_theta_sf; /* (ia) */
+    void* d_rho_qv_sf;    /* (ia) */
+    void* d_rho_theta_rd; /* (ka, ia) */
+} moist_state_host;
+
+typedef struct moist_ctx moist_ctx;
+
+/* library identification */
+int moist_abi_version(void);
+const char* moist_status_string(int status);
+
+/* Context = one device-resident State plus Params (replaces device(), moist.jl:227-228).
+ * Fails with MOIST_ERR_ARG for nx < 2, nz < 2, halo != 2, ns < 1 or a NULL grid vector. */
+int moist_ctx_create(const moist_params* p, int precision, int flags, moist_ctx** out);
+int moist_ctx_destroy(moist_ctx* ctx);
+const char* moist_last_error(const moist_ctx* ctx);
+int moist_nan_field(const moist_ctx* ctx);
+
+/* Copy a host State into the context (reference layout, halos included in the host arrays).
+ * The library keeps interior columns; halo columns are re-derived periodically, as every
+ * reference code path on the large step does before reading them. */
+int moist_upload_state(moist_ctx* ctx, const moist_state_host* s);
+/* Copy the context State to host arrays; halo columns are written as periodic copies. */
+int moist_download_state(moist_ctx* ctx, moist_state_host* s);
+
+/* rk3_step!(s, p) applied nsteps times (moist.jl:1589-1683). */
+int moist_rk3_step(moist_ctx* ctx, int nsteps);
+
+/* compute_step!(d_rho_phys, d_rho_u_phys, d_rho_theta_phys, d_rho_qv_phys, d_rho_qc_phys,
+ * d_rho_qr_phys, s, s0, p, dt, ns) (moist.jl:1039-1580): one RK stage on the context state s,
+ * with s0 given as a host State (its rho, rho_u, rho_w, rho_theta, rho_qv, rho_qc, rho_qr are
+ * read) and the six tendency fields given as host (ka, ia) arrays in that order. */
+int moist_compute_step(moist_ctx* ctx, const void* const phys[6], const moist_state_host* s0,
+                       double dt, int ns);
+
+/* cloud_microphysics!(...) (moist.jl:554-671) on the context state: fills d_rho_{theta,qv,qc,qr}_mp
+ * (download them with moist_download_state). */
+int moist_cloud_microphysics(moist_ctx* ctx);
+
+/* rain_sedimentation!(d_rho_qr_sed, d_prec, rho_qr, rho, p) (moist.jl:674-707): fills
+ * d_rho_qr_sed in the context and, if d_prec is not NULL, the host array d_prec (ia, type T). */
+int moist_rain_sedimentation(moist_ctx* ctx, void* d_prec);
+
+/* implicit_correction!(rho_w, drho_w, theta, rt2pres, dt, p) (moist.jl:974-1030) for one
+ * column on the device: host arrays of length nz and type T; rho_w is updated in place.
+ * Only p->nz, p->dz, p->z, p->grav and p->beta_offcenter are read. */
+int moist_implicit_correction(const moist_params* p, int precision, int flags, void* rho_w,
+                              const void* drho_w, const void* theta, const void* rt2pres,
+                              double dt);
+
+/* Device evaluation of the scalar helpers, for the restated unit tests (runtests.jl:25-80,
+ * 377-401): out[j] = helper(in[j*nin ...]) for j < n, computed by the same device functions
+ * the kernels use. Values are passed as double and rounded to the precision first. */
+enum {
+    MOIST_HELPER_F2H = 0,          /* in: vf1, vf2, dz1, dz2          out: 1 (moist.jl:243-251) */
+    MOIST_HELPER_KOREN = 1,        /* in: r                           out: 1 (moist.jl:844-847) */
+    MOIST_HELPER_SAT_VP = 2,       /* in: T                           out: es, des/dT (253-260) */
+    MOIST_HELPER_SAT_Q = 3,        /* in: p, es                       out: qsat, dqsat/des (263-273) */
+    MOIST_HELPER_EXP = 4,          /* in: x                           out: exp(x) */
+    MOIST_HELPER_POW = 5           /* in: x, y                        out: x^y */
+};
+int moist_eval_helper(const moist_params* p, int precision, int helper, int n, const double* in,
+                      double* out);
+
+/* Domain budgets (compensated FP64 sums on the device, deterministic order):
+ * out[0] = mass  sum(rho*dz*dx), out[1] = water sum((rho_qv+rho_qc+rho_qr)*dz*dx) + sum(prec*dx),
+ * out[2] = total energy (kinetic + potential + internal, the terms of moist.jl:1839-1852)*dx*dz,
+ * out[3] = accumulated surface rain sum(prec*dx). */
+int moist_budget(moist_ctx* ctx, double out[4]);
+
+/* Stream of the context (a cudaStream_t), for callers that order their own work after it. */
+void* moist_stream(moist_ctx* ctx);
+/* Block until the context stream is idle. */
+int moist_synchronize(moist_ctx* ctx);
+/* Run nsteps large steps, timed with CUDA events recorded on the context stream around them;
+ * *ms receives the elapsed device time. */
+int moist_time_steps(moist_ctx* ctx, int nsteps, float* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOIST2D_H */
