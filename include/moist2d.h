@@ -140,7 +140,9 @@ int moist_abi_version(void);
 const char* moist_status_string(int status);
 
 /* Context = one device-resident State plus Params (replaces device(), moist.jl:227-228).
- * Fails with MOIST_ERR_ARG for nx < 2, nz < 2, halo != 2, ns < 1 or a NULL grid vector. */
+ * Fails with MOIST_ERR_ARG for nx < 1, nz < 2 (or > 1024), halo < 0, ns < 1 or a NULL grid
+ * vector. The RK-stage entry points (rk3_step, compute_step, time_steps) further need
+ * halo = 2 and nx >= 2, the shapes on which the reference's stencils stay inside the array. */
 int moist_ctx_create(const moist_params* p, int precision, int flags, moist_ctx** out);
 int moist_ctx_destroy(moist_ctx* ctx);
 const char* moist_last_error(const moist_ctx* ctx);

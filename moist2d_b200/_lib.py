@@ -1,0 +1,50 @@
+"""ctypes binding of libmoist2d_sm100a.so (the CUDA library). There is no CPU fallback: if the
+library or a CUDA device is missing, calls raise."""
+import ctypes as C
+import os
+
+from .abi import moist_params, moist_state_host
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+SO_PATH = os.path.join(_HERE, "libmoist2d_sm100a.so")
+_lib = None
+
+EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "moist_ctx_destroy",
+           "moist_last_error", "moist_nan_field", "moist_upload_state", "moist_download_state",
+           "moist_rk3_step", "moist_compute_step", "moist_cloud_microphysics",
+           "moist_rain_sedimentation", "moist_implicit_correction", "moist_eval_helper",
+           "moist_budget", "moist_stream", "moist_synchronize", "moist_time_steps")
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(SO_PATH):
+            raise RuntimeError("libmoist2d_sm100a.so is not built (run __graft_entry__.build() or "
+                               "make -C moist2d_b200/csrc); there is no CPU fallback")
+        L = C.CDLL(SO_PATH)
+        P, S, V, I, D = C.POINTER(moist_params), C.POINTER(moist_state_host), C.c_void_p, C.c_int, C.c_double
+        Ctx = C.c_void_p
+        L.moist_abi_version.restype = I
+        L.moist_status_string.argtypes = [I]
+        L.moist_status_string.restype = C.c_char_p
+        L.moist_ctx_create.argtypes = [P, I, I, C.POINTER(Ctx)]
+        L.moist_ctx_destroy.argtypes = [Ctx]
+        L.moist_last_error.argtypes = [Ctx]
+        L.moist_last_error.restype = C.c_char_p
+        L.moist_nan_field.argtypes = [Ctx]
+        L.moist_upload_state.argtypes = [Ctx, S]
+        L.moist_download_state.argtypes = [Ctx, S]
+        L.moist_rk3_step.argtypes = [Ctx, I]
+        L.moist_compute_step.argtypes = [Ctx, C.POINTER(V), S, D, I]
+        L.moist_cloud_microphysics.argtypes = [Ctx]
+        L.moist_rain_sedimentation.argtypes = [Ctx, V]
+        L.moist_implicit_correction.argtypes = [P, I, I, V, V, V, V, D]
+        L.moist_eval_helper.argtypes = [P, I, I, I, C.POINTER(D), C.POINTER(D)]
+        L.moist_budget.argtypes = [Ctx, C.POINTER(D)]
+        L.moist_stream.argtypes = [Ctx]
+        L.moist_stream.restype = V
+        L.moist_synchronize.argtypes = [Ctx]
+        L.moist_time_steps.argtypes = [Ctx, I, C.POINTER(C.c_float)]
+        _lib = L
+    return _lib

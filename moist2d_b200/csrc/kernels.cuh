@@ -1,0 +1,776 @@
+// kernels.cuh - CUDA kernels of the large step (sm_100a).
+//
+// One large step (rk3_step!, moist.jl:1589-1683) is
+//   [sf] [rd] physics  ->  3 x ( diag, tend, thomas_factors, ns_s x substep, tracer, update )  ->  prec
+// sf/rd run only when do_sf/do_rd are set. See model.cuh for the layout and arithmetic rules.
+#pragma once
+
+#include <climits>
+
+#include "model.cuh"
+
+namespace moist {
+
+template <class T>
+struct StateP {
+    T *rho, *ru, *rw, *rt, *qv, *qc, *qr;
+};
+
+template <class T>
+struct PhysP {  // the six phys tendencies of compute_step! (moist.jl:1039)
+    T *d_rho, *d_u, *d_th, *d_qv, *d_qc, *d_qr;
+};
+
+// error word: err[0] = smallest MOIST_FIELD_* with a NaN (INT_MAX if none)
+__device__ __forceinline__ bool halted(const int* err) { return *(volatile const int*)err != INT_MAX; }
+
+#define MOIST_IDX(k, i) ((size_t)(k) * P + (i))
+
+// ----------------------------------------------------------------------------- physics
+
+// surface_fluxes! (moist.jl:714-751), one thread per column. ru_left / rho_right are the
+// reference's halo reads rho_u[ks, is-1] and rho[ks, ie+1], which hold the values of the
+// last halo exchange (start of the last RK stage), not the current interior.
+template <class T>
+__global__ void k_surface_fluxes(DevParams<T> p, StateP<T> s, const T* ru_left, const T* rho_right,
+                                 T* d_u_sf, T* d_th_sf, T* d_qv_sf, T* mflux, T* shflux, T* lhflux,
+                                 const int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = p.nx;
+    if (i >= nx || halted(err)) return;
+    const T rho = s.rho[i], qv = s.qv[i] / rho, qc = s.qc[i] / rho, qr = s.qr[i] / rho;
+    const T qd = T(1.0) - qv - qc - qr;
+    const T r = p.Rd * qd + p.Rv * qv;
+    const T cp = p.Cpd * qd + p.Cpv * qv + p.Cpl * (qc + qr);
+    const T cv = cp - r;
+    const T ru_m = (i == 0) ? *ru_left : s.ru[i - 1];
+    const T rho_p1 = (i == nx - 1) ? *rho_right : s.rho[i + 1];
+    T uabs = mm::mabs(ru_m + s.ru[i]) * T(0.5) / rho;
+    uabs = jmax(uabs, p.uabs_min);
+    const T theta_ks = s.rt[i] / rho;
+    const T pi_ks = mm::mpow(r * s.rt[i] / p.P0, r / cv);
+    const T pi_surf = pi_ks + p.dz[0] * T(0.5) * p.GRAV / (cp * theta_ks);
+    const T p_surf = p.P0 * mm::mpow(pi_surf, cp / r);
+    const T rho_surf = p_surf / (r * p.temp_surf);
+    const T theta_surf = p.temp_surf / pi_surf;
+    const T u = s.ru[i] / (rho + rho_p1) * T(2.0);
+    const T mf = -rho_surf * p.Cd * u * mm::mabs(u);
+    mflux[i] = mf;
+    d_u_sf[i] = mf / p.dz[0];
+    const T sh = rho_surf * p.Ch * uabs * (theta_surf - theta_ks) * pi_surf;
+    d_th_sf[i] = sh / (pi_ks * p.dz[0]);
+    shflux[i] = sh * cp;
+    T es, d1, qsat_s, d2;
+    sat_vp(p.temp_surf, p, es, d1);
+    sat_q(p_surf, es, p, qsat_s, d2);
+    const T lh = rho_surf * p.Ce * uabs * (qsat_s - qv);
+    d_qv_sf[i] = lh / p.dz[0];
+    lhflux[i] = lh * p.Lv;
+}
+
+template <class T>
+__device__ __forceinline__ T tanh_m(T x) {  // tanh from the shared exp
+    const T e = mm::mexp(T(2) * x);
+    return (e - T(1)) / (e + T(1));
+}
+
+// gray_radiation! (moist.jl:776-840), one thread per column; LW_up / LW_dn scratch [nz+1][P]
+template <class T>
+__global__ void k_gray_radiation(DevParams<T> p, StateP<T> s, const T* theta_ref, T* lw_up,
+                                 T* lw_dn, T* d_th_rd, const int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    if (i >= nx || halted(err)) return;
+    auto col = [&](int k, T& cpk, T& pik, T& tempk, T& epsk, T& tauk) {
+        const size_t c = MOIST_IDX(k, i);
+        const T rho = s.rho[c];
+        const T qv = s.qv[c] / rho, qc = s.qc[c] / rho, qr = s.qr[c] / rho;
+        const T qd = T(1.0) - qv - qc - qr;
+        const T r = p.Rd * qd + p.Rv * qv;
+        cpk = p.Cpd * qd + p.Cpv * qv + p.Cpl * (qc + qr);
+        const T cv = cpk - r;
+        pik = mm::mpow(r * s.rt[c] / p.P0, r / cv);
+        tempk = s.rt[c] / rho * pik;
+        const T dq = p.k_abs_qv * s.qv[c] * p.dz[k];
+        const T dc = p.k_abs_qc * s.qc[c] * p.dz[k];
+        const T dr = p.k_abs_qr * s.qr[c] * p.dz[k];
+        epsk = T(1.0) - mm::mexp(-(dq + dc + dr));
+        tauk = T(1.0) - epsk;
+    };
+    T cpk, pik, tempk, epsk, tauk;
+    T up = p.surf_emissivity * p.SIGMA * mm::mpow4(p.temp_surf);
+    lw_up[MOIST_IDX(0, i)] = up;
+    for (int k = 0; k < nz; k++) {
+        col(k, cpk, pik, tempk, epsk, tauk);
+        up = up * tauk + epsk * p.SIGMA * mm::mpow4(tempk);
+        lw_up[MOIST_IDX(k + 1, i)] = up;
+    }
+    T dn = T(0.0);
+    lw_dn[MOIST_IDX(nz, i)] = dn;
+    for (int k = nz - 1; k >= 0; k--) {
+        col(k, cpk, pik, tempk, epsk, tauk);
+        dn = dn * tauk + epsk * p.SIGMA * mm::mpow4(tempk);
+        lw_dn[MOIST_IDX(k, i)] = dn;
+    }
+    const T dz_trans = T(2.0e3);
+    for (int k = 0; k < nz; k++) {
+        col(k, cpk, pik, tempk, epsk, tauk);
+        const T divF = ((lw_up[MOIST_IDX(k + 1, i)] - lw_dn[MOIST_IDX(k + 1, i)]) -
+                        (lw_up[MOIST_IDX(k, i)] - lw_dn[MOIST_IDX(k, i)])) / p.dz[k];
+        const T hr = -divF / (cpk * pik);
+        const T alpha = T(0.5) * (T(1.0) + tanh_m((p.z[k] - (p.z_trop + dz_trans * T(0.5))) / dz_trans)) /
+                        p.tau_cooling;
+        const size_t c = MOIST_IDX(k, i);
+        const T cr = -(s.rt[c] - s.rho[c] * theta_ref[k]) * alpha;
+        d_th_rd[c] = hr + cr;
+    }
+}
+
+// Kessler microphysics + rain sedimentation + assembly of the six phys tendencies
+// (moist.jl:1593-1644), one thread per cell.
+template <class T>
+__global__ void k_physics(DevParams<T> p, StateP<T> s, T* d_th_mp, T* d_qv_mp, T* d_qc_mp, T* d_qr_mp,
+                          T* d_qr_sed, T* d_prec, const T* d_th_rd, const T* d_u_sf, const T* d_th_sf,
+                          const T* d_qv_sf, PhysP<T> ph, const int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    if (i >= nx || k >= nz || halted(err)) return;
+    const size_t c = MOIST_IDX(k, i);
+    const T rho = s.rho[c], rt = s.rt[c], rqr = s.qr[c];
+    T dqv = T(0), dqc = T(0), dqr = T(0), dth = T(0);
+    if (p.do_mp) kessler_cell(rho, rt, s.qv[c], s.qc[c], rqr, p, dqv, dqc, dqr, dth);
+    T sed = T(0);
+    if (p.do_mp && p.do_sed) {
+        const T vt = terminal_velocity(rqr, rho, p);
+        const T flux_kp = (k == nz - 1) ? T(0.0) : s.qr[c + P] * terminal_velocity(s.qr[c + P], s.rho[c + P], p);
+        const T flux_km = rqr * vt;
+        sed = (flux_kp - flux_km) / p.dz[k];
+        if (k == 0) d_prec[i] = rqr * vt;
+    } else if (k == 0) {
+        d_prec[i] = T(0);
+    }
+    d_th_mp[c] = dth;
+    d_qv_mp[c] = dqv;
+    d_qc_mp[c] = dqc;
+    d_qr_mp[c] = dqr;
+    d_qr_sed[c] = sed;
+    // phys assembly, in the reference's order (moist.jl:1633-1643)
+    const T th_rd = p.do_rd ? d_th_rd[c] : T(0.0);
+    T d_rho = sed;
+    if (k == 0) d_rho += d_qv_sf[i];
+    T d_u = T(0.0);
+    if (k == 0) d_u += d_u_sf[i];
+    T d_th = dth + th_rd + d_rho * rt / rho;
+    if (k == 0) d_th += d_th_sf[i];
+    T d_qv = dqv;
+    if (k == 0) d_qv += d_qv_sf[i];
+    ph.d_rho[c] = d_rho;
+    ph.d_u[c] = d_u;
+    ph.d_th[c] = d_th;
+    ph.d_qv[c] = d_qv;
+    ph.d_qc[c] = dqc;
+    ph.d_qr[c] = dqr + sed;
+}
+
+// ----------------------------------------------------------------------------- stage prologue
+
+// diagnostics (moist.jl:1048-1062) and face velocities u_face, w_face (1091-1097, 1185-1189)
+template <class T>
+__global__ void k_diag(DevParams<T> p, StateP<T> s, T* pres, T* theta, T* rt2pres, T* u_face,
+                       T* w_face, const int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    if (i >= nx || k >= nz || halted(err)) return;
+    const size_t c = MOIST_IDX(k, i);
+    const T rho = s.rho[c], rt = s.rt[c];
+    const T qv = s.qv[c] / rho, qc = s.qc[c] / rho, qr = s.qr[c] / rho;
+    const T qd = T(1.0) - qv - qc - qr;
+    const T r = p.Rd * qd + p.Rv * qv;
+    const T cp = p.Cpd * qd + p.Cpv * qv + p.Cpl * (qc + qr);
+    const T cv = cp - r;
+    const T pr = p.P0 * mm::mpow(r * rt / p.P0, cp / cv);
+    pres[c] = pr;
+    theta[c] = rt / rho;
+    rt2pres[c] = cp / cv * pr / rt;
+    const int ip = wrapx(i + 1, nx);
+    u_face[c] = s.ru[c] * T(2.0) / (rho + s.rho[MOIST_IDX(k, ip)]);
+    if (k < nz - 1) w_face[c] = s.rw[c] / f2h(rho, s.rho[c + P], p.dz[k], p.dz[k + 1]);
+}
+
+template <class T>
+struct TendArgs {
+    StateP<T> s, s0;
+    PhysP<T> ph;
+    const T *pres, *theta, *u_face, *w_face;
+    T *R_rho, *R_ru, *R_rw, *R_rt;
+    T *rho_p, *ru_p, *rw_p, *rt_p, *mfx, *mfz;
+    T *ru_left, *rho_right;  // halo values of the stage's exchange, for surface_fluxes!
+};
+
+// slow tendencies R_rho, R_rho_u, R_rho_w, R_rho_theta (moist.jl:1079-1332), perturbation
+// initialisation and the saved momentum fluxes (1339-1348)
+template <class T>
+__global__ void k_tend(DevParams<T> p, TendArgs<T> a, const int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    if (i >= nx || k >= nz || halted(err)) return;
+    const T EPS = p.EPS, dx = p.dx, GRAV = p.GRAV;
+    const T* dz = p.dz;
+    const T* z = p.z;
+    const int im = wrapx(i - 1, nx), im2 = wrapx(i - 2, nx), ip = wrapx(i + 1, nx), ip2 = wrapx(i + 2, nx);
+    const int ke = nz - 1;
+    const size_t c = MOIST_IDX(k, i);
+    const T* rho = a.s.rho;
+    const T* ru = a.s.ru;
+    const T* rw = a.s.rw;
+    const T* uf = a.u_face;
+    const T* wf = a.w_face;
+    const T* th = a.theta;
+    auto R = [&](int kk, int ii) { return MOIST_IDX(kk, ii); };
+
+    if (k == 0 && i == 0) {
+        *a.ru_left = ru[R(0, nx - 1)];
+        *a.rho_right = rho[R(0, 0)];
+    }
+
+    // --- R_rho (1079-1086)
+    {
+        const T flux_kp = k == ke ? T(0.0) : rw[c];
+        const T flux_km = k == 0 ? T(0.0) : rw[c - P];
+        const T advection = -((ru[c] - ru[R(k, im)]) / dx + (flux_kp - flux_km) / dz[k]);
+        a.R_rho[c] = advection + a.ph.d_rho[c];
+    }
+    // --- R_rho_u (1098-1178)
+    {
+        const T rho_u_ip = T(0.5) * (ru[c] + ru[R(k, ip)]);
+        T f_ip;
+        if (rho_u_ip > EPS)
+            f_ip = up3(rho_u_ip, uf[R(k, im)], uf[c], uf[R(k, ip)]);
+        else if (rho_u_ip < -EPS)
+            f_ip = up3(rho_u_ip, uf[R(k, ip2)], uf[R(k, ip)], uf[c]);
+        else
+            f_ip = rho_u_ip * (uf[c] + uf[R(k, ip)]) * T(0.5);
+        const T rho_u_im = T(0.5) * (ru[R(k, im)] + ru[c]);
+        T f_im;
+        if (rho_u_im > EPS)
+            f_im = up3(rho_u_im, uf[R(k, im2)], uf[R(k, im)], uf[c]);
+        else if (rho_u_im < -EPS)
+            f_im = up3(rho_u_im, uf[R(k, ip)], uf[c], uf[R(k, im)]);
+        else
+            f_im = rho_u_im * (uf[R(k, im)] + uf[c]) * T(0.5);
+        const T druudx = (f_ip - f_im) / dx;
+        T f_kp;
+        if (k == ke) {
+            f_kp = T(0.0);
+        } else {
+            const T rho_w_kp = T(0.5) * (rw[c] + rw[R(k, ip)]);
+            if (rho_w_kp > EPS && k > 0)
+                f_kp = up3(rho_w_kp, uf[c - P], uf[c], uf[c + P]);
+            else if (rho_w_kp < -EPS && k < ke - 1)
+                f_kp = up3(rho_w_kp, uf[c + 2 * P], uf[c + P], uf[c]);
+            else
+                f_kp = rho_w_kp * f2h(uf[c], uf[c + P], dz[k], dz[k + 1]);
+        }
+        T f_km;
+        if (k == 0) {
+            f_km = T(0.0);
+        } else {
+            const T rho_w_km = T(0.5) * (rw[c - P] + rw[R(k - 1, ip)]);
+            if (rho_w_km > EPS && k > 1)
+                f_km = up3(rho_w_km, uf[c - 2 * P], uf[c - P], uf[c]);
+            else if (rho_w_km < -EPS && k < ke)
+                f_km = up3(rho_w_km, uf[c + P], uf[c], uf[c - P]);
+            else
+                f_km = rho_w_km * f2h(uf[c - P], uf[c], dz[k - 1], dz[k]);
+        }
+        const T drwudz = (f_kp - f_km) / dz[k];
+        const T advection = -druudx - drwudz;
+        const T u_ip = (uf[R(k, ip)] - uf[c]) / dx;
+        const T u_im = (uf[c] - uf[R(k, im)]) / dx;
+        const T u_xx = (u_ip * rho[R(k, ip)] - u_im * rho[c]) / dx;
+        const T u_kp = k == ke ? T(0.0) : (uf[c + P] - uf[c]) / (z[k + 1] - z[k]);
+        const T u_km = k == 0 ? T(0.0) : (uf[c] - uf[c - P]) / (z[k] - z[k - 1]);
+        const T rho_kp = k == ke ? T(0.0) : T(0.25) * (rho[c] + rho[c + P] + rho[R(k, ip)] + rho[R(k + 1, ip)]);
+        const T rho_km = k == 0 ? T(0.0) : T(0.25) * (rho[c - P] + rho[c] + rho[R(k - 1, ip)] + rho[R(k, ip)]);
+        const T u_zz = (u_kp * rho_kp - u_km * rho_km) / dz[k];
+        const T diffusion = p.nu * (u_xx + u_zz);
+        const T dpdx = (a.pres[R(k, ip)] - a.pres[c]) / dx;
+        a.R_ru[c] = advection - dpdx + diffusion + a.ph.d_u[c];
+    }
+    // --- R_rho_w (1190-1278)
+    if (k < ke) {
+        const T rho_u_ip = f2h(ru[c], ru[c + P], z[k], z[k + 1]);  // z weights, as written (1196)
+        T f_ip;
+        if (rho_u_ip > EPS)
+            f_ip = up3(rho_u_ip, wf[R(k, im)], wf[c], wf[R(k, ip)]);
+        else if (rho_u_ip < -EPS)
+            f_ip = up3(rho_u_ip, wf[R(k, ip2)], wf[R(k, ip)], wf[c]);
+        else
+            f_ip = rho_u_ip * (wf[c] + wf[R(k, ip)]) * T(0.5);
+        const T rho_u_im = f2h(ru[R(k, im)], ru[R(k + 1, im)], dz[k], dz[k + 1]);
+        T f_im;
+        if (rho_u_im > EPS)
+            f_im = up3(rho_u_im, wf[R(k, im2)], wf[R(k, im)], wf[c]);
+        else if (rho_u_im < -EPS)
+            f_im = up3(rho_u_im, wf[R(k, ip)], wf[c], wf[R(k, im)]);
+        else
+            f_im = rho_u_im * (wf[R(k, im)] + wf[c]) * T(0.5);
+        const T drwudx = (f_ip - f_im) / dx;
+        T f_kp;
+        if (k == ke - 1) {
+            f_kp = T(0.0);
+        } else {
+            const T rho_w_kp = f2h(rw[c], rw[c + P], dz[k], dz[k + 1]);
+            if (rho_w_kp > EPS && k > 0)
+                f_kp = up3(rho_w_kp, wf[c - P], wf[c], wf[c + P]);
+            else if (rho_w_kp < -EPS && k < ke - 2)
+                f_kp = up3(rho_w_kp, wf[c + 2 * P], wf[c + P], wf[c]);
+            else
+                f_kp = rho_w_kp * f2h(wf[c], wf[c + P], dz[k], dz[k + 1]);
+        }
+        T f_km;
+        if (k == 0) {
+            f_km = T(0.0);
+        } else {
+            const T rho_w_km = f2h(rw[c - P], rw[c], dz[k - 1], dz[k]);
+            if (rho_w_km > EPS && k > 1)
+                f_km = up3(rho_w_km, wf[c - 2 * P], wf[c - P], wf[c]);
+            else if (rho_w_km < -EPS && k < ke - 1)
+                f_km = up3(rho_w_km, wf[c + P], wf[c], wf[c - P]);
+            else
+                f_km = rho_w_km * f2h(wf[c - P], wf[c], dz[k - 1], dz[k]);
+        }
+        const T drwwdz = (f_kp - f_km) / (z[k + 1] - z[k]);
+        const T advection = -drwudx - drwwdz;
+        const T w_ip = (wf[R(k, ip)] - wf[c]) / dx;
+        const T w_im = (wf[c] - wf[R(k, im)]) / dx;
+        const T rho_ip = T(0.25) * (rho[c] + rho[c + P] + rho[R(k, ip)] + rho[R(k + 1, ip)]);
+        const T rho_im = T(0.25) * (rho[R(k, im)] + rho[R(k + 1, im)] + rho[c] + rho[c + P]);
+        const T w_xx = (w_ip * rho_ip - w_im * rho_im) / dx;
+        const T w_kp = k == ke - 1 ? T(0.0) : (wf[c + P] - wf[c]) / dz[k + 1];
+        const T w_km = k == 0 ? T(0.0) : (wf[c] - wf[c - P]) / dz[k];
+        const T w_zz = (w_kp * rho[c + P] - w_km * rho[c]) / (z[k + 1] - z[k]);
+        const T diffusion = p.nu * (w_xx + w_zz);
+        T sigma = T(0.0);
+        const T zfk = p.zf[k];
+        if (zfk > (T(1.0) - p.zf_sponge) * p.H)
+            sigma = (GRAV / T(30.0)) * ((zfk - (T(1.0) - p.zf_sponge) * p.H) / (p.zf_sponge * p.H));
+        const T sponge = -sigma * rw[c];
+        const T dpdz = (a.pres[c + P] - a.pres[c]) / (z[k + 1] - z[k]);
+        const T buoyancy = -GRAV * (rho[c] + rho[c + P]) * T(0.5);
+        a.R_rw[c] = advection - dpdz + buoyancy + diffusion + sponge;
+    }
+    // --- R_rho_theta (1284-1331)
+    {
+        const T ru_i = ru[c], ru_m = ru[R(k, im)];
+        T f_ip, f_im, f_kp, f_km;
+        if (ru_i > EPS)
+            f_ip = up3(ru_i, th[R(k, im)], th[c], th[R(k, ip)]);
+        else if (ru_i < -EPS)
+            f_ip = up3(ru_i, th[R(k, ip2)], th[R(k, ip)], th[c]);
+        else
+            f_ip = ru_i * (th[c] + th[R(k, ip)]) * T(0.5);
+        if (ru_m > EPS)
+            f_im = up3(ru_m, th[R(k, im2)], th[R(k, im)], th[c]);
+        else if (ru_m < -EPS)
+            f_im = up3(ru_m, th[R(k, ip)], th[c], th[R(k, im)]);
+        else
+            f_im = ru_m * (th[R(k, im)] + th[c]) * T(0.5);
+        if (k == ke) {
+            f_kp = T(0.0);
+        } else {
+            const T w = rw[c];
+            if (w > EPS && k > 0)
+                f_kp = up3(w, th[c - P], th[c], th[c + P]);
+            else if (w < -EPS && k < ke - 1)
+                f_kp = up3(w, th[c + 2 * P], th[c + P], th[c]);
+            else
+                f_kp = w * f2h(th[c], th[c + P], dz[k], dz[k + 1]);
+        }
+        if (k == 0) {
+            f_km = T(0.0);
+        } else {
+            const T w = rw[c - P];
+            if (w > EPS && k > 1)
+                f_km = up3(w, th[c - 2 * P], th[c - P], th[c]);
+            else if (w < -EPS && k < ke)
+                f_km = up3(w, th[c + P], th[c], th[c - P]);
+            else
+                f_km = w * f2h(th[c - P], th[c], dz[k - 1], dz[k]);
+        }
+        const T advection = -((f_ip - f_im) / dx + (f_kp - f_km) / dz[k]);
+        a.R_rt[c] = advection + a.ph.d_th[c];
+    }
+    // --- perturbations and saved momentum fluxes (1339-1348)
+    a.rho_p[c] = a.s0.rho[c] - rho[c];
+    a.ru_p[c] = a.s0.ru[c] - ru[c];
+    a.rw_p[c] = a.s0.rw[c] - rw[c];
+    a.rt_p[c] = a.s0.rt[c] - a.s.rt[c];
+    a.mfx[c] = ru[c];
+    a.mfz[c] = rw[c];
+}
+
+// Per-stage factorisation of the w-p tridiagonal system (implicit_correction!, moist.jl:
+// 982-1021; solve_tridiagonal!, 956-966). The coefficients depend only on theta, rt2pres and
+// dt_s, which are fixed during a stage, so the pivots and modified super-diagonal are formed
+// once per stage; each substep then repeats only the right-hand-side recurrence.
+template <class T, class TT>
+__global__ void k_thomas_factors(DevParams<T> p, const T* theta, const T* rt2pres, T dt_s, T* ta, T* tb,
+                                 T* tc, TT* tcp, TT* tpiv, const int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    if (i >= nx || halted(err)) return;
+    const T* dz = p.dz;
+    const T* z = p.z;
+    const int ke = nz - 1, n = nz - 1;
+    const T fact_tp = T(0.5) * (T(1.0) + p.beta);
+    const T dt_tp2 = (dt_s * fact_tp) * (dt_s * fact_tp);
+    T th_prev = T(0), th_cur = f2h(theta[MOIST_IDX(0, i)], theta[MOIST_IDX(1, i)], dz[0], dz[1]);
+    TT cp_prev = TT(0);
+    for (int j = 0; j < n; j++) {
+        const int k = j;
+        const T th_next = (k + 1 <= ke - 1) ? f2h(theta[MOIST_IDX(k + 1, i)], theta[MOIST_IDX(k + 2, i)], dz[k + 1], dz[k + 2]) : T(0);
+        const T r_k = rt2pres[MOIST_IDX(k, i)], r_kp = rt2pres[MOIST_IDX(k + 1, i)];
+        const T b = dt_tp2 * (r_k / dz[k] + r_kp / dz[k + 1]) * th_cur / (z[k + 1] - z[k]);
+        const T a = (k > 0) ? -dt_tp2 * (r_k * th_prev / ((z[k + 1] - z[k]) * dz[k]) - p.GRAV / (dz[k] + dz[k + 1])) : T(0);
+        const T c = (k < ke - 1) ? -dt_tp2 * (r_kp * th_next / ((z[k + 1] - z[k]) * dz[k + 1]) + p.GRAV / (dz[k] + dz[k + 1])) : T(0);
+        ta[MOIST_IDX(j, i)] = a;
+        tb[MOIST_IDX(j, i)] = b;
+        tc[MOIST_IDX(j, i)] = c;
+        const T bb = b + T(1.0);
+        TT piv, cpj;
+        if (j == 0) {
+            piv = (TT)bb;
+            cpj = (TT)c / piv;
+        } else {
+            piv = (TT)bb - (TT)a * cp_prev;
+            cpj = (TT)c / piv;
+        }
+        tcp[MOIST_IDX(j, i)] = cpj;
+        tpiv[MOIST_IDX(j, i)] = piv;
+        cp_prev = cpj;
+        th_prev = th_cur;
+        th_cur = th_next;
+    }
+}
+
+template <class T, class TT>
+struct SubArgs {
+    const T *R_rho, *R_ru, *R_rw, *R_rt, *theta, *rt2pres, *s_rw;
+    const T *ru_in, *rt_in, *rt_old;  // rho_u_p, rho_theta_p and rho_theta_p_old at substep start
+    T *ru_out, *rt_out;               // rho_u_p, rho_theta_p after the substep
+    T *rho_p, *rw_p, *mfx, *mfz;      // updated in place (each column owns its entries)
+    const T *ta, *tb, *tc;
+    const TT *tcp, *tpiv;
+    TT* dprime;                       // scratch [nz][P]
+};
+
+// One acoustic substep (moist.jl:1355-1459), one thread per column i: horizontal forward
+// step of rho_u_p at faces i-1/2 (recomputed, bitwise equal to column i-1's) and i+1/2,
+// explicit rho_p / rho_theta_p, off-centred right-hand side, Thomas sweep for rho_w_p,
+// vertical rho_p / rho_theta_p updates, time-averaged momentum fluxes.
+template <class T, class TT>
+__global__ void k_substep(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T, double fact_tp64,
+                          const int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    if (i >= nx || halted(err)) return;
+    const T dx = p.dx, EPS = p.EPS;
+    const T* dz = p.dz;
+    const T* z = p.z;
+    const int im = wrapx(i - 1, nx), ip = wrapx(i + 1, nx);
+    const int ke = nz - 1, n = nz - 1;
+    const T fact_tpT = T(0.5) * (T(1.0) + p.beta);
+    const T fact_tmT = T(0.5) * (T(1.0) - p.beta);
+    const T fact = fact_tmT / fact_tpT;
+    auto u_update = [&](int k, int cc) {
+        const int cn = wrapx(cc + 1, nx);
+        const size_t a0 = MOIST_IDX(k, cc), a1 = MOIST_IDX(k, cn);
+        T grad_x = (a.rt_in[a1] - a.rt_in[a0]) / dx;
+        const T grad_x_old = (a.rt_old[a1] - a.rt_old[a0]) / dx;
+        grad_x = grad_x + p.gamma_d * (grad_x - grad_x_old);
+        const T rt2pres_h = (a.rt2pres[a0] + a.rt2pres[a1]) * T(0.5);
+        return a.ru_in[a0] + dt_s * (a.R_ru[a0] - rt2pres_h * grad_x);
+    };
+    T rho_tp_prev = T(0), rt_tp_prev = T(0);
+    TT dprev = TT(0);
+    for (int k = 0; k < nz; k++) {
+        const size_t c = MOIST_IDX(k, i);
+        const T u_m = u_update(k, im);
+        const T u_p = u_update(k, i);
+        a.ru_out[c] = u_p;
+        a.mfx[c] = a.mfx[c] + u_p / ns_T;
+        T advection = -(u_p - u_m) / dx;
+        T inc = dt_s * (a.R_rho[c] + advection);
+        const T rho_tp = (T)((double)a.rho_p[c] + fact_tp64 * (double)inc);
+        a.rho_p[c] = a.rho_p[c] + inc;
+        const T th_i = a.theta[c], th_ip = a.theta[MOIST_IDX(k, ip)], th_im = a.theta[MOIST_IDX(k, im)];
+        const T flux_ip = (th_ip + th_i) * T(0.5) * u_p;
+        const T flux_im = (th_i + th_im) * T(0.5) * u_m;
+        advection = -(flux_ip - flux_im) / dx;
+        inc = dt_s * (a.R_rt[c] + advection);
+        const T rtp = a.rt_in[c];
+        const T rt_tp = (T)((double)rtp + fact_tp64 * (double)inc);
+        a.rt_out[c] = rtp + inc;
+        if (k >= 1) {
+            const int j = k - 1;
+            const size_t cj = c - P;
+            const T buoyancy = (rt_tp - rt_tp_prev) / (z[k] - z[j]);
+            const T grav = -p.GRAV * T(0.5) * (rho_tp + rho_tp_prev);
+            const T rt2pres_h = (a.rt2pres[cj] + a.rt2pres[c]) * T(0.5);
+            const T drho_w = dt_s * (a.R_rw[cj] - rt2pres_h * buoyancy + grav);
+            const T w_j = a.rw_p[cj];
+            T d = w_j + drho_w;
+            if (j > 0) d -= a.ta[cj] * fact * w_j;
+            d -= a.tb[cj] * fact * w_j;
+            if (j < n - 1) d -= a.tc[cj] * fact * a.rw_p[c];
+            TT dp;
+            if (j == 0)
+                dp = (TT)d / a.tpiv[cj];
+            else
+                dp = ((TT)d - (TT)a.ta[cj] * dprev) / a.tpiv[cj];
+            a.dprime[cj] = dp;
+            dprev = dp;
+        }
+        rho_tp_prev = rho_tp;
+        rt_tp_prev = rt_tp;
+    }
+    // back substitution (moist.jl:968-970)
+    {
+        TT x = dprev;
+        a.rw_p[MOIST_IDX(n - 1, i)] = (T)x;
+        for (int j = n - 2; j >= 0; j--) {
+            x = a.dprime[MOIST_IDX(j, i)] - a.tcp[MOIST_IDX(j, i)] * x;
+            a.rw_p[MOIST_IDX(j, i)] = (T)x;
+        }
+    }
+    // vertical rho_p, rho_theta_p updates (1412-1446) and momentum flux averages (1452-1458)
+    const T* th = a.theta;
+    for (int k = 0; k < nz; k++) {
+        const size_t c = MOIST_IDX(k, i);
+        {
+            const T flux_kp = k == ke ? T(0.0) : a.rw_p[c];
+            const T flux_km = k == 0 ? T(0.0) : a.rw_p[c - P];
+            const T advection = -(flux_kp - flux_km) / dz[k];
+            a.rho_p[c] = a.rho_p[c] + dt_s * advection;
+        }
+        T flux_kp, flux_km;
+        if (k == ke) {
+            flux_kp = T(0.0);
+        } else {
+            const T wp = a.rw_p[c];
+            if (wp > EPS && k > 0)
+                flux_kp = up3(wp, th[c - P], th[c], th[c + P]);
+            else if (a.s_rw[c] < -EPS && k < ke - 1)  // selector on s.rho_w, as written (1426)
+                flux_kp = up3(wp, th[c + 2 * P], th[c + P], th[c]);
+            else
+                flux_kp = wp * f2h(th[c], th[c + P], dz[k], dz[k + 1]);
+        }
+        if (k == 0) {
+            flux_km = T(0.0);
+        } else {
+            const T wp = a.rw_p[c - P];
+            const T sw = a.s_rw[c - P];
+            if (sw > EPS && k > 1)
+                flux_km = up3(wp, th[c - 2 * P], th[c - P], th[c]);
+            else if (sw < -EPS && k < ke)
+                flux_km = up3(wp, th[c + P], th[c], th[c - P]);
+            else
+                flux_km = wp * f2h(th[c - P], th[c], dz[k - 1], dz[k]);
+        }
+        const T advection = -(flux_kp - flux_km) / dz[k];
+        a.rt_out[c] = a.rt_out[c] + dt_s * advection;
+        if (k < ke) a.mfz[c] = a.mfz[c] + a.rw_p[c] / ns_T;
+    }
+}
+
+// ----------------------------------------------------------------------------- tracers
+
+template <class T>
+struct TracerArgs {
+    const T* q_old[3];   // rho_qv, rho_qc, rho_qr at the start of the sweep
+    T* q_new[3];         // results
+    const T* q0[3];      // s0 tracers
+    const T* dphys[3];   // d_rho_q*_phys
+    const T *rho, *mfx, *mfz;
+    T dt;                // stage dt
+};
+
+// The tracer update of one cell (moist.jl:1479-1515), given the scalar values s = rho_q/rho it
+// reads: "new" values at (k, i-1), (k, i-2), (k-1, i), (k-2, i) and stage-start values elsewhere.
+template <class T>
+__device__ __forceinline__ T tracer_cell(const DevParams<T>& p, const TracerArgs<T>& a, int t, int k, int i,
+                                         T s_c, T s_ip1, T s_ip2, T s_kp1, T s_kp2, T s_im1, T s_im2,
+                                         T s_km1, T s_km2, T lin_km1, T lin_k, T lin_kp1) {
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    const int ke = nz - 1;
+    const T EPS = p.EPS, dx = p.dx;
+    const T* dz = p.dz;
+    const T* z = p.z;
+    const size_t c = MOIST_IDX(k, i);
+    const int im = wrapx(i - 1, nx), ip = wrapx(i + 1, nx);
+    const T fx_ip = limited_flux_x(a.mfx[c], s_im1, s_c, s_ip1, s_ip2, EPS);
+    const T fx_im = limited_flux_x(a.mfx[MOIST_IDX(k, im)], s_im2, s_im1, s_c, s_ip1, EPS);
+    const T adv_x = (fx_ip - fx_im) / dx;
+    const T fz_kp = k == ke ? T(0.0)
+                            : limited_flux_z(a.mfz[c], s_km1, s_c, s_kp1, s_kp2, k, nz, dz[k], dz[k + 1], lin_k,
+                                             lin_kp1, p.dt, EPS);
+    const T fz_km = k == 0 ? T(0.0)
+                           : limited_flux_z(a.mfz[c - P], s_km2, s_km1, s_c, s_kp1, k - 1, nz, dz[k - 1], dz[k],
+                                            lin_km1, lin_k, p.dt, EPS);
+    const T adv_z = (fz_kp - fz_km) / dz[k];
+    const T advection = -(adv_x + adv_z);
+    const T* rho = a.rho;
+    const T r_c = rho[c];
+    const T scalar_kp = k == ke ? T(0.0) : s_kp1;
+    const T scalar_km = k == 0 ? T(0.0) : s_km1;
+    const T dsdx_ip = (rho[MOIST_IDX(k, ip)] + r_c) * T(0.5) * (s_ip1 - s_c) / dx;
+    const T dsdx_im = (r_c + rho[MOIST_IDX(k, im)]) * T(0.5) * (s_c - s_im1) / dx;
+    const T diff_x = p.kappa * (dsdx_ip - dsdx_im) / dx;
+    const T dsdz_kp = k == ke ? T(0.0) : f2h(rho[c + P], r_c, dz[k + 1], dz[k]) * (scalar_kp - s_c) / (z[k + 1] - z[k]);
+    const T dsdz_km = k == 0 ? T(0.0) : f2h(r_c, rho[c - P], dz[k], dz[k - 1]) * (s_c - scalar_km) / (z[k] - z[k - 1]);
+    const T diff_z = p.kappa * (dsdz_kp - dsdz_km) / dz[k];
+    const T diffusion = diff_x + diff_z;
+    return a.q0[t][c] + a.dt * (advection + diffusion + a.dphys[t][c]);
+}
+
+// Exact lexicographic Gauss-Seidel sweep (moist.jl:1469-1518: i outer, k inner, in place),
+// one block per tracer, thread k owns row k and processes column i = t - k at wavefront step t.
+// Cell (k, i) depends on updated (k, i-1), (k, i-2), (k-1, i), (k-2, i), which are final by step
+// t - 1 / t - 2; a 3-slot ring in shared memory carries the row neighbours' new values.
+template <class T>
+__global__ void k_tracer_wavefront(DevParams<T> p, TracerArgs<T> a, const int* err) {
+    extern __shared__ unsigned char smem_raw[];
+    T* ring = reinterpret_cast<T*>(smem_raw);  // [3][nz]
+    const int t = blockIdx.x;
+    const int k = threadIdx.x;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    if (halted(err)) return;
+    const T* qo = a.q_old[t];
+    const T* rho = a.rho;
+    auto s_old = [&](int kk, int ii) { const size_t cc = MOIST_IDX(kk, ii); return qo[cc] / rho[cc]; };
+    // halo column read by the linear-index clamp: reference column 1 = interior column nx-2
+    const int hcol = nx - 2;
+    const bool active = k < nz;
+    // values at (k, i-1), (k, i-2) for i = 0 are the halo columns' stage-start copies
+    T prev1 = active ? s_old(k, nx - 1) : T(0);
+    T prev2 = active ? s_old(k, nx - 2) : T(0);
+    const int nsteps = nx + nz - 1;
+    for (int step = 0; step < nsteps; step++) {
+        const int i = step - k;
+        if (active && i >= 0 && i < nx) {
+            const int ip = wrapx(i + 1, nx), ip2 = wrapx(i + 2, nx);
+            const T s_c = s_old(k, i);
+            const T s_ip1 = s_old(k, ip);
+            const T s_ip2 = s_old(k, ip2);
+            const T s_kp1 = (k + 1 < nz) ? s_old(k + 1, i) : T(0);
+            const T s_kp2 = (k + 2 < nz) ? s_old(k + 2, i) : T(0);
+            const T s_km1 = (k >= 1) ? ring[((step - 1) % 3) * nz + (k - 1)] : T(0);
+            const T s_km2 = (k >= 2) ? ring[((step - 2) % 3) * nz + (k - 2)] : T(0);
+            const T lin_km1 = (k >= 1) ? qo[MOIST_IDX(k - 1, hcol)] : T(0);
+            const T lin_k = qo[MOIST_IDX(k, hcol)];
+            const T lin_kp1 = (k + 1 < nz) ? qo[MOIST_IDX(k + 1, hcol)] : T(0);
+            const T qn = tracer_cell(p, a, t, k, i, s_c, s_ip1, s_ip2, s_kp1, s_kp2, prev1, prev2, s_km1, s_km2,
+                                     lin_km1, lin_k, lin_kp1);
+            const size_t c = MOIST_IDX(k, i);
+            a.q_new[t][c] = qn;
+            const T sn = qn / rho[c];
+            ring[(step % 3) * nz + k] = sn;
+            prev2 = prev1;
+            prev1 = sn;
+        }
+        __syncthreads();
+    }
+}
+
+// ----------------------------------------------------------------------------- stage epilogue
+
+template <class T>
+struct UpdArgs {
+    StateP<T> s_in, s_out;  // s_out.X = s_in.X + X_p; s_out.q* are the sweep results
+    const T *rho_p, *ru_p, *rw_p, *rt_p;
+    PhysP<T> ph;
+};
+
+// state update (moist.jl:1522-1539) and NaN checks (1542-1578)
+template <class T>
+__global__ void k_update(DevParams<T> p, UpdArgs<T> a, int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    if (i >= nx || k >= nz || halted(err)) return;
+    const size_t c = MOIST_IDX(k, i);
+    const T rho = a.s_in.rho[c] + a.rho_p[c];
+    const T ru = a.s_in.ru[c] + a.ru_p[c];
+    const T rt = a.s_in.rt[c] + a.rt_p[c];
+    a.s_out.rho[c] = rho;
+    a.s_out.ru[c] = ru;
+    a.s_out.rt[c] = rt;
+    T rw = a.s_in.rw[c];
+    if (k < nz - 1) rw = rw + a.rw_p[c];
+    a.s_out.rw[c] = rw;
+    int bad = INT_MAX;
+    const T v[12] = {rho, ru, rw, rt, a.s_out.qv[c], a.s_out.qc[c], a.s_out.qr[c], a.ph.d_u[c], a.ph.d_th[c],
+                     a.ph.d_qv[c], a.ph.d_qc[c], a.ph.d_qr[c]};
+#pragma unroll
+    for (int f = 11; f >= 0; f--)
+        if (v[f] != v[f]) bad = f;
+    if (bad != INT_MAX) atomicMin(err + 1, bad);  // err[1]: pending, promoted at stage end
+}
+
+// promote the stage's NaN report (err[1]) to the halt word (err[0])
+__global__ void k_stage_end(int* err) {
+    if (err[1] != INT_MAX && err[0] == INT_MAX) err[0] = err[1];
+}
+
+template <class T>
+__global__ void k_prec(DevParams<T> p, T* prec, const T* d_prec, const int* err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.nx || halted(err)) return;
+    prec[i] = prec[i] + d_prec[i] * p.dt;
+}
+
+// ----------------------------------------------------------------------------- layout moves
+
+// (ka, ia) column-major host layout <-> [nz][P] interior device layout, through a 32x32 tile
+template <class T>
+__global__ void k_from_ref(int nx, int nz, int halo, int P, const T* __restrict__ src, T* __restrict__ dst) {
+    __shared__ T tile[32][33];
+    const int k0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+    const int ka = nz;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = i0 + r, k = k0 + threadIdx.x;
+        if (i < nx && k < nz) tile[r][threadIdx.x] = src[(size_t)(i + halo) * ka + k];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int k = k0 + r, i = i0 + threadIdx.x;
+        if (i < nx && k < nz) dst[(size_t)k * P + i] = tile[threadIdx.x][r];
+    }
+}
+
+template <class T>
+__global__ void k_to_ref(int nx, int nz, int halo, int P, const T* __restrict__ src, T* __restrict__ dst) {
+    __shared__ T tile[32][33];
+    const int k0 = blockIdx.x * 32;
+    const int ia = nx + 2 * halo;
+    const int j0 = blockIdx.y * 32;  // reference column index
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int k = k0 + r, j = j0 + threadIdx.x;
+        if (j < ia && k < nz) {
+            int i = j - halo;
+            i = ((i % nx) + nx) % nx;  // halo columns as periodic copies
+            tile[r][threadIdx.x] = src[(size_t)k * P + i];
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int j = j0 + r, k = k0 + threadIdx.x;
+        if (j < ia && k < nz) dst[(size_t)j * nz + k] = tile[threadIdx.x][r];
+    }
+}
+
+}  // namespace moist

@@ -1,0 +1,794 @@
+// moist2d.cu - C-ABI of libmoist2d_sm100a.so: contexts, device buffers, step orchestration.
+//
+// A context owns one device-resident State in the [nz][P] interior layout (model.cuh) and
+// every temporary of the large step; nothing is allocated while stepping. Entry points return
+// after the work they queued on the context stream has finished.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/moist2d.h"
+#include "kernels.cuh"
+
+using namespace moist;
+
+namespace {
+
+struct CtxBase {
+    virtual ~CtxBase() {}
+    virtual int upload(const moist_state_host* s) = 0;
+    virtual int download(moist_state_host* s) = 0;
+    virtual int rk3(int nsteps) = 0;
+    virtual int compute_step(const void* const phys[6], const moist_state_host* s0, double dt, int ns) = 0;
+    virtual int microphysics() = 0;
+    virtual int sedimentation(void* d_prec) = 0;
+    virtual int budget(double out[4]) = 0;
+    virtual int time_steps(int nsteps, float* ms) = 0;
+};
+
+}  // namespace
+
+struct moist_ctx {
+    int precision = MOIST_F32;
+    int flags = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int nan_field = -1;
+    CtxBase* impl = nullptr;
+};
+
+namespace {
+
+int set_err(moist_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return set_err(owner, MOIST_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CKL()                                                                                           \
+    do {                                                                                                \
+        cudaError_t e_ = cudaGetLastError();                                                            \
+        if (e_ != cudaSuccess)                                                                          \
+            return set_err(owner, MOIST_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e_));  \
+    } while (0)
+
+inline unsigned cdiv(int a, int b) { return (unsigned)((a + b - 1) / b); }
+
+template <class T>
+DevParams<T> make_params(const moist_params* c, int P) {
+    DevParams<T> p{};
+    p.nx = c->nx;
+    p.nz = c->nz;
+    p.P = P;
+    p.dx = (T)c->dx;
+    p.dt = (T)c->dt;
+    p.H = (T)c->h;
+    p.nu = (T)c->nu;
+    p.kappa = (T)c->kappa;
+    p.gamma_d = (T)c->gamma_d;
+    p.beta = (T)c->beta_offcenter;
+    p.zf_sponge = (T)c->zf_sponge;
+    p.EPS = (T)c->eps;
+    p.GRAV = (T)c->grav;
+    p.Rd = (T)c->rd;
+    p.Rv = (T)c->rv;
+    p.Cpd = (T)c->cpd;
+    p.Cpv = (T)c->cpv;
+    p.Cpl = (T)c->cpl;
+    p.P0 = (T)c->p0;
+    p.Lv = (T)c->lv;
+    p.SIGMA = (T)c->sigma;
+    p.EPSvap = (T)c->epsvap;
+    p.K_auto = (T)c->k_auto;
+    p.Qc_threshold = (T)c->qc_threshold;
+    p.K_accr = (T)c->k_accr;
+    p.K_evap = (T)c->k_evap;
+    p.A_term = (T)c->a_term;
+    p.B_term = (T)c->b_term;
+    p.T0 = (T)c->t0;
+    p.ES0 = (T)c->es0;
+    p.A_SAT = (T)c->a_sat;
+    p.B_SAT = (T)c->b_sat;
+    p.Cd = (T)c->cd;
+    p.Ch = (T)c->ch;
+    p.Ce = (T)c->ce;
+    p.uabs_min = (T)c->uabs_min;
+    p.temp_surf = (T)c->temp_surf;
+    p.k_abs_qv = (T)c->k_abs_qv;
+    p.k_abs_qc = (T)c->k_abs_qc;
+    p.k_abs_qr = (T)c->k_abs_qr;
+    p.surf_emissivity = (T)c->surf_emissivity;
+    p.tau_cooling = (T)c->tau_cooling;
+    p.z_trop = (T)c->z_tropopause;
+    p.do_mp = c->do_mp;
+    p.do_auto = c->do_auto;
+    p.do_accr = c->do_accr;
+    p.do_revap = c->do_revap;
+    p.do_sed = c->do_sed;
+    p.do_rd = c->do_rd;
+    p.do_sf = c->do_sf;
+    return p;
+}
+
+template <class T, class TT>
+struct Ctx : CtxBase {
+    moist_ctx* owner;
+    DevParams<T> dp;
+    int nx, nz, halo, P, ns;
+    size_t fsz;  // elements of one [nz][P] field
+    cudaStream_t st;
+    std::vector<void*> allocs;
+
+    StateP<T> cur, nxt, s0b;
+    T* tmpq[3];
+    PhysP<T> ph;
+    T *d_th_mp, *d_qv_mp, *d_qc_mp, *d_qr_mp, *d_qr_sed, *d_th_rd, *lw_up, *lw_dn;
+    T *pres, *theta, *rt2p, *uface, *wface, *R_rho, *R_ru, *R_rw, *R_rt;
+    T *rho_p, *ru_p[2], *rw_p, *rt_p[3], *mfx, *mfz, *ta, *tb, *tc;
+    TT *tcp, *tpiv, *dprime;
+    T *prec, *d_prec, *mflux, *shflux, *lhflux, *d_u_sf, *d_th_sf, *d_qv_sf, *theta_ref;
+    T *halo_vals;  // [0] = rho_u[ks, is-1], [1] = rho[ks, ie+1] as of the last exchange
+    T *g_dz, *g_z, *g_zf;
+    T* staging;
+    int* err;
+    bool rd_dirty = true;
+
+    explicit Ctx(moist_ctx* o) : owner(o) {}
+
+    ~Ctx() override {
+        if (st) cudaStreamSynchronize(st);
+        for (void* a : allocs) cudaFree(a);
+    }
+
+    template <class U>
+    int alloc(U** ptr, size_t n) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(U));
+        if (e != cudaSuccess) return set_err(owner, MOIST_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(U), cudaGetErrorString(e));
+        allocs.push_back(q);
+        *ptr = (U*)q;
+        return MOIST_OK;
+    }
+
+#define AL(ptr, n)                               \
+    do {                                         \
+        int r_ = alloc(&(ptr), (n));             \
+        if (r_ != MOIST_OK) return r_;           \
+        CK(cudaMemsetAsync((ptr), 0, std::max<size_t>((n), 1) * sizeof(*(ptr)), st)); \
+    } while (0)
+
+    int init(const moist_params* c) {
+        nx = c->nx;
+        nz = c->nz;
+        halo = c->halo;
+        ns = c->ns;
+        P = (nx + 31) / 32 * 32;
+        fsz = (size_t)nz * P;
+        st = owner->stream;
+        dp = make_params<T>(c, P);
+        for (T** f : {&cur.rho, &cur.ru, &cur.rw, &cur.rt, &cur.qv, &cur.qc, &cur.qr, &nxt.rho, &nxt.ru, &nxt.rw,
+                      &nxt.rt, &nxt.qv, &nxt.qc, &nxt.qr, &tmpq[0], &tmpq[1], &tmpq[2], &ph.d_rho, &ph.d_u,
+                      &ph.d_th, &ph.d_qv, &ph.d_qc, &ph.d_qr, &d_th_mp, &d_qv_mp, &d_qc_mp, &d_qr_mp, &d_qr_sed,
+                      &d_th_rd, &pres, &theta, &rt2p, &uface, &wface, &R_rho, &R_ru, &R_rw, &R_rt, &rho_p,
+                      &ru_p[0], &ru_p[1], &rw_p, &rt_p[0], &rt_p[1], &rt_p[2], &mfx, &mfz, &ta, &tb, &tc})
+            AL(*f, fsz);
+        s0b = StateP<T>{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+        AL(lw_up, (size_t)(nz + 1) * P);
+        AL(lw_dn, (size_t)(nz + 1) * P);
+        AL(tcp, fsz);
+        AL(tpiv, fsz);
+        AL(dprime, fsz);
+        for (T** f : {&prec, &d_prec, &mflux, &shflux, &lhflux, &d_u_sf, &d_th_sf, &d_qv_sf}) AL(*f, (size_t)P);
+        AL(theta_ref, (size_t)nz);
+        AL(halo_vals, 2);
+        AL(g_dz, (size_t)nz);
+        AL(g_z, (size_t)nz);
+        AL(g_zf, (size_t)nz);
+        AL(staging, (size_t)nz * (nx + 2 * halo) + 32);
+        AL(err, 2);
+        CK(cudaMemcpyAsync(g_dz, c->dz, nz * sizeof(T), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(g_z, c->z, nz * sizeof(T), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(g_zf, c->zf, nz * sizeof(T), cudaMemcpyHostToDevice, st));
+        dp.dz = g_dz;
+        dp.z = g_z;
+        dp.zf = g_zf;
+        CK(reset_err());
+        CK(cudaStreamSynchronize(st));
+        return MOIST_OK;
+    }
+
+    cudaError_t reset_err() {
+        const int v[2] = {INT_MAX, INT_MAX};
+        return cudaMemcpyAsync(err, v, sizeof v, cudaMemcpyHostToDevice, st);
+    }
+
+    // finish: wait for the stream, read the NaN word
+    int finish() {
+        int h[2];
+        CK(cudaMemcpyAsync(h, err, sizeof h, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        CKL();
+        if (h[0] != INT_MAX) {
+            owner->nan_field = h[0];
+            static const char* names[12] = {"rho", "rho_u", "rho_w", "rho_theta", "rho_qv", "rho_qc", "rho_qr",
+                                            "d_rho_u_phys", "d_rho_theta_phys", "d_rho_qv_phys", "d_rho_qc_phys",
+                                            "d_rho_qr_phys"};
+            return set_err(owner, MOIST_ERR_NAN, "NaN detected in %s", h[0] >= 0 && h[0] < 12 ? names[h[0]] : "?");
+        }
+        owner->nan_field = -1;
+        return MOIST_OK;
+    }
+
+    // ------------------------------------------------------------------ layout moves
+    int put2d(const void* host, T* dev) {
+        if (!host) return MOIST_OK;
+        const size_t n = (size_t)nz * (nx + 2 * halo);
+        CK(cudaMemcpyAsync(staging, host, n * sizeof(T), cudaMemcpyHostToDevice, st));
+        dim3 b(32, 8), g(cdiv(nz, 32), cdiv(nx, 32));
+        k_from_ref<T><<<g, b, 0, st>>>(nx, nz, halo, P, staging, dev);
+        CKL();
+        return MOIST_OK;
+    }
+    int get2d(const T* dev, void* host, bool halos) {
+        if (!host) return MOIST_OK;
+        const int ia = nx + 2 * halo;
+        const size_t n = (size_t)nz * ia;
+        if (!halos) {  // keep the caller's halo columns: start from their current values
+            CK(cudaMemcpyAsync(staging, host, n * sizeof(T), cudaMemcpyHostToDevice, st));
+        }
+        dim3 b(32, 8), g(cdiv(nz, 32), cdiv(halos ? ia : nx, 32));
+        if (halos) {
+            k_to_ref<T><<<g, b, 0, st>>>(nx, nz, halo, P, dev, staging);
+        } else {
+            // interior only: write columns halo .. halo+nx-1 through an offset view
+            k_to_ref<T><<<g, b, 0, st>>>(nx, nz, 0, P, dev, staging + (size_t)halo * nz);
+        }
+        CKL();
+        CK(cudaMemcpyAsync(host, staging, n * sizeof(T), cudaMemcpyDeviceToHost, st));
+        return MOIST_OK;
+    }
+    int put1dx(const void* host, T* dev) {
+        if (!host) return MOIST_OK;
+        CK(cudaMemcpyAsync(dev, (const T*)host + halo, nx * sizeof(T), cudaMemcpyHostToDevice, st));
+        return MOIST_OK;
+    }
+    int get1dx(const T* dev, void* host) {
+        if (!host) return MOIST_OK;
+        CK(cudaMemcpyAsync((T*)host + halo, dev, nx * sizeof(T), cudaMemcpyDeviceToHost, st));
+        return MOIST_OK;
+    }
+
+    int upload(const moist_state_host* s) override {
+        int r;
+        StateP<T>& d = cur;
+        const void* f2[7] = {s->rho, s->rho_u, s->rho_w, s->rho_theta, s->rho_qv, s->rho_qc, s->rho_qr};
+        T* dv[7] = {d.rho, d.ru, d.rw, d.rt, d.qv, d.qc, d.qr};
+        for (int j = 0; j < 7; j++)
+            if ((r = put2d(f2[j], dv[j])) != MOIST_OK) return r;
+        const void* g2[6] = {s->d_rho_theta_mp, s->d_rho_qv_mp, s->d_rho_qc_mp, s->d_rho_qr_mp, s->d_rho_qr_sed,
+                             s->d_rho_theta_rd};
+        T* gv[6] = {d_th_mp, d_qv_mp, d_qc_mp, d_qr_mp, d_qr_sed, d_th_rd};
+        for (int j = 0; j < 6; j++)
+            if ((r = put2d(g2[j], gv[j])) != MOIST_OK) return r;
+        if (s->d_rho_theta_rd) rd_dirty = true;
+        const void* f1[8] = {s->prec, s->mflux, s->shflux, s->lhflux, s->d_rho_u_sf, s->d_rho_theta_sf,
+                             s->d_rho_qv_sf, nullptr};
+        T* d1[8] = {prec, mflux, shflux, lhflux, d_u_sf, d_th_sf, d_qv_sf, nullptr};
+        for (int j = 0; j < 7; j++)
+            if ((r = put1dx(f1[j], d1[j])) != MOIST_OK) return r;
+        if (s->theta_ref) CK(cudaMemcpyAsync(theta_ref, s->theta_ref, nz * sizeof(T), cudaMemcpyHostToDevice, st));
+        // halo values the surface fluxes read before the next exchange (moist.jl:723, 736)
+        if (halo >= 1) {
+            if (s->rho_u) CK(cudaMemcpyAsync(halo_vals, (const T*)s->rho_u + (size_t)(halo - 1) * nz, sizeof(T), cudaMemcpyHostToDevice, st));
+            if (s->rho) CK(cudaMemcpyAsync(halo_vals + 1, (const T*)s->rho + (size_t)(nx + halo) * nz, sizeof(T), cudaMemcpyHostToDevice, st));
+        }
+        CK(cudaStreamSynchronize(st));
+        return MOIST_OK;
+    }
+
+    int download(moist_state_host* s) override {
+        int r;
+        const void* f2[7] = {s->rho, s->rho_u, s->rho_w, s->rho_theta, s->rho_qv, s->rho_qc, s->rho_qr};
+        T* dv[7] = {cur.rho, cur.ru, cur.rw, cur.rt, cur.qv, cur.qc, cur.qr};
+        for (int j = 0; j < 7; j++) {
+            if ((r = get2d(dv[j], const_cast<void*>(f2[j]), true)) != MOIST_OK) return r;
+            CK(cudaStreamSynchronize(st));  // staging buffer reused
+        }
+        void* g2[6] = {s->d_rho_theta_mp, s->d_rho_qv_mp, s->d_rho_qc_mp, s->d_rho_qr_mp, s->d_rho_qr_sed,
+                       s->d_rho_theta_rd};
+        T* gv[6] = {d_th_mp, d_qv_mp, d_qc_mp, d_qr_mp, d_qr_sed, d_th_rd};
+        for (int j = 0; j < 6; j++) {
+            if ((r = get2d(gv[j], g2[j], false)) != MOIST_OK) return r;
+            CK(cudaStreamSynchronize(st));
+        }
+        void* f1[7] = {s->prec, s->mflux, s->shflux, s->lhflux, s->d_rho_u_sf, s->d_rho_theta_sf, s->d_rho_qv_sf};
+        T* d1[7] = {prec, mflux, shflux, lhflux, d_u_sf, d_th_sf, d_qv_sf};
+        for (int j = 0; j < 7; j++)
+            if ((r = get1dx(d1[j], f1[j])) != MOIST_OK) return r;
+        if (s->theta_ref) CK(cudaMemcpyAsync(s->theta_ref, theta_ref, nz * sizeof(T), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return MOIST_OK;
+    }
+
+    // ------------------------------------------------------------------ the large step
+    int launch_physics(int mode) {  // mode bit 1: microphysics, bit 2: sedimentation, 4: full step
+        const dim3 b(32, 8), g(cdiv(nx, 32), cdiv(nz, 8));
+        const bool full = mode & 4;
+        if (full) {
+            if (dp.do_sf) {
+                k_surface_fluxes<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, cur, halo_vals, halo_vals + 1, d_u_sf, d_th_sf,
+                                                                  d_qv_sf, mflux, shflux, lhflux, err);
+                CKL();
+            } else {
+                for (T* f : {d_u_sf, d_th_sf, d_qv_sf, mflux, shflux, lhflux})
+                    CK(cudaMemsetAsync(f, 0, P * sizeof(T), st));
+            }
+            if (dp.do_rd) {
+                k_gray_radiation<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, cur, theta_ref, lw_up, lw_dn, d_th_rd, err);
+                CKL();
+                rd_dirty = true;
+            } else if (rd_dirty) {
+                CK(cudaMemsetAsync(d_th_rd, 0, fsz * sizeof(T), st));
+                rd_dirty = false;
+            }
+        }
+        DevParams<T> q = dp;
+        if (!full) {  // the unit entry points ignore the process switches checked by rk3_step!
+            q.do_mp = 1;
+            q.do_sed = 1;
+        }
+        k_physics<T><<<g, b, 0, st>>>(q, cur, d_th_mp, d_qv_mp, d_qc_mp, d_qr_mp, d_qr_sed, d_prec, d_th_rd, d_u_sf,
+                                      d_th_sf, d_qv_sf, ph, err);
+        CKL();
+        return MOIST_OK;
+    }
+
+    int run_stage(StateP<T> s_in, StateP<T> s0, T* const qout[3], StateP<T> s_out, T dt_stage, int ns_s) {
+        const dim3 b2(32, 8), g2(cdiv(nx, 32), cdiv(nz, 8));
+        const unsigned gc = cdiv(nx, 128);
+        k_diag<T><<<g2, b2, 0, st>>>(dp, s_in, pres, theta, rt2p, uface, wface, err);
+        CKL();
+        TendArgs<T> ta_{s_in, s0, ph, pres, theta, uface, wface, R_rho, R_ru, R_rw, R_rt, rho_p, ru_p[0], rw_p,
+                        rt_p[0], mfx, mfz, halo_vals, halo_vals + 1};
+        k_tend<T><<<g2, b2, 0, st>>>(dp, ta_, err);
+        CKL();
+        const T dt_s = dt_stage / T(ns_s);
+        k_thomas_factors<T, TT><<<gc, 128, 0, st>>>(dp, theta, rt2p, dt_s, ta, tb, tc, tcp, tpiv, err);
+        CKL();
+        const double fact_tp64 = (double)T(0.5) * (1.0 + (double)dp.beta);
+        for (int n = 1; n <= ns_s; n++) {
+            SubArgs<T, TT> sa;
+            sa.R_rho = R_rho;
+            sa.R_ru = R_ru;
+            sa.R_rw = R_rw;
+            sa.R_rt = R_rt;
+            sa.theta = theta;
+            sa.rt2pres = rt2p;
+            sa.s_rw = s_in.rw;
+            sa.ru_in = ru_p[(n - 1) % 2];
+            sa.ru_out = ru_p[n % 2];
+            sa.rt_in = rt_p[(n - 1) % 3];
+            sa.rt_old = rt_p[n >= 2 ? (n - 2) % 3 : 0];
+            sa.rt_out = rt_p[n % 3];
+            sa.rho_p = rho_p;
+            sa.rw_p = rw_p;
+            sa.mfx = mfx;
+            sa.mfz = mfz;
+            sa.ta = ta;
+            sa.tb = tb;
+            sa.tc = tc;
+            sa.tcp = tcp;
+            sa.tpiv = tpiv;
+            sa.dprime = dprime;
+            k_substep<T, TT><<<gc, 128, 0, st>>>(dp, sa, dt_s, T(ns_s), fact_tp64, err);
+            CKL();
+        }
+        TracerArgs<T> tr;
+        const T* qin[3] = {s_in.qv, s_in.qc, s_in.qr};
+        const T* q0[3] = {s0.qv, s0.qc, s0.qr};
+        const T* dq[3] = {ph.d_qv, ph.d_qc, ph.d_qr};
+        for (int j = 0; j < 3; j++) {
+            tr.q_old[j] = qin[j];
+            tr.q_new[j] = qout[j];
+            tr.q0[j] = q0[j];
+            tr.dphys[j] = dq[j];
+        }
+        tr.rho = s_in.rho;
+        tr.mfx = mfx;
+        tr.mfz = mfz;
+        tr.dt = dt_stage;
+        const int nthr = (nz + 31) / 32 * 32;
+        k_tracer_wavefront<T><<<3, nthr, 3 * nz * sizeof(T), st>>>(dp, tr, err);
+        CKL();
+        UpdArgs<T> ua{s_in, s_out, rho_p, ru_p[ns_s % 2], rw_p, rt_p[ns_s % 3], ph};
+        k_update<T><<<g2, b2, 0, st>>>(dp, ua, err);
+        CKL();
+        k_stage_end<<<1, 1, 0, st>>>(err);
+        CKL();
+        return MOIST_OK;
+    }
+
+    static StateP<T> with_q(StateP<T> s, T* const q[3]) {
+        s.qv = q[0];
+        s.qc = q[1];
+        s.qr = q[2];
+        return s;
+    }
+
+    int launch_step() {
+        int r;
+        if ((r = launch_physics(4)) != MOIST_OK) return r;
+        const T dt = dp.dt;
+        const int ns1 = std::max(1, (int)std::ceil(ns / 3.0));
+        const int ns2 = std::max(1, (int)std::ceil(ns / 2.0));
+        T* const nq[3] = {nxt.qv, nxt.qc, nxt.qr};
+        if ((r = run_stage(cur, cur, nq, nxt, dt / T(3), ns1)) != MOIST_OK) return r;
+        if ((r = run_stage(nxt, cur, tmpq, with_q(nxt, tmpq), dt / T(2), ns2)) != MOIST_OK) return r;
+        if ((r = run_stage(with_q(nxt, tmpq), cur, nq, nxt, dt, ns)) != MOIST_OK) return r;
+        k_prec<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, prec, d_prec, err);
+        CKL();
+        std::swap(cur, nxt);
+        return MOIST_OK;
+    }
+
+    int check_stage_shape() {
+        if (halo != 2 || nx < 2)
+            return set_err(owner, MOIST_ERR_ARG, "the RK stages need halo = 2 and nx >= 2 (got halo = %d, nx = %d)",
+                           halo, nx);
+        return MOIST_OK;
+    }
+
+    int rk3(int nsteps) override {
+        if (int r = check_stage_shape()) return r;
+        CK(reset_err());
+        for (int n = 0; n < nsteps; n++) {
+            int r = launch_step();
+            if (r != MOIST_OK) return r;
+        }
+        return finish();
+    }
+
+    int time_steps(int nsteps, float* ms) override {
+        if (int r = check_stage_shape()) return r;
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(reset_err());
+        CK(cudaEventRecord(e0, st));
+        for (int n = 0; n < nsteps; n++) {
+            int r = launch_step();
+            if (r != MOIST_OK) return r;
+        }
+        CK(cudaEventRecord(e1, st));
+        CK(cudaEventSynchronize(e1));
+        CK(cudaEventElapsedTime(ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return finish();
+    }
+
+    int compute_step(const void* const phys[6], const moist_state_host* s0, double dt, int ns_s) override {
+        if (ns_s < 1) return set_err(owner, MOIST_ERR_ARG, "ns must be >= 1");
+        if (int r0 = check_stage_shape()) return r0;
+        int r;
+        if (!s0b.rho) {
+            for (T** f : {&s0b.rho, &s0b.ru, &s0b.rw, &s0b.rt, &s0b.qv, &s0b.qc, &s0b.qr}) AL(*f, fsz);
+        }
+        const void* f2[7] = {s0->rho, s0->rho_u, s0->rho_w, s0->rho_theta, s0->rho_qv, s0->rho_qc, s0->rho_qr};
+        T* dv[7] = {s0b.rho, s0b.ru, s0b.rw, s0b.rt, s0b.qv, s0b.qc, s0b.qr};
+        for (int j = 0; j < 7; j++) {
+            if (!f2[j]) return set_err(owner, MOIST_ERR_ARG, "s0 field %d is NULL", j);
+            if ((r = put2d(f2[j], dv[j])) != MOIST_OK) return r;
+            CK(cudaStreamSynchronize(st));
+        }
+        T* pv[6] = {ph.d_rho, ph.d_u, ph.d_th, ph.d_qv, ph.d_qc, ph.d_qr};
+        for (int j = 0; j < 6; j++) {
+            if (!phys[j]) return set_err(owner, MOIST_ERR_ARG, "phys field %d is NULL", j);
+            if ((r = put2d(phys[j], pv[j])) != MOIST_OK) return r;
+            CK(cudaStreamSynchronize(st));
+        }
+        CK(reset_err());
+        T* const nq[3] = {nxt.qv, nxt.qc, nxt.qr};
+        if ((r = run_stage(cur, s0b, nq, nxt, (T)dt, ns_s)) != MOIST_OK) return r;
+        std::swap(cur, nxt);
+        return finish();
+    }
+
+    int microphysics() override {
+        CK(reset_err());
+        int r = launch_physics(1);
+        if (r != MOIST_OK) return r;
+        return finish();
+    }
+
+    int sedimentation(void* host_d_prec) override {
+        CK(reset_err());
+        int r = launch_physics(2);
+        if (r != MOIST_OK) return r;
+        if (host_d_prec) {
+            std::vector<T> tmp(nx + 2 * halo, T(0));
+            CK(cudaMemcpyAsync(tmp.data() + halo, d_prec, nx * sizeof(T), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            std::memcpy((T*)host_d_prec + halo, tmp.data() + halo, nx * sizeof(T));
+        }
+        return finish();
+    }
+
+    int budget(double out[4]) override {
+        return set_err(owner, MOIST_ERR_UNSUPPORTED, "budget not available yet");
+    }
+};
+
+// device helper evaluation and single-column implicit correction (unit-test entry points)
+template <class T>
+__global__ void k_eval_helper(DevParams<T> p, int helper, int n, const double* in, double* out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    switch (helper) {
+        case MOIST_HELPER_F2H:
+            out[j] = (double)f2h((T)in[4 * j], (T)in[4 * j + 1], (T)in[4 * j + 2], (T)in[4 * j + 3]);
+            break;
+        case MOIST_HELPER_KOREN:
+            out[j] = (double)koren((T)in[j]);
+            break;
+        case MOIST_HELPER_SAT_VP: {
+            T es, d;
+            sat_vp((T)in[j], p, es, d);
+            out[2 * j] = es;
+            out[2 * j + 1] = d;
+            break;
+        }
+        case MOIST_HELPER_SAT_Q: {
+            T q, d;
+            sat_q((T)in[2 * j], (T)in[2 * j + 1], p, q, d);
+            out[2 * j] = q;
+            out[2 * j + 1] = d;
+            break;
+        }
+        case MOIST_HELPER_EXP:
+            out[j] = (double)mm::mexp((T)in[j]);
+            break;
+        case MOIST_HELPER_POW:
+            out[j] = (double)mm::mpow((T)in[2 * j], (T)in[2 * j + 1]);
+            break;
+    }
+}
+
+// implicit_correction! for one column: the per-stage factorisation followed by one substep's
+// right-hand side, elimination and back substitution, exactly as k_thomas_factors + k_substep
+template <class T, class TT>
+__global__ void k_implicit_column(DevParams<T> p, T* rho_w, const T* drho_w, const T* theta, const T* rt2pres,
+                                  T dt) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int nz = p.nz, n = nz - 1, ke = nz - 1;
+    const T* dz = p.dz;
+    const T* z = p.z;
+    const T fact_tp = T(0.5) * (T(1.0) + p.beta);
+    const T fact_tm = T(0.5) * (T(1.0) - p.beta);
+    const T dt_tp2 = (dt * fact_tp) * (dt * fact_tp);
+    const T fact = fact_tm / fact_tp;
+    TT cp_prev = TT(0), d_prev = TT(0);
+    extern __shared__ unsigned char sm[];
+    TT* cps = reinterpret_cast<TT*>(sm);
+    TT* dps = cps + n;
+    for (int j = 0; j < n; j++) {
+        const int k = j;
+        const T th_cur = f2h(theta[k], theta[k + 1], dz[k], dz[k + 1]);
+        const T th_prev = k > 0 ? f2h(theta[k - 1], theta[k], dz[k - 1], dz[k]) : T(0);
+        const T th_next = (k + 1 <= ke - 1) ? f2h(theta[k + 1], theta[k + 2], dz[k + 1], dz[k + 2]) : T(0);
+        const T b = dt_tp2 * (rt2pres[k] / dz[k] + rt2pres[k + 1] / dz[k + 1]) * th_cur / (z[k + 1] - z[k]);
+        const T a = (k > 0) ? -dt_tp2 * (rt2pres[k] * th_prev / ((z[k + 1] - z[k]) * dz[k]) - p.GRAV / (dz[k] + dz[k + 1])) : T(0);
+        const T c = (k < ke - 1) ? -dt_tp2 * (rt2pres[k + 1] * th_next / ((z[k + 1] - z[k]) * dz[k + 1]) + p.GRAV / (dz[k] + dz[k + 1])) : T(0);
+        T d = rho_w[k] + drho_w[k];
+        if (k > 0) d -= a * fact * rho_w[k];
+        d -= b * fact * rho_w[k];
+        const T bb = b + T(1.0);
+        if (k < ke - 1) d -= c * fact * rho_w[k + 1];
+        TT piv, cpj, dpj;
+        if (j == 0) {
+            piv = (TT)bb;
+            cpj = (TT)c / piv;
+            dpj = (TT)d / piv;
+        } else {
+            piv = (TT)bb - (TT)a * cp_prev;
+            cpj = (TT)c / piv;
+            dpj = ((TT)d - (TT)a * d_prev) / piv;
+        }
+        cps[j] = cpj;
+        dps[j] = dpj;
+        cp_prev = cpj;
+        d_prev = dpj;
+    }
+    TT x = dps[n - 1];
+    rho_w[n - 1] = (T)x;
+    for (int j = n - 2; j >= 0; j--) {
+        x = dps[j] - cps[j] * x;
+        rho_w[j] = (T)x;
+    }
+}
+
+template <class T>
+int eval_helper_t(const moist_params* c, int helper, int n, const double* in, double* out) {
+    moist_ctx* owner = nullptr;
+    DevParams<T> p = make_params<T>(c, 0);
+    int nin = (helper == MOIST_HELPER_F2H) ? 4 : (helper == MOIST_HELPER_SAT_Q || helper == MOIST_HELPER_POW) ? 2 : 1;
+    int nout = (helper == MOIST_HELPER_SAT_VP || helper == MOIST_HELPER_SAT_Q) ? 2 : 1;
+    if (helper < 0 || helper > MOIST_HELPER_POW) return MOIST_ERR_ARG;
+    double *din = nullptr, *dout = nullptr;
+    CK(cudaMalloc(&din, std::max(1, n * nin) * sizeof(double)));
+    CK(cudaMalloc(&dout, std::max(1, n * nout) * sizeof(double)));
+    CK(cudaMemcpy(din, in, n * nin * sizeof(double), cudaMemcpyHostToDevice));
+    if (n > 0) k_eval_helper<T><<<cdiv(n, 128), 128>>>(p, helper, n, din, dout);
+    CKL();
+    CK(cudaMemcpy(out, dout, n * nout * sizeof(double), cudaMemcpyDeviceToHost));
+    cudaFree(din);
+    cudaFree(dout);
+    return MOIST_OK;
+}
+
+template <class T, class TT>
+int implicit_t(const moist_params* c, void* rho_w, const void* drho_w, const void* theta, const void* rt2pres,
+               double dt) {
+    moist_ctx* owner = nullptr;
+    const int nz = c->nz;
+    DevParams<T> p = make_params<T>(c, 0);
+    T* buf = nullptr;
+    CK(cudaMalloc(&buf, 6 * nz * sizeof(T)));
+    T *w = buf, *dw = buf + nz, *th = buf + 2 * nz, *r2 = buf + 3 * nz, *gdz = buf + 4 * nz, *gz = buf + 5 * nz;
+    CK(cudaMemcpy(w, rho_w, nz * sizeof(T), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dw, drho_w, nz * sizeof(T), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(th, theta, nz * sizeof(T), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(r2, rt2pres, nz * sizeof(T), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(gdz, c->dz, nz * sizeof(T), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(gz, c->z, nz * sizeof(T), cudaMemcpyHostToDevice));
+    p.dz = gdz;
+    p.z = gz;
+    k_implicit_column<T, TT><<<1, 32, 2 * nz * sizeof(TT)>>>(p, w, dw, th, r2, (T)dt);
+    CKL();
+    CK(cudaMemcpy(rho_w, w, nz * sizeof(T), cudaMemcpyDeviceToHost));
+    cudaFree(buf);
+    return MOIST_OK;
+}
+
+}  // namespace
+
+// ============================================================================ C-ABI
+
+extern "C" {
+#pragma GCC visibility push(default)
+
+int moist_abi_version(void) { return MOIST2D_ABI_VERSION; }
+
+const char* moist_status_string(int s) {
+    switch (s) {
+        case MOIST_OK: return "ok";
+        case MOIST_ERR_NAN: return "NaN detected";
+        case MOIST_ERR_ARG: return "invalid argument";
+        case MOIST_ERR_CUDA: return "CUDA error";
+        case MOIST_ERR_TIMEOUT: return "device wait timed out";
+        case MOIST_ERR_UNSUPPORTED: return "unsupported";
+        case MOIST_ERR_NOMEM: return "out of device memory";
+        default: return "unknown status";
+    }
+}
+
+int moist_ctx_create(const moist_params* p, int precision, int flags, moist_ctx** out) {
+    if (!out) return MOIST_ERR_ARG;
+    *out = nullptr;
+    if (!p || !p->zf || !p->dz || !p->z) return MOIST_ERR_ARG;
+    // any halo / nx >= 1 is accepted for the physics entry points (the reference's own
+    // microphysics testset uses halo = 0, Nx = 1); the RK stages need halo = 2 and nx >= 2
+    if (p->nx < 1 || p->nz < 2 || p->halo < 0 || p->ns < 1 || p->nz > 1024) return MOIST_ERR_ARG;
+    if (precision != MOIST_F32 && precision != MOIST_F64) return MOIST_ERR_ARG;
+    moist_ctx* c = new moist_ctx();
+    c->precision = precision;
+    c->flags = flags;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return MOIST_ERR_CUDA;
+    }
+    int r;
+    if (precision == MOIST_F64) {
+        auto* x = new Ctx<double, double>(c);
+        c->impl = x;
+        r = x->init(p);
+    } else if (flags & MOIST_FLAG_TRI_NATIVE) {
+        auto* x = new Ctx<float, float>(c);
+        c->impl = x;
+        r = x->init(p);
+    } else {
+        auto* x = new Ctx<float, double>(c);
+        c->impl = x;
+        r = x->init(p);
+    }
+    if (r != MOIST_OK) {
+        delete c->impl;
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return r;
+    }
+    *out = c;
+    return MOIST_OK;
+}
+
+int moist_ctx_destroy(moist_ctx* c) {
+    if (!c) return MOIST_ERR_ARG;
+    delete c->impl;
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return MOIST_OK;
+}
+
+const char* moist_last_error(const moist_ctx* c) { return c ? c->err.c_str() : "null context"; }
+int moist_nan_field(const moist_ctx* c) { return c ? c->nan_field : -1; }
+
+int moist_upload_state(moist_ctx* c, const moist_state_host* s) {
+    if (!c || !s) return MOIST_ERR_ARG;
+    return c->impl->upload(s);
+}
+int moist_download_state(moist_ctx* c, moist_state_host* s) {
+    if (!c || !s) return MOIST_ERR_ARG;
+    return c->impl->download(s);
+}
+int moist_rk3_step(moist_ctx* c, int nsteps) {
+    if (!c || nsteps < 0) return MOIST_ERR_ARG;
+    return c->impl->rk3(nsteps);
+}
+int moist_compute_step(moist_ctx* c, const void* const phys[6], const moist_state_host* s0, double dt, int ns) {
+    if (!c || !phys || !s0) return MOIST_ERR_ARG;
+    return c->impl->compute_step(phys, s0, dt, ns);
+}
+int moist_cloud_microphysics(moist_ctx* c) {
+    if (!c) return MOIST_ERR_ARG;
+    return c->impl->microphysics();
+}
+int moist_rain_sedimentation(moist_ctx* c, void* d_prec) {
+    if (!c) return MOIST_ERR_ARG;
+    return c->impl->sedimentation(d_prec);
+}
+int moist_budget(moist_ctx* c, double out[4]) {
+    if (!c || !out) return MOIST_ERR_ARG;
+    return c->impl->budget(out);
+}
+void* moist_stream(moist_ctx* c) { return c ? (void*)c->stream : nullptr; }
+int moist_synchronize(moist_ctx* c) {
+    if (!c) return MOIST_ERR_ARG;
+    return cudaStreamSynchronize(c->stream) == cudaSuccess ? MOIST_OK : MOIST_ERR_CUDA;
+}
+int moist_time_steps(moist_ctx* c, int nsteps, float* ms) {
+    if (!c || !ms || nsteps < 0) return MOIST_ERR_ARG;
+    return c->impl->time_steps(nsteps, ms);
+}
+
+int moist_implicit_correction(const moist_params* p, int precision, int flags, void* rho_w, const void* drho_w,
+                              const void* theta, const void* rt2pres, double dt) {
+    if (!p || !p->dz || !p->z || p->nz < 2 || !rho_w || !drho_w || !theta || !rt2pres) return MOIST_ERR_ARG;
+    if (precision == MOIST_F64) return implicit_t<double, double>(p, rho_w, drho_w, theta, rt2pres, dt);
+    if (flags & MOIST_FLAG_TRI_NATIVE) return implicit_t<float, float>(p, rho_w, drho_w, theta, rt2pres, dt);
+    return implicit_t<float, double>(p, rho_w, drho_w, theta, rt2pres, dt);
+}
+
+int moist_eval_helper(const moist_params* p, int precision, int helper, int n, const double* in, double* out) {
+    if (!p || n < 0 || (n > 0 && (!in || !out))) return MOIST_ERR_ARG;
+    return precision == MOIST_F64 ? eval_helper_t<double>(p, helper, n, in, out)
+                                  : eval_helper_t<float>(p, helper, n, in, out);
+}
+
+}  // extern "C"

@@ -1,0 +1,159 @@
+"""Reference-shaped host API over the CUDA library.
+
+The functions mirror moist.jl's entry points (same names, argument meaning and in-place
+semantics): `rk3_step(s, p)` (moist.jl:1589), `compute_step(phys, s, s0, p, dt, ns)` (1039),
+`cloud_microphysics(s, p)` (554), `rain_sedimentation(s, p)` (674),
+`implicit_correction(rho_w, drho_w, theta, rt2pres, dt, p)` (974). A NaN found by the
+end-of-stage check raises FloatingPointError("NaN detected in <field>"), the counterpart of the
+reference's error(...) (moist.jl:1543-1577).
+
+`Model` keeps a State resident on the device between calls (the reference's device() hook,
+moist.jl:227-228): upload once, step many times, download when needed.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from ._lib import lib
+
+
+def _raise(rc, ctx=None, what=""):
+    if rc == abi.MOIST_OK:
+        return
+    L = lib()
+    msg = L.moist_last_error(ctx).decode() if ctx else L.moist_status_string(rc).decode()
+    if rc == abi.MOIST_ERR_NAN:
+        raise FloatingPointError(msg)
+    if rc == abi.MOIST_ERR_ARG:
+        raise ValueError("%s: invalid argument %s" % (what, msg))
+    if rc == abi.MOIST_ERR_UNSUPPORTED:
+        raise NotImplementedError("%s: %s" % (what, msg))
+    raise RuntimeError("%s failed (%s): %s" % (what, L.moist_status_string(rc).decode(), msg))
+
+
+class Model:
+    """A device-resident State with its Params (one CUDA stream)."""
+
+    def __init__(self, p, flags=0):
+        self.p = p
+        self._cp = p.to_c()
+        self.flags = flags
+        self.ctx = C.c_void_p()
+        _raise(lib().moist_ctx_create(C.byref(self._cp), p.precision, flags, C.byref(self.ctx)),
+               None, "moist_ctx_create")
+
+    def close(self):
+        if self.ctx:
+            lib().moist_ctx_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload(self, s):
+        h = s.to_c()
+        _raise(lib().moist_upload_state(self.ctx, C.byref(h)), self.ctx, "moist_upload_state")
+
+    def download(self, s):
+        h = s.to_c()
+        _raise(lib().moist_download_state(self.ctx, C.byref(h)), self.ctx, "moist_download_state")
+        return s
+
+    def step(self, nsteps=1):
+        _raise(lib().moist_rk3_step(self.ctx, int(nsteps)), self.ctx, "moist_rk3_step")
+
+    def time_steps(self, nsteps):
+        ms = C.c_float()
+        _raise(lib().moist_time_steps(self.ctx, int(nsteps), C.byref(ms)), self.ctx, "moist_time_steps")
+        return ms.value
+
+    def budget(self):
+        out = (C.c_double * 4)()
+        _raise(lib().moist_budget(self.ctx, out), self.ctx, "moist_budget")
+        return np.array(out[:])
+
+    def synchronize(self):
+        _raise(lib().moist_synchronize(self.ctx), self.ctx, "moist_synchronize")
+
+    @property
+    def nan_field(self):
+        return lib().moist_nan_field(self.ctx)
+
+
+def rk3_step(s, p, nsteps=1, flags=0):
+    """rk3_step!(s, p) applied nsteps times; s is updated in place."""
+    with Model(p, flags) as m:
+        m.upload(s)
+        try:
+            m.step(nsteps)
+        finally:
+            m.download(s)
+    return s
+
+
+def compute_step(phys, s, s0, p, dt, ns, flags=0):
+    """compute_step!(phys..., s, s0, p, dt, ns); phys = six (ka, ia) arrays in the reference order."""
+    keep = [np.asfortranarray(a, dtype=p.T) for a in phys]
+    arr = (C.c_void_p * 6)(*[a.ctypes.data for a in keep])
+    h0 = s0.to_c()
+    with Model(p, flags) as m:
+        m.upload(s)
+        try:
+            _raise(lib().moist_compute_step(m.ctx, arr, C.byref(h0), float(dt), int(ns)), m.ctx,
+                   "moist_compute_step")
+        finally:
+            m.download(s)
+    return s
+
+
+def cloud_microphysics(s, p):
+    """cloud_microphysics!(d_rho_qv_mp, ..., rho, ..., p): fills s.d_rho_*_mp."""
+    with Model(p) as m:
+        m.upload(s)
+        _raise(lib().moist_cloud_microphysics(m.ctx), m.ctx, "moist_cloud_microphysics")
+        m.download(s)
+    return s
+
+
+def rain_sedimentation(s, p):
+    """rain_sedimentation!(d_rho_qr_sed, d_prec, rho_qr, rho, p): fills s.d_rho_qr_sed and
+    returns d_prec."""
+    d_prec = np.zeros(p.ia, dtype=p.T)
+    with Model(p) as m:
+        m.upload(s)
+        _raise(lib().moist_rain_sedimentation(m.ctx, d_prec.ctypes.data), m.ctx,
+               "moist_rain_sedimentation")
+        m.download(s)
+    return d_prec
+
+
+def implicit_correction(rho_w, drho_w, theta, rt2pres, dt, p, flags=0):
+    cp = p.to_c()
+    for a in (rho_w, drho_w, theta, rt2pres):
+        assert a.dtype == p.T and a.flags["C_CONTIGUOUS"]
+    _raise(lib().moist_implicit_correction(C.byref(cp), p.precision, flags, rho_w.ctypes.data,
+                                           drho_w.ctypes.data, theta.ctypes.data,
+                                           rt2pres.ctypes.data, float(dt)), None,
+           "moist_implicit_correction")
+
+
+def eval_helper(p, helper, inputs, nout):
+    cp = p.to_c()
+    x = np.ascontiguousarray(inputs, dtype=np.float64)
+    n = x.shape[0]
+    out = np.zeros(n * nout, dtype=np.float64)
+    _raise(lib().moist_eval_helper(C.byref(cp), p.precision, helper, n,
+                                   x.ctypes.data_as(C.POINTER(C.c_double)),
+                                   out.ctypes.data_as(C.POINTER(C.c_double))), None,
+           "moist_eval_helper")
+    return out.reshape(n, nout) if nout > 1 else out

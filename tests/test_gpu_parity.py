@@ -1,0 +1,125 @@
+"""GPU parity: the CUDA library against the CPU oracle through the C-ABI.
+
+The kernels and the oracle evaluate the same expressions in the same order with the same
+scalar math and no contraction, so results are compared bit for bit (all interior cells of
+all prognostic fields and the accumulated rain) in Float32 (FP64 and native Thomas
+elimination) and Float64."""
+import numpy as np
+import pytest
+
+from moist2d_b200 import abi, model
+from moist2d_b200.params import Params, State
+from oracle import bind
+
+import refsets
+from impls import GpuImpl
+from states import bubble_case, compare, small_case
+
+pytestmark = pytest.mark.gpu
+
+MODES = [(np.float32, False), (np.float32, True), (np.float64, False)]
+MODE_IDS = ["f32-tri64", "f32-tri32", "f64"]
+
+
+def _flags(tri_native):
+    return abi.MOIST_FLAG_TRI_NATIVE if tri_native else 0
+
+
+def _tri64(T, tri_native):
+    return T is np.float64 or not tri_native
+
+
+@pytest.mark.parametrize("testset", refsets.DEVICE_SETS, ids=[f.__name__[2:] for f in refsets.DEVICE_SETS])
+@pytest.mark.parametrize("tri_native", [False, True], ids=["tri64", "tri_native"])
+def test_reference_testset_gpu(testset, tri_native, FT):
+    testset(GpuImpl(tri_native=tri_native), FT)
+
+
+@pytest.mark.parametrize("T,tri_native", MODES, ids=MODE_IDS)
+def test_microphysics_bitwise(T, tri_native):
+    p, s = bubble_case(T)
+    a, b = s.copy(), s.copy()
+    model.cloud_microphysics(a, p)
+    bind.cloud_microphysics(b, p)
+    compare(a, b, p, fields=("d_rho_theta_mp", "d_rho_qv_mp", "d_rho_qc_mp", "d_rho_qr_mp"))
+    assert np.any(b.d_rho_qr_mp != 0) and np.any(b.d_rho_qc_mp != 0)
+
+
+@pytest.mark.parametrize("T,tri_native", MODES, ids=MODE_IDS)
+def test_sedimentation_bitwise(T, tri_native):
+    p, s = bubble_case(T)
+    a, b = s.copy(), s.copy()
+    da = model.rain_sedimentation(a, p)
+    db = bind.rain_sedimentation(b, p)
+    compare(a, b, p, fields=("d_rho_qr_sed",))
+    is0, ie0 = p.is_ - 1, p.ie
+    assert np.array_equal(da[is0:ie0], db[is0:ie0])
+
+
+@pytest.mark.parametrize("T,tri_native", MODES, ids=MODE_IDS)
+def test_compute_step_bitwise(T, tri_native):
+    p, s0 = bubble_case(T, seed=9)
+    p2, s = bubble_case(T, seed=10)  # a different current state: nonzero perturbations
+    rng = np.random.default_rng(3)
+    phys = [np.asfortranarray((rng.standard_normal((p.ka, p.ia)) * sc).astype(T))
+            for sc in (1e-5, 1e-4, 1e-3, 1e-6, 1e-6, 1e-6)]
+    a, b = s.copy(), s.copy()
+    model.compute_step(phys, a, s0, p, p.dt / T(2), 4, flags=_flags(tri_native))
+    bind.compute_step(phys, b, s0, p, p.dt / T(2), 4, tri64=_tri64(T, tri_native))
+    compare(a, b, p, fields=("rho", "rho_u", "rho_w", "rho_theta", "rho_qv", "rho_qc", "rho_qr"))
+
+
+@pytest.mark.parametrize("T,tri_native", MODES, ids=MODE_IDS)
+@pytest.mark.parametrize("nsteps", [1, 5])
+def test_rk3_bitwise_bubble(T, tri_native, nsteps):
+    p, s = bubble_case(T)
+    a, b = s.copy(), s.copy()
+    model.rk3_step(a, p, nsteps, flags=_flags(tri_native))
+    bind.rk3_step(b, p, nsteps, tri64=_tri64(T, tri_native))
+    compare(a, b, p, fields=("rho", "rho_u", "rho_w", "rho_theta", "rho_qv", "rho_qc", "rho_qr", "prec",
+                             "d_rho_qr_sed", "d_rho_theta_mp"))
+
+
+@pytest.mark.parametrize("T,tri_native", MODES, ids=MODE_IDS)
+@pytest.mark.parametrize("nx,nz", [(2, 2), (3, 3), (4, 4), (5, 2), (2, 5), (7, 6), (33, 9)])
+def test_rk3_bitwise_small_shapes(T, tri_native, nx, nz):
+    p, s = small_case(T, nx, nz, do_sf=False, do_rd=False)
+    a, b = s.copy(), s.copy()
+    model.rk3_step(a, p, 3, flags=_flags(tri_native))
+    bind.rk3_step(b, p, 3, tri64=_tri64(T, tri_native))
+    compare(a, b, p)
+
+
+@pytest.mark.parametrize("T,tri_native", MODES, ids=MODE_IDS)
+def test_rk3_bitwise_surface_flux_and_radiation(T, tri_native):
+    """Default Params: surface fluxes and gray radiation on, 4 steps (the stale halo values the
+    surface fluxes read are tracked across steps)."""
+    p, s = small_case(T, 6, 8)
+    assert p.do_sf and p.do_rd
+    a, b = s.copy(), s.copy()
+    model.rk3_step(a, p, 4, flags=_flags(tri_native))
+    bind.rk3_step(b, p, 4, tri64=_tri64(T, tri_native))
+    compare(a, b, p, fields=("rho", "rho_u", "rho_w", "rho_theta", "rho_qv", "rho_qc", "rho_qr", "prec",
+                             "mflux", "shflux", "lhflux", "d_rho_theta_rd"))
+
+
+@pytest.mark.parametrize("T", [np.float32, np.float64])
+def test_nan_is_reported_like_the_reference(T):
+    p, s = small_case(T, 4, 4, do_sf=False, do_rd=False)
+    s.rho_qv[1, p.is_] = np.nan  # a NaN written into the uploaded state (host-side injection)
+    a, b = s.copy(), s.copy()
+    with pytest.raises(FloatingPointError) as eg:
+        model.rk3_step(a, p, 2)
+    with pytest.raises(FloatingPointError) as eo:
+        bind.rk3_step(b, p, 2)
+    assert str(eg.value) == str(eo.value)
+
+
+def test_invalid_params_rejected():
+    p = Params(np.float32, Nx=4, Nz=4, H=430.0, dz0=100.0, z_fact=1.05, halo=1)
+    with pytest.raises(ValueError):
+        model.rk3_step(State(p), p)
+    p = Params(np.float32, Nx=1, Nz=4, H=430.0, dz0=100.0, z_fact=1.05)
+    s = State(p)
+    with pytest.raises(ValueError):
+        model.rk3_step(s, p)
