@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark of the large time step (rk3_step!) on B200: cell-steps/s.
+
+One step = one large step (rk3_step!, moist.jl:1589) of the whole domain; one cell-step = one
+interior cell advanced by one large step. Default workload: the 2048 x 128 analytic-sounding
+domain with five seeded warm bubbles (dx = 250 m, dz = 125 m, dt = 2 s, ns = 8), Float32
+state with FP64 w-p elimination, synthetic seeded input.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload plain|bubble] [--precision f32|f64]
+
+value:  device time of K steps (CUDA events on the context stream, L2 flushed by a 256 MiB
+        write before every timed step), max over ranks, cells x K x N / time.
+e2e:    the same metric through the reference-facing call rk3_step!(s, p) on a host State
+        (moist_rk3_step_host: upload, step, download every step, page-locked host arrays),
+        wall clock around each call.
+roofline: the kernel group with the largest device time; achieved = its algorithmic bytes per
+        launch (words per cell below x cells) / its mean launch time from the same events.
+Multi-GPU: independent replicas (the domain does not shard; ensemble members would).
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-steps/s on 1 B200: batched/adjoint vs plain fwd at FP64-tol; HBM % of peak"
+
+# algorithmic words per cell per launch of each kernel group (1 word = sizeof(T)): the unique
+# inter-phase field traffic of the reference algorithm, W(ns) = 10 + sum_stages(50 + 20 m_s)
+GROUPS = ("physics", "prologue", "substep", "tracer", "update", "other")
+WORDS = {"physics": 10, "prologue": 23, "substep": 20, "tracer": 16, "update": 11, "other": 0}
+
+
+def words_per_cell_step(ns):
+    ms = (max(1, -(-ns // 3)), max(1, -(-ns // 2)), ns)
+    return 10 + sum(50 + 20 * m for m in ms)
+
+
+def group_instances(ns):
+    """Launch instances of each group per large step."""
+    ms = (max(1, -(-ns // 3)), max(1, -(-ns // 2)), ns)
+    return {"physics": 1, "prologue": 3, "substep": sum(ms), "tracer": 3, "update": 3, "other": 1}
+
+
+def make_workload(name, T):
+    from moist2d_b200.init import sounding_bubbles, warm_bubble
+    if name == "plain":
+        p, s = sounding_bubbles(T)
+        desc = ("plain forward, 2048x128 cells (dx=250 m, dz=125 m), analytic sounding + 5 seeded "
+                "warm bubbles, dt=2 s, ns=8")
+    elif name == "bubble":
+        p, s = warm_bubble(T)
+        desc = "warm moist bubble, 200x100 cells of 100 m, dt=1 s, ns=6"
+    else:
+        raise SystemExit("unknown workload " + name)
+    return p, s, desc
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(workload, precision):
+    """DRAM bytes per launch of each kernel group from a committed ncu capture, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        d = json.load(f)
+    return d.get("%s-%s" % (workload, precision), {})
+
+
+class Clocks:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(workload, T, budget_s=12.0, max_steps=40):
+    """The oracle's threaded build timed on the host cores on a bounded sample of the workload."""
+    from oracle import bind  # noqa: F401  (builds the oracle if needed)
+    so = os.path.join(ROOT, "oracle", "libmoist_oracle_omp.so")
+    if not os.path.exists(so):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    L = C.CDLL(so)
+    p, s, _ = make_workload(workload, T)
+    cp = p.to_c()
+    h = s.to_c()
+    cells = p.Nx * p.Nz
+    L.oracle_rk3_step(C.byref(cp), p.precision, 1, C.byref(h), 1)  # warm-up step
+    n, t0 = 0, time.perf_counter()
+    while n < max_steps and time.perf_counter() - t0 < budget_s:
+        L.oracle_rk3_step(C.byref(cp), p.precision, 1, C.byref(h), 1)
+        n += 1
+    dt = time.perf_counter() - t0
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": cells * n / dt, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+            "sample": "%d large steps of the %dx%d domain after 1 warm-up step (%.1f s), threaded "
+                      "C++ restatement of rk3_step! (OpenMP over columns)" % (n, p.Nx, p.Nz, dt)}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's CPU path (no Julia here: the threaded oracle port)."""
+    if rank != 0:
+        return
+    T = np.float32 if args.precision == "f32" else np.float64
+    from oracle import bind  # noqa: F401
+    so = os.path.join(ROOT, "oracle", "libmoist_oracle_omp.so")
+    if not os.path.exists(so):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    L = C.CDLL(so)
+    p, s, desc = make_workload(args.workload, T)
+    cp = p.to_c()
+    h = s.to_c()
+    cells = p.Nx * p.Nz
+    for _ in range(args.warmup):
+        L.oracle_rk3_step(C.byref(cp), p.precision, 1, C.byref(h), 1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        L.oracle_rk3_step(C.byref(cp), p.precision, 1, C.byref(h), 1)
+    dt = time.perf_counter() - t0
+    value = cells * args.steps / dt
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "cell-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+            "config": {"workload": desc, "cells": cells,
+                       "reference": "Julia moist.jl is not runnable here (no Julia toolchain); "
+                                    "its CPU path is timed as the threaded C++ restatement"},
+            "cpu_baseline": {"value": value, "unit": "cell-steps/s", "kind": "port", "cores": cores,
+                             "sample": "%d timed large steps of the full domain after %d warm-up "
+                                       "steps" % (args.steps, args.warmup)},
+            "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--workload", default="plain", choices=("plain", "bubble"))
+    ap.add_argument("--precision", default="f32", choices=("f32", "f64"))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end measurement")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    from moist2d_b200 import _lib, abi
+    from moist2d_b200.model import Model, _raise
+    L = _lib.lib()
+    _raise(L.moist_set_device(local_rank), None, "moist_set_device")
+
+    T = np.float32 if args.precision == "f32" else np.float64
+    p, s, desc = make_workload(args.workload, T)
+    cells = p.Nx * p.Nz
+    bpw = np.dtype(T).itemsize
+    m = Model(p)
+    m.upload(s)
+    ext = torch.cuda.ExternalStream(L.moist_stream(m.ctx), device=torch.device("cuda", local_rank))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    total = C.c_float()
+    gms = (C.c_float * abi.MOIST_NGROUPS)()
+    gl = (C.c_longlong * abi.MOIST_NGROUPS)()
+
+    for _ in range(args.warmup):
+        _raise(L.moist_step_profile(m.ctx, 1, C.byref(total), gms, gl), m.ctx, "warm-up step")
+
+    clocks = Clocks(local_rank)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    step_ms = 0.0
+    group_ms = np.zeros(abi.MOIST_NGROUPS)
+    launches = np.zeros(abi.MOIST_NGROUPS, dtype=np.int64)
+    for _ in range(args.steps):
+        with torch.cuda.stream(ext):
+            flush.zero_()  # evict L2 (126 MB) before the step
+        _raise(L.moist_step_profile(m.ctx, 1, C.byref(total), gms, gl), m.ctx, "timed step")
+        step_ms += total.value
+        group_ms += np.array(gms[:])
+        launches += np.array(gl[:])
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+
+    t_local = step_ms / args.steps
+    if world > 1:
+        t = torch.tensor([t_local], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    else:
+        t_max = t_local
+    value = cells * world / (t_max / 1e3)
+
+    # end to end: rk3_step!(s, p) on a page-locked host State, every step
+    e2e = None
+    if not args.no_e2e:
+        ia, ka = p.ia, p.ka
+        fields = ("rho", "rho_u", "rho_w", "rho_theta", "rho_qv", "rho_qc", "rho_qr")
+        tdt = torch.float32 if T is np.float32 else torch.float64
+        pinned = {}
+        for f in fields:
+            a = torch.empty((ia, ka), dtype=tdt, pin_memory=True).numpy().T  # (ka, ia) column-major
+            a[...] = getattr(s, f)
+            pinned[f] = a
+        prec = torch.zeros(ia, dtype=tdt, pin_memory=True).numpy()
+        h = abi.moist_state_host()
+        for f in fields:
+            setattr(h, f, pinned[f].ctypes.data)
+        h.prec = prec.ctypes.data
+        nbytes = (len(fields) * ka * ia + ia) * bpw
+        for _ in range(2):
+            _raise(L.moist_rk3_step_host(m.ctx, C.byref(h), 1), m.ctx, "e2e warm-up")
+        ne2e = max(3, args.steps // 2)
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(ne2e):
+            _raise(L.moist_rk3_step_host(m.ctx, C.byref(h), 1), m.ctx, "e2e step")
+        te = (time.perf_counter() - t0) / ne2e
+        if world > 1:
+            tt = torch.tensor([te], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        e2e = {"value": cells * world / te, "unit": "cell-steps/s", "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "ms_per_step": te * 1e3,
+               "how": "moist_rk3_step_host: H2D of the 7 prognostic fields + prec from page-locked "
+                      "memory, one rk3 step, D2H of the same, wall clock per call"}
+
+    # roofline of the dominant kernel group, from the events of the timed region
+    inst = group_instances(p.ns)
+    gnames = GROUPS
+    gi = int(np.argmax(group_ms))
+    gname = gnames[gi]
+    n_inst = inst[gname] * args.steps
+    mean_ms = group_ms[gi] / n_inst
+    alg_bytes = WORDS[gname] * bpw * cells
+    achieved = alg_bytes / (mean_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic(args.workload, args.precision).get(gname)
+    roofline = {"bound": "hbm", "kernel": gname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "algorithmic_bytes_per_launch": alg_bytes, "mean_launch_ms": mean_ms,
+                "peak_kind": peak_kind,
+                "step_frac": cells * words_per_cell_step(p.ns) * bpw / (t_max / 1e3) / 1e9 / peak}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline(args.workload, T)
+        except Exception as e:  # a baseline failure must not hide the GPU number
+            cpu = {"value": None, "error": str(e)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": args.precision, "data": "synthetic",
+            "config": {"workload": desc, "cells": cells, "precision": args.precision +
+                       (" state, fp64 w-p elimination" if args.precision == "f32" else ""),
+                       "l2": "flushed before every timed step (256 MiB write)",
+                       "parallelism": "replicas" if world > 1 else "single domain",
+                       "words_per_cell_step": words_per_cell_step(p.ns)},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches.sum()),
+            "kernel_ms_per_step": {g: float(group_ms[j] / args.steps) for j, g in enumerate(gnames)},
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+
+    m.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -139,6 +139,11 @@ typedef struct moist_ctx moist_ctx;
 int moist_abi_version(void);
 const char* moist_status_string(int status);
 
+/* Select the CUDA device on which this host thread creates contexts (cudaSetDevice in the
+ * library's runtime; the default is device 0). A context remembers its device and makes it
+ * current at each of its entry points. */
+int moist_set_device(int device);
+
 /* Context = one device-resident State plus Params (replaces device(), moist.jl:227-228).
  * Fails with MOIST_ERR_ARG for nx < 1, nz < 2 (or > 1024), halo < 0, ns < 1 or a NULL grid
  * vector. The RK-stage entry points (rk3_step, compute_step, time_steps) further need
@@ -157,6 +162,12 @@ int moist_download_state(moist_ctx* ctx, moist_state_host* s);
 
 /* rk3_step!(s, p) applied nsteps times (moist.jl:1589-1683). */
 int moist_rk3_step(moist_ctx* ctx, int nsteps);
+
+/* rk3_step!(s, p) on a host State, the reference's calling convention (moist.jl:1589): copy s
+ * to the device, apply nsteps large steps, copy the State back into s. Equivalent to
+ * moist_upload_state + moist_rk3_step + moist_download_state with one synchronisation. Host
+ * arrays in page-locked memory let the copies run at full bus speed. */
+int moist_rk3_step_host(moist_ctx* ctx, moist_state_host* s, int nsteps);
 
 /* compute_step!(d_rho_phys, d_rho_u_phys, d_rho_theta_phys, d_rho_qv_phys, d_rho_qc_phys,
  * d_rho_qr_phys, s, s0, p, dt, ns) (moist.jl:1039-1580): one RK stage on the context state s,
@@ -199,6 +210,23 @@ int moist_eval_helper(const moist_params* p, int precision, int helper, int n, c
  * out[2] = total energy (kinetic + potential + internal, the terms of moist.jl:1839-1852)*dx*dz,
  * out[3] = accumulated surface rain sum(prec*dx). */
 int moist_budget(moist_ctx* ctx, double out[4]);
+
+/* Kernel groups of one large step, for moist_step_profile. */
+enum {
+    MOIST_KGROUP_PHYSICS = 0,   /* surface fluxes, radiation, Kessler + sedimentation + phys assembly */
+    MOIST_KGROUP_PROLOGUE = 1,  /* per stage: diagnostics, slow tendencies, w-p factorisation */
+    MOIST_KGROUP_SUBSTEP = 2,   /* per acoustic substep */
+    MOIST_KGROUP_TRACER = 3,    /* per stage: Koren tracer transport (Gauss-Seidel order) */
+    MOIST_KGROUP_UPDATE = 4,    /* per stage: state update and NaN check */
+    MOIST_KGROUP_OTHER = 5,     /* precipitation accumulation */
+    MOIST_NGROUPS = 6
+};
+/* Run nsteps large steps with CUDA events recorded on the context stream before each kernel
+ * group: *total_ms = device time from the first to the last event, group_ms[g] = time spent
+ * in group g, group_launches[g] = kernels launched in group g (arrays of MOIST_NGROUPS; any
+ * pointer may be NULL). */
+int moist_step_profile(moist_ctx* ctx, int nsteps, float* total_ms, float* group_ms,
+                       long long* group_launches);
 
 /* Stream of the context (a cudaStream_t), for callers that order their own work after it. */
 void* moist_stream(moist_ctx* ctx);

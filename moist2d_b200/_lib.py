@@ -13,7 +13,8 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_last_error", "moist_nan_field", "moist_upload_state", "moist_download_state",
            "moist_rk3_step", "moist_compute_step", "moist_cloud_microphysics",
            "moist_rain_sedimentation", "moist_implicit_correction", "moist_eval_helper",
-           "moist_budget", "moist_stream", "moist_synchronize", "moist_time_steps")
+           "moist_budget", "moist_stream", "moist_synchronize", "moist_time_steps",
+           "moist_rk3_step_host", "moist_step_profile", "moist_set_device")
 
 
 def lib():
@@ -46,5 +47,9 @@ def lib():
         L.moist_stream.restype = V
         L.moist_synchronize.argtypes = [Ctx]
         L.moist_time_steps.argtypes = [Ctx, I, C.POINTER(C.c_float)]
+        L.moist_rk3_step_host.argtypes = [Ctx, S, I]
+        L.moist_set_device.argtypes = [I]
+        L.moist_step_profile.argtypes = [Ctx, I, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                         C.POINTER(C.c_longlong)]
         _lib = L
     return _lib

@@ -17,6 +17,14 @@ MOIST_ERR_NOMEM = 6
 
 MOIST_FLAG_TRI_NATIVE = 1
 
+MOIST_KGROUP_PHYSICS = 0
+MOIST_KGROUP_PROLOGUE = 1
+MOIST_KGROUP_SUBSTEP = 2
+MOIST_KGROUP_TRACER = 3
+MOIST_KGROUP_UPDATE = 4
+MOIST_KGROUP_OTHER = 5
+MOIST_NGROUPS = 6
+
 MOIST_HELPER_F2H = 0
 MOIST_HELPER_KOREN = 1
 MOIST_HELPER_SAT_VP = 2

@@ -30,11 +30,14 @@ struct CtxBase {
     virtual int sedimentation(void* d_prec) = 0;
     virtual int budget(double out[4]) = 0;
     virtual int time_steps(int nsteps, float* ms) = 0;
+    virtual int profile(int nsteps, float* total_ms, float* group_ms, long long* group_launches) = 0;
+    virtual int rk3_host(moist_state_host* s, int nsteps) = 0;
 };
 
 }  // namespace
 
 struct moist_ctx {
+    int device = 0;
     int precision = MOIST_F32;
     int flags = 0;
     cudaStream_t stream = nullptr;
@@ -149,11 +152,36 @@ struct Ctx : CtxBase {
     T* staging;
     int* err;
     bool rd_dirty = true;
+    // profiling: events recorded before each kernel group when active
+    bool prof_on = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<int> ev_group;
+    long long launches[MOIST_NGROUPS] = {0};
+
+    int mark(int group, int nkernels) {
+        launches[group] += nkernels;
+        if (!prof_on) return MOIST_OK;
+        const size_t j = ev_group.size();
+        if (j >= ev_pool.size()) {
+            cudaEvent_t e;
+            CK(cudaEventCreate(&e));
+            ev_pool.push_back(e);
+        }
+        CK(cudaEventRecord(ev_pool[j], st));
+        ev_group.push_back(group);
+        return MOIST_OK;
+    }
+#define MARK(g, n)                              \
+    do {                                        \
+        int m_ = mark((g), (n));                \
+        if (m_ != MOIST_OK) return m_;          \
+    } while (0)
 
     explicit Ctx(moist_ctx* o) : owner(o) {}
 
     ~Ctx() override {
         if (st) cudaStreamSynchronize(st);
+        for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
         for (void* a : allocs) cudaFree(a);
     }
 
@@ -276,6 +304,15 @@ struct Ctx : CtxBase {
     }
 
     int upload(const moist_state_host* s) override {
+        int r = queue_upload(s);
+        if (r != MOIST_OK) return r;
+        CK(cudaStreamSynchronize(st));
+        return MOIST_OK;
+    }
+
+    // queue the copies and layout moves of a host State on the stream (no synchronisation;
+    // stream order keeps the single staging buffer consistent)
+    int queue_upload(const moist_state_host* s) {
         int r;
         StateP<T>& d = cur;
         const void* f2[7] = {s->rho, s->rho_u, s->rho_w, s->rho_theta, s->rho_qv, s->rho_qc, s->rho_qr};
@@ -299,31 +336,34 @@ struct Ctx : CtxBase {
             if (s->rho_u) CK(cudaMemcpyAsync(halo_vals, (const T*)s->rho_u + (size_t)(halo - 1) * nz, sizeof(T), cudaMemcpyHostToDevice, st));
             if (s->rho) CK(cudaMemcpyAsync(halo_vals + 1, (const T*)s->rho + (size_t)(nx + halo) * nz, sizeof(T), cudaMemcpyHostToDevice, st));
         }
-        CK(cudaStreamSynchronize(st));
         return MOIST_OK;
     }
 
     int download(moist_state_host* s) override {
+        int r = queue_download(s);
+        if (r != MOIST_OK) return r;
+        CK(cudaStreamSynchronize(st));
+        return MOIST_OK;
+    }
+
+    int queue_download(moist_state_host* s) {
         int r;
         const void* f2[7] = {s->rho, s->rho_u, s->rho_w, s->rho_theta, s->rho_qv, s->rho_qc, s->rho_qr};
         T* dv[7] = {cur.rho, cur.ru, cur.rw, cur.rt, cur.qv, cur.qc, cur.qr};
         for (int j = 0; j < 7; j++) {
             if ((r = get2d(dv[j], const_cast<void*>(f2[j]), true)) != MOIST_OK) return r;
-            CK(cudaStreamSynchronize(st));  // staging buffer reused
         }
         void* g2[6] = {s->d_rho_theta_mp, s->d_rho_qv_mp, s->d_rho_qc_mp, s->d_rho_qr_mp, s->d_rho_qr_sed,
                        s->d_rho_theta_rd};
         T* gv[6] = {d_th_mp, d_qv_mp, d_qc_mp, d_qr_mp, d_qr_sed, d_th_rd};
         for (int j = 0; j < 6; j++) {
             if ((r = get2d(gv[j], g2[j], false)) != MOIST_OK) return r;
-            CK(cudaStreamSynchronize(st));
         }
         void* f1[7] = {s->prec, s->mflux, s->shflux, s->lhflux, s->d_rho_u_sf, s->d_rho_theta_sf, s->d_rho_qv_sf};
         T* d1[7] = {prec, mflux, shflux, lhflux, d_u_sf, d_th_sf, d_qv_sf};
         for (int j = 0; j < 7; j++)
             if ((r = get1dx(d1[j], f1[j])) != MOIST_OK) return r;
         if (s->theta_ref) CK(cudaMemcpyAsync(s->theta_ref, theta_ref, nz * sizeof(T), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
         return MOIST_OK;
     }
 
@@ -331,6 +371,7 @@ struct Ctx : CtxBase {
     int launch_physics(int mode) {  // mode bit 1: microphysics, bit 2: sedimentation, 4: full step
         const dim3 b(32, 8), g(cdiv(nx, 32), cdiv(nz, 8));
         const bool full = mode & 4;
+        MARK(MOIST_KGROUP_PHYSICS, 1 + (full && dp.do_sf) + (full && dp.do_rd));
         if (full) {
             if (dp.do_sf) {
                 k_surface_fluxes<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, cur, halo_vals, halo_vals + 1, d_u_sf, d_th_sf,
@@ -363,6 +404,7 @@ struct Ctx : CtxBase {
     int run_stage(StateP<T> s_in, StateP<T> s0, T* const qout[3], StateP<T> s_out, T dt_stage, int ns_s) {
         const dim3 b2(32, 8), g2(cdiv(nx, 32), cdiv(nz, 8));
         const unsigned gc = cdiv(nx, 128);
+        MARK(MOIST_KGROUP_PROLOGUE, 3);
         k_diag<T><<<g2, b2, 0, st>>>(dp, s_in, pres, theta, rt2p, uface, wface, err);
         CKL();
         TendArgs<T> ta_{s_in, s0, ph, pres, theta, uface, wface, R_rho, R_ru, R_rw, R_rt, rho_p, ru_p[0], rw_p,
@@ -374,6 +416,7 @@ struct Ctx : CtxBase {
         CKL();
         const double fact_tp64 = (double)T(0.5) * (1.0 + (double)dp.beta);
         for (int n = 1; n <= ns_s; n++) {
+            MARK(MOIST_KGROUP_SUBSTEP, 1);
             SubArgs<T, TT> sa;
             sa.R_rho = R_rho;
             sa.R_ru = R_ru;
@@ -415,8 +458,10 @@ struct Ctx : CtxBase {
         tr.mfz = mfz;
         tr.dt = dt_stage;
         const int nthr = (nz + 31) / 32 * 32;
+        MARK(MOIST_KGROUP_TRACER, 1);
         k_tracer_wavefront<T><<<3, nthr, 3 * nz * sizeof(T), st>>>(dp, tr, err);
         CKL();
+        MARK(MOIST_KGROUP_UPDATE, 2);
         UpdArgs<T> ua{s_in, s_out, rho_p, ru_p[ns_s % 2], rw_p, rt_p[ns_s % 3], ph};
         k_update<T><<<g2, b2, 0, st>>>(dp, ua, err);
         CKL();
@@ -442,6 +487,7 @@ struct Ctx : CtxBase {
         if ((r = run_stage(cur, cur, nq, nxt, dt / T(3), ns1)) != MOIST_OK) return r;
         if ((r = run_stage(nxt, cur, tmpq, with_q(nxt, tmpq), dt / T(2), ns2)) != MOIST_OK) return r;
         if ((r = run_stage(with_q(nxt, tmpq), cur, nq, nxt, dt, ns)) != MOIST_OK) return r;
+        MARK(MOIST_KGROUP_OTHER, 1);
         k_prec<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, prec, d_prec, err);
         CKL();
         std::swap(cur, nxt);
@@ -484,6 +530,45 @@ struct Ctx : CtxBase {
         return finish();
     }
 
+    int profile(int nsteps, float* total_ms, float* group_ms, long long* group_launches) override {
+        if (int r = check_stage_shape()) return r;
+        CK(reset_err());
+        for (int g = 0; g < MOIST_NGROUPS; g++) launches[g] = 0;
+        ev_group.clear();
+        prof_on = true;
+        int r = MOIST_OK;
+        for (int n = 0; n < nsteps && r == MOIST_OK; n++) r = launch_step();
+        if (r == MOIST_OK) r = mark(MOIST_KGROUP_OTHER, 0);
+        prof_on = false;
+        if (r != MOIST_OK) return r;
+        CK(cudaStreamSynchronize(st));
+        for (int g = 0; g < MOIST_NGROUPS; g++) {
+            if (group_ms) group_ms[g] = 0.f;
+            if (group_launches) group_launches[g] = launches[g];
+        }
+        float tot = 0.f;
+        for (size_t j = 0; j + 1 < ev_group.size(); j++) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ev_pool[j], ev_pool[j + 1]));
+            if (group_ms) group_ms[ev_group[j]] += ms;
+            tot += ms;
+        }
+        if (total_ms) *total_ms = tot;
+        return finish();
+    }
+
+    int rk3_host(moist_state_host* s, int nsteps) override {
+        if (int r = check_stage_shape()) return r;
+        int r = queue_upload(s);
+        if (r != MOIST_OK) return r;
+        CK(reset_err());
+        for (int n = 0; n < nsteps && r == MOIST_OK; n++) r = launch_step();
+        if (r != MOIST_OK) return r;
+        r = queue_download(s);
+        if (r != MOIST_OK) return r;
+        return finish();
+    }
+
     int compute_step(const void* const phys[6], const moist_state_host* s0, double dt, int ns_s) override {
         if (ns_s < 1) return set_err(owner, MOIST_ERR_ARG, "ns must be >= 1");
         if (int r0 = check_stage_shape()) return r0;
@@ -496,13 +581,11 @@ struct Ctx : CtxBase {
         for (int j = 0; j < 7; j++) {
             if (!f2[j]) return set_err(owner, MOIST_ERR_ARG, "s0 field %d is NULL", j);
             if ((r = put2d(f2[j], dv[j])) != MOIST_OK) return r;
-            CK(cudaStreamSynchronize(st));
         }
         T* pv[6] = {ph.d_rho, ph.d_u, ph.d_th, ph.d_qv, ph.d_qc, ph.d_qr};
         for (int j = 0; j < 6; j++) {
             if (!phys[j]) return set_err(owner, MOIST_ERR_ARG, "phys field %d is NULL", j);
             if ((r = put2d(phys[j], pv[j])) != MOIST_OK) return r;
-            CK(cudaStreamSynchronize(st));
         }
         CK(reset_err());
         T* const nq[3] = {nxt.qv, nxt.qc, nxt.qr};
@@ -698,6 +781,10 @@ int moist_ctx_create(const moist_params* p, int precision, int flags, moist_ctx*
     if (p->nx < 1 || p->nz < 2 || p->halo < 0 || p->ns < 1 || p->nz > 1024) return MOIST_ERR_ARG;
     if (precision != MOIST_F32 && precision != MOIST_F64) return MOIST_ERR_ARG;
     moist_ctx* c = new moist_ctx();
+    if (cudaGetDevice(&c->device) != cudaSuccess) {
+        delete c;
+        return MOIST_ERR_CUDA;
+    }
     c->precision = precision;
     c->flags = flags;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -730,6 +817,7 @@ int moist_ctx_create(const moist_params* p, int precision, int flags, moist_ctx*
 
 int moist_ctx_destroy(moist_ctx* c) {
     if (!c) return MOIST_ERR_ARG;
+    cudaSetDevice(c->device);
     delete c->impl;
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -739,32 +827,49 @@ int moist_ctx_destroy(moist_ctx* c) {
 const char* moist_last_error(const moist_ctx* c) { return c ? c->err.c_str() : "null context"; }
 int moist_nan_field(const moist_ctx* c) { return c ? c->nan_field : -1; }
 
+// the context's device is made current for the calling thread at every entry point
+#define CTX_DEVICE(c)                                                   \
+    do {                                                                \
+        if (cudaSetDevice((c)->device) != cudaSuccess) return MOIST_ERR_CUDA; \
+    } while (0)
+
+int moist_set_device(int device) {
+    return cudaSetDevice(device) == cudaSuccess ? MOIST_OK : MOIST_ERR_CUDA;
+}
+
 int moist_upload_state(moist_ctx* c, const moist_state_host* s) {
     if (!c || !s) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
     return c->impl->upload(s);
 }
 int moist_download_state(moist_ctx* c, moist_state_host* s) {
     if (!c || !s) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
     return c->impl->download(s);
 }
 int moist_rk3_step(moist_ctx* c, int nsteps) {
     if (!c || nsteps < 0) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
     return c->impl->rk3(nsteps);
 }
 int moist_compute_step(moist_ctx* c, const void* const phys[6], const moist_state_host* s0, double dt, int ns) {
     if (!c || !phys || !s0) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
     return c->impl->compute_step(phys, s0, dt, ns);
 }
 int moist_cloud_microphysics(moist_ctx* c) {
     if (!c) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
     return c->impl->microphysics();
 }
 int moist_rain_sedimentation(moist_ctx* c, void* d_prec) {
     if (!c) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
     return c->impl->sedimentation(d_prec);
 }
 int moist_budget(moist_ctx* c, double out[4]) {
     if (!c || !out) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
     return c->impl->budget(out);
 }
 void* moist_stream(moist_ctx* c) { return c ? (void*)c->stream : nullptr; }
@@ -774,7 +879,20 @@ int moist_synchronize(moist_ctx* c) {
 }
 int moist_time_steps(moist_ctx* c, int nsteps, float* ms) {
     if (!c || !ms || nsteps < 0) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
     return c->impl->time_steps(nsteps, ms);
+}
+
+int moist_rk3_step_host(moist_ctx* c, moist_state_host* s, int nsteps) {
+    if (!c || !s || nsteps < 0) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
+    return c->impl->rk3_host(s, nsteps);
+}
+
+int moist_step_profile(moist_ctx* c, int nsteps, float* total_ms, float* group_ms, long long* group_launches) {
+    if (!c || nsteps < 0) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
+    return c->impl->profile(nsteps, total_ms, group_ms, group_launches);
 }
 
 int moist_implicit_correction(const moist_params* p, int precision, int flags, void* rho_w, const void* drho_w,

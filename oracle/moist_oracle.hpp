@@ -33,6 +33,15 @@
 #include "../include/moist2d.h"
 #include "../moist2d_b200/csrc/moist_math.h"
 
+// ORACLE_OMP builds the timed CPU baseline: the column loops run under OpenMP like the
+// reference's Threads.@threads; without it every loop runs on one thread in reference order.
+#ifdef ORACLE_OMP
+#include <omp.h>
+#define OMP_FOR _Pragma("omp parallel for schedule(static)")
+#else
+#define OMP_FOR
+#endif
+
 namespace oracle {
 
 using mm::jmax;
@@ -227,6 +236,7 @@ void cloud_microphysics(A2<T> d_rho_qv_phys, A2<T> d_rho_qc_phys, A2<T> d_rho_qr
                         A2<T> d_rho_theta_phys, A2<T> rho, A2<T> rho_theta, A2<T> rho_qv,
                         A2<T> rho_qc, A2<T> rho_qr, const Par<T>& p) {
     const T Rd = p.Rd, Rv = p.Rv, Cpd = p.Cpd, Cpv = p.Cpv, Cpl = p.Cpl, P0 = p.P0, Lv = p.Lv;
+    OMP_FOR
     for (int i = p.is; i <= p.ie; i++) {
         for (int k = p.ks; k <= p.ke; k++) {
             d_rho_qv_phys(k, i) = T(0.0);
@@ -323,12 +333,14 @@ template <class T>
 void rain_sedimentation(A2<T> d_rho_qr_sed, T* d_prec, A2<T> rho_qr, A2<T> rho, const Par<T>& p) {
     Field<T> Vt_f(p.ka, p.ia);
     A2<T> Vt = Vt_f.a();
+    OMP_FOR
     for (int i = p.is; i <= p.ie; i++)
         for (int k = p.ks; k <= p.ke; k++) {
             const T rho_qr_eff = jmax(T(0.0), rho_qr(k, i));
             Vt(k, i) = rho_qr_eff > T(1e-12) ? p.A_term * mm::mpow(rho_qr_eff / rho(k, i), p.B_term)
                                              : T(0.0);
         }
+    OMP_FOR
     for (int i = p.is; i <= p.ie; i++) {
         for (int k = p.ks; k <= p.ke; k++) {
             const T flux_kp = (k == p.ke) ? T(0.0) : rho_qr(k + 1, i) * Vt(k + 1, i);
@@ -468,7 +480,8 @@ inline T compute_limited_flux_x(A2<T> scalar_rho, A2<T> rho, A2<T> rho_u, int k,
 
 template <class T>
 inline T compute_limited_flux_z(A2<T> scalar_rho, A2<T> rho, A2<T> rho_w, int k, int i,
-                                const Par<T>& p) {
+                                const Par<T>& p, const T* lin = nullptr) {
+    if (!lin) lin = scalar_rho.d;
     const T EPS = p.EPS;
     const T dt = p.dt;  // the large step (moist.jl:900)
     const T rhow_face = rho_w(k, i);
@@ -479,7 +492,7 @@ inline T compute_limited_flux_z(A2<T> scalar_rho, A2<T> rho, A2<T> rho_w, int k,
         if (k == p.ks) {
             s_face = f2h(s_k, s_kp1, p.dz[k], p.dz[k + 1]);
             // linear index scalar_rho[k]: element (k, column 1) of the full array (moist.jl:917)
-            s_face = jmin(s_face, scalar_rho.lin(k) / (rhow_face * dt));
+            s_face = jmin(s_face, lin[k] / (rhow_face * dt));
         } else {
             const T s_km1 = scalar_rho(k - 1, i) / rho(k - 1, i);
             const T r_num = s_kp1 - s_k;
@@ -491,7 +504,7 @@ inline T compute_limited_flux_z(A2<T> scalar_rho, A2<T> rho, A2<T> rho_w, int k,
     } else if (rhow_face < -EPS) {
         if (k == p.ke - 1) {
             s_face = f2h(s_k, s_kp1, p.dz[k], p.dz[k + 1]);
-            s_face = jmin(s_face, scalar_rho.lin(k + 1) / (-rhow_face * dt));  // moist.jl:930
+            s_face = jmin(s_face, lin[k + 1] / (-rhow_face * dt));  // moist.jl:930
         } else {
             const T s_kp2 = scalar_rho(k + 2, i) / rho(k + 2, i);
             const T r_num = s_k - s_kp1;
@@ -564,6 +577,43 @@ void implicit_correction(T* rho_w, const T* drho_w, const T* theta, const T* rt2
     for (int k = ks; k <= ke - 1; k++) rho_w[k] = (T)D[k - ks];
 }
 
+// ---------------------------------------------------------------- one tracer cell (1479-1515)
+
+// The update of rho_scalar at (k, i) (moist.jl:1479-1515), in place. lin is column 1 of the full
+// array, which the linear-index boundary clamp of compute_limited_flux_z reads.
+template <class T>
+inline void tracer_cell(A2<T> rs, const T* lin, A2<T> rs0, A2<T> d_phys, A2<T> rho, A2<T> mom_flux_x,
+                        A2<T> mom_flux_z, const Par<T>& p, T dt, int k, int i) {
+    const int ks = p.ks, ke = p.ke;
+    const T dx = p.dx, kappa = p.kappa;
+    const std::vector<T>& dz = p.dz;
+    const std::vector<T>& z = p.z;
+    const T flux_x_ip = compute_limited_flux_x(rs, rho, mom_flux_x, k, i, p);
+    const T flux_x_im = compute_limited_flux_x(rs, rho, mom_flux_x, k, i - 1, p);
+    const T adv_x = (flux_x_ip - flux_x_im) / dx;
+    const T flux_z_kp = k == ke ? T(0.0) : compute_limited_flux_z(rs, rho, mom_flux_z, k, i, p, lin);
+    const T flux_z_km = k == ks ? T(0.0) : compute_limited_flux_z(rs, rho, mom_flux_z, k - 1, i, p, lin);
+    const T adv_z = (flux_z_kp - flux_z_km) / dz[k];
+    const T advection = -(adv_x + adv_z);
+    const T scalar_c = rs(k, i) / rho(k, i);
+    const T scalar_ip = rs(k, i + 1) / rho(k, i + 1);
+    const T scalar_im = rs(k, i - 1) / rho(k, i - 1);
+    const T scalar_kp = k == ke ? T(0.0) : rs(k + 1, i) / rho(k + 1, i);
+    const T scalar_km = k == ks ? T(0.0) : rs(k - 1, i) / rho(k - 1, i);
+    const T dsdx_ip = (rho(k, i + 1) + rho(k, i)) * T(0.5) * (scalar_ip - scalar_c) / dx;
+    const T dsdx_im = (rho(k, i) + rho(k, i - 1)) * T(0.5) * (scalar_c - scalar_im) / dx;
+    const T diff_x = kappa * (dsdx_ip - dsdx_im) / dx;
+    const T dsdz_kp = k == ke ? T(0.0)
+                              : f2h(rho(k + 1, i), rho(k, i), dz[k + 1], dz[k]) * (scalar_kp - scalar_c) /
+                                    (z[k + 1] - z[k]);
+    const T dsdz_km = k == ks ? T(0.0)
+                              : f2h(rho(k, i), rho(k - 1, i), dz[k], dz[k - 1]) * (scalar_c - scalar_km) /
+                                    (z[k] - z[k - 1]);
+    const T diff_z = kappa * (dsdz_kp - dsdz_km) / dz[k];
+    const T diffusion = diff_x + diff_z;
+    rs(k, i) = rs0(k, i) + dt * (advection + diffusion + d_phys(k, i));
+}
+
 // ---------------------------------------------------------------- one RK stage (1039-1580)
 
 // returns -1, or the index (MOIST_FIELD_*) of the first field found with a NaN
@@ -582,6 +632,7 @@ int compute_step(A2<T> d_rho_phys, A2<T> d_rho_u_phys, A2<T> d_rho_theta_phys, A
     // --- diagnostics (moist.jl:1045-1065)
     Field<T> pres_f(ka, ia), theta_f(ka, ia), rt2pres_f(ka, ia);
     A2<T> pres = pres_f.a(), theta = theta_f.a(), rt2pres = rt2pres_f.a();
+    OMP_FOR
     for (int i = is; i <= ie + 1; i++)
         for (int k = ks; k <= ke; k++) {
             const T qv = s.rho_qv.a()(k, i) / rho(k, i);
@@ -607,6 +658,7 @@ int compute_step(A2<T> d_rho_phys, A2<T> d_rho_u_phys, A2<T> d_rho_theta_phys, A
           R_rho_theta = R_rho_theta_f.a();
 
     // --- R_rho (moist.jl:1079-1086)
+    OMP_FOR
     for (int i = is; i <= ie; i++)
         for (int k = ks; k <= ke; k++) {
             const T flux_kp = k == ke ? T(0.0) : rho_w(k, i);
@@ -618,10 +670,12 @@ int compute_step(A2<T> d_rho_phys, A2<T> d_rho_u_phys, A2<T> d_rho_theta_phys, A
     // --- R_rho_u (moist.jl:1091-1179)
     Field<T> u_face_f(ka, ia);
     A2<T> u_face = u_face_f.a();
+    OMP_FOR
     for (int i = is; i <= ie; i++)
         for (int k = ks; k <= ke; k++)
             u_face(k, i) = rho_u(k, i) * T(2.0) / (rho(k, i) + rho(k, i + 1));
     exchange_halo(u_face, p);
+    OMP_FOR
     for (int i = is; i <= ie; i++)
         for (int k = ks; k <= ke; k++) {
             const T rho_u_ip = T(0.5) * (rho_u(k, i) + rho_u(k, i + 1));
@@ -703,9 +757,11 @@ int compute_step(A2<T> d_rho_phys, A2<T> d_rho_u_phys, A2<T> d_rho_theta_phys, A
     // --- R_rho_w (moist.jl:1184-1278)
     Field<T> w_face_f(ka, ia);
     A2<T> w_face = w_face_f.a();
+    OMP_FOR
     for (int i = is - 2; i <= ie + 2; i++)
         for (int k = ks; k <= ke - 1; k++)
             w_face(k, i) = rho_w(k, i) / f2h(rho(k, i), rho(k + 1, i), dz[k], dz[k + 1]);
+    OMP_FOR
     for (int i = is; i <= ie; i++)
         for (int k = ks; k <= ke - 1; k++) {
             const T rho_u_ip = f2h(rho_u(k, i), rho_u(k + 1, i), z[k], z[k + 1]);  // z weights (1196)
@@ -788,6 +844,7 @@ int compute_step(A2<T> d_rho_phys, A2<T> d_rho_u_phys, A2<T> d_rho_theta_phys, A
         }
 
     // --- R_rho_theta (moist.jl:1284-1332)
+    OMP_FOR
     for (int i = is; i <= ie; i++)
         for (int k = ks; k <= ke; k++) {
             T flux_ip, flux_im, flux_kp, flux_km;
@@ -831,7 +888,8 @@ int compute_step(A2<T> d_rho_phys, A2<T> d_rho_u_phys, A2<T> d_rho_theta_phys, A
     Field<T> rho_p_f(ka, ia), rho_u_p_f(ka, ia), rho_w_p_f(ka, ia), rho_theta_p_f(ka, ia);
     A2<T> rho_p = rho_p_f.a(), rho_u_p = rho_u_p_f.a(), rho_w_p = rho_w_p_f.a(),
           rho_theta_p = rho_theta_p_f.a();
-    for (size_t j = 0; j < (size_t)ka * ia; j++) {
+    OMP_FOR
+    for (long j = 0; j < (long)ka * ia; j++) {
         rho_p.d[j] = s0.rho.v[j] - s.rho.v[j];
         rho_u_p.d[j] = s0.rho_u.v[j] - s.rho_u.v[j];
         rho_w_p.d[j] = s0.rho_w.v[j] - s.rho_w.v[j];
@@ -845,9 +903,9 @@ int compute_step(A2<T> d_rho_phys, A2<T> d_rho_u_phys, A2<T> d_rho_theta_phys, A
 
     // --- acoustic substeps (moist.jl:1351-1461)
     const T dt_s = dt / T(ns);
-    std::vector<T> rho_p_tp(ka), rho_theta_p_tp(ka), drho_w_p(ka, T(0));
     for (int n = 1; n <= ns; n++) {
         if (n > 1) exchange_halo(rho_theta_p, p);
+        OMP_FOR
         for (int i = is; i <= ie; i++)
             for (int k = ks; k <= ke; k++) {
                 T grad_x = (rho_theta_p(k, i + 1) - rho_theta_p(k, i)) / dx;
@@ -860,7 +918,9 @@ int compute_step(A2<T> d_rho_phys, A2<T> d_rho_u_phys, A2<T> d_rho_theta_phys, A
         rho_theta_p_old_f.v = rho_theta_p_f.v;
         // Float64 factor even in Float32 runs: T(0.5) * (1.0 + beta) (moist.jl:1375)
         const double fact_tp = (double)T(0.5) * (1.0 + (double)p.beta_offcenter);
+        OMP_FOR
         for (int i = is; i <= ie; i++) {
+            std::vector<T> rho_p_tp(ka), rho_theta_p_tp(ka), drho_w_p(ka, T(0));
             for (int k = ks; k <= ke; k++) {
                 T advection = -(rho_u_p(k, i) - rho_u_p(k, i - 1)) / dx;
                 T inc = dt_s * (R_rho(k, i) + advection);
@@ -913,6 +973,7 @@ int compute_step(A2<T> d_rho_phys, A2<T> d_rho_u_phys, A2<T> d_rho_theta_phys, A
                 rho_theta_p(k, i) += dt_s * advection;
             }
         }
+        OMP_FOR
         for (int i = is; i <= ie; i++) {
             for (int k = ks; k <= ke; k++) mom_flux_x(k, i) += rho_u_p(k, i) / T(ns);
             for (int k = ks; k <= ke - 1; k++) mom_flux_z(k, i) += rho_w_p(k, i) / T(ns);
@@ -925,41 +986,43 @@ int compute_step(A2<T> d_rho_phys, A2<T> d_rho_u_phys, A2<T> d_rho_theta_phys, A
     exchange_halo(s.rho_qr.a(), p);
 
     // --- tracer transport: in-place, lexicographic Gauss-Seidel order (moist.jl:1469-1518)
+    A2<T> trs[3] = {s.rho_qv.a(), s.rho_qc.a(), s.rho_qr.a()};
+    A2<T> tr0[3] = {s0.rho_qv.a(), s0.rho_qc.a(), s0.rho_qr.a()};
+    A2<T> dph[3] = {d_rho_qv_phys, d_rho_qc_phys, d_rho_qr_phys};
+#ifndef ORACLE_OMP
     for (int i = is; i <= ie; i++)
-        for (int k = ks; k <= ke; k++) {
-            A2<T> trs[3] = {s.rho_qv.a(), s.rho_qc.a(), s.rho_qr.a()};
-            A2<T> tr0[3] = {s0.rho_qv.a(), s0.rho_qc.a(), s0.rho_qr.a()};
-            A2<T> dph[3] = {d_rho_qv_phys, d_rho_qc_phys, d_rho_qr_phys};
-            for (int t = 0; t < 3; t++) {
-                A2<T> rs = trs[t];
-                const T flux_x_ip = compute_limited_flux_x(rs, rho, mom_flux_x, k, i, p);
-                const T flux_x_im = compute_limited_flux_x(rs, rho, mom_flux_x, k, i - 1, p);
-                const T adv_x = (flux_x_ip - flux_x_im) / dx;
-                const T flux_z_kp = k == ke ? T(0.0) : compute_limited_flux_z(rs, rho, mom_flux_z, k, i, p);
-                const T flux_z_km = k == ks ? T(0.0) : compute_limited_flux_z(rs, rho, mom_flux_z, k - 1, i, p);
-                const T adv_z = (flux_z_kp - flux_z_km) / dz[k];
-                const T advection = -(adv_x + adv_z);
-                const T scalar_c = rs(k, i) / rho(k, i);
-                const T scalar_ip = rs(k, i + 1) / rho(k, i + 1);
-                const T scalar_im = rs(k, i - 1) / rho(k, i - 1);
-                const T scalar_kp = k == ke ? T(0.0) : rs(k + 1, i) / rho(k + 1, i);
-                const T scalar_km = k == ks ? T(0.0) : rs(k - 1, i) / rho(k - 1, i);
-                const T dsdx_ip = (rho(k, i + 1) + rho(k, i)) * T(0.5) * (scalar_ip - scalar_c) / dx;
-                const T dsdx_im = (rho(k, i) + rho(k, i - 1)) * T(0.5) * (scalar_c - scalar_im) / dx;
-                const T diff_x = kappa * (dsdx_ip - dsdx_im) / dx;
-                const T dsdz_kp = k == ke ? T(0.0)
-                                          : f2h(rho(k + 1, i), rho(k, i), dz[k + 1], dz[k]) *
-                                                (scalar_kp - scalar_c) / (z[k + 1] - z[k]);
-                const T dsdz_km = k == ks ? T(0.0)
-                                          : f2h(rho(k, i), rho(k - 1, i), dz[k], dz[k - 1]) *
-                                                (scalar_c - scalar_km) / (z[k] - z[k - 1]);
-                const T diff_z = kappa * (dsdz_kp - dsdz_km) / dz[k];
-                const T diffusion = diff_x + diff_z;
-                rs(k, i) = tr0[t](k, i) + dt * (advection + diffusion + dph[t](k, i));
+        for (int k = ks; k <= ke; k++)
+            for (int t = 0; t < 3; t++) tracer_cell(trs[t], trs[t].d, tr0[t], dph[t], rho, mom_flux_x, mom_flux_z, p, dt, k, i);
+#else
+    // Threads.@threads over i: each thread sweeps a contiguous chunk of columns in order and
+    // reads the two columns left of its chunk from the pre-sweep values
+    {
+        std::vector<std::vector<T>> snap(3);
+        for (int t = 0; t < 3; t++) snap[t] = std::vector<T>(trs[t].d, trs[t].d + (size_t)ka * ia);
+#pragma omp parallel
+        {
+            const int nt = omp_get_num_threads(), tid = omp_get_thread_num();
+            const int nxi = ie - is + 1;
+            const int i0 = is + (int)((long)nxi * tid / nt), i1 = is + (int)((long)nxi * (tid + 1) / nt);
+            if (i1 > i0) {
+                for (int t = 0; t < 3; t++) {
+                    std::vector<T> buf((size_t)ka * (i1 - i0 + 4));
+                    for (int i = i0 - 2; i < i1 + 2; i++)
+                        for (int k = 0; k < ka; k++) buf[k + (size_t)ka * (i - i0 + 2)] = snap[t][k + (size_t)ka * i];
+                    A2<T> loc{buf.data() - (ptrdiff_t)ka * (i0 - 2), ka};
+                    for (int i = i0; i < i1; i++)
+                        for (int k = ks; k <= ke; k++)
+                            tracer_cell(loc, snap[t].data(), tr0[t], dph[t], rho, mom_flux_x, mom_flux_z, p, dt, k, i);
+                    for (int i = i0; i < i1; i++)
+                        for (int k = 0; k < ka; k++) trs[t](k, i) = loc(k, i);
+                }
             }
         }
+    }
+#endif
 
     // --- state update (moist.jl:1522-1539)
+    OMP_FOR
     for (int i = is; i <= ie; i++) {
         for (int k = ks; k <= ke; k++) {
             rho(k, i) = rho(k, i) + rho_p(k, i);
