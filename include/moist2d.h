@@ -191,6 +191,29 @@ int moist_implicit_correction(const moist_params* p, int precision, int flags, v
                               const void* drho_w, const void* theta, const void* rt2pres,
                               double dt);
 
+/* Allocation-free variant of moist_implicit_correction for callers that must not have a
+ * library allocate device memory behind them (a host that routes all device memory through its
+ * own pool, such as Julia's CUDA.jl; code running while its stream is captured into a CUDA
+ * graph; fixed device-memory budgets). It has no counterpart in the reference.
+ * Solves implicit_correction! for ncols columns at once. rho_w (updated in place), drho_w,
+ * theta and rt2pres are DEVICE arrays of type T laid out (nz, ncols) with z fastest (column j
+ * starts at element j*nz); p->dz, p->z (host) give the grid; p->grav and p->beta_offcenter
+ * are read. The work is queued on `stream` (a cudaStream_t, NULL = default stream) and the
+ * call returns without waiting. It calls no cudaMalloc or cudaFree: its scratch is one
+ * fixed array of MOIST_NOALLOC_SCRATCH_BYTES per device, held by every GPU that loads the
+ * library until exit. Limit: 2*(nz-1)*ncols*sizeof(elimination type) + 2*nz*sizeof(T)
+ * (rounded up to 256) <= MOIST_NOALLOC_SCRATCH_BYTES (e.g. 2048 columns of 128 levels with the
+ * FP64 elimination); larger calls return MOIST_ERR_ARG and write the reason to err (if not
+ * NULL). The first call on a device looks up the scratch array's device address; make that
+ * first call before any stream capture. All calls share the array and nothing in it needs to
+ * start at zero (every element is written before it is read); calls that overlap on the same
+ * GPU (for example on two streams) race on it, so serialise them. */
+#define MOIST_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)
+int moist_implicit_correction_noalloc(const moist_params* p, int precision, int flags, int ncols,
+                                      void* rho_w, const void* drho_w, const void* theta,
+                                      const void* rt2pres, double dt, void* stream, char* err,
+                                      size_t errlen);
+
 /* Device evaluation of the scalar helpers, for the restated unit tests (runtests.jl:25-80,
  * 377-401): out[j] = helper(in[j*nin ...]) for j < n, computed by the same device functions
  * the kernels use. Values are passed as double and rounded to the precision first. */

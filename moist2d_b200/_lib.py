@@ -14,7 +14,8 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_rk3_step", "moist_compute_step", "moist_cloud_microphysics",
            "moist_rain_sedimentation", "moist_implicit_correction", "moist_eval_helper",
            "moist_budget", "moist_stream", "moist_synchronize", "moist_time_steps",
-           "moist_rk3_step_host", "moist_step_profile", "moist_set_device")
+           "moist_rk3_step_host", "moist_step_profile", "moist_set_device",
+           "moist_implicit_correction_noalloc")
 
 
 def lib():
@@ -49,6 +50,8 @@ def lib():
         L.moist_time_steps.argtypes = [Ctx, I, C.POINTER(C.c_float)]
         L.moist_rk3_step_host.argtypes = [Ctx, S, I]
         L.moist_set_device.argtypes = [I]
+        L.moist_implicit_correction_noalloc.argtypes = [P, I, I, I, V, V, V, V, D, V, C.c_char_p,
+                                                        C.c_size_t]
         L.moist_step_profile.argtypes = [Ctx, I, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                          C.POINTER(C.c_longlong)]
         _lib = L
