@@ -73,7 +73,10 @@ enum {
 enum {
     /* In a MOIST_F32 context the w-p tridiagonal elimination runs in FP64 by default; this flag
      * selects the reference's literal Float32 elimination (moist.jl:952-971) instead. */
-    MOIST_FLAG_TRI_NATIVE = 1
+    MOIST_FLAG_TRI_NATIVE = 1,
+    /* Run the tracer transport as one exact wavefront per tracer instead of the tiled sweep
+     * (same results bit for bit, much slower; kept for cross-checking). */
+    MOIST_FLAG_TRACER_WAVEFRONT = 2
 };
 
 /*
@@ -250,6 +253,11 @@ enum {
  * pointer may be NULL). */
 int moist_step_profile(moist_ctx* ctx, int nsteps, float* total_ms, float* group_ms,
                        long long* group_launches);
+
+/* Diagnostic of the tiled tracer sweep: counts[p] (p < n, p < 64) = sweeps since the last call
+ * that reached their bitwise fixed point after p passes; the counters are reset.
+ * MOIST_ERR_UNSUPPORTED when the context runs the wavefront sweep. */
+int moist_tracer_pass_counts(moist_ctx* ctx, int* counts, int n);
 
 /* Stream of the context (a cudaStream_t), for callers that order their own work after it. */
 void* moist_stream(moist_ctx* ctx);

@@ -15,7 +15,7 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_rain_sedimentation", "moist_implicit_correction", "moist_eval_helper",
            "moist_budget", "moist_stream", "moist_synchronize", "moist_time_steps",
            "moist_rk3_step_host", "moist_step_profile", "moist_set_device",
-           "moist_implicit_correction_noalloc")
+           "moist_implicit_correction_noalloc", "moist_tracer_pass_counts")
 
 
 def lib():
@@ -50,6 +50,7 @@ def lib():
         L.moist_time_steps.argtypes = [Ctx, I, C.POINTER(C.c_float)]
         L.moist_rk3_step_host.argtypes = [Ctx, S, I]
         L.moist_set_device.argtypes = [I]
+        L.moist_tracer_pass_counts.argtypes = [Ctx, C.POINTER(I), I]
         L.moist_implicit_correction_noalloc.argtypes = [P, I, I, I, V, V, V, V, D, V, C.c_char_p,
                                                         C.c_size_t]
         L.moist_step_profile.argtypes = [Ctx, I, C.POINTER(C.c_float), C.POINTER(C.c_float),

@@ -161,57 +161,40 @@ __device__ __forceinline__ T terminal_velocity(T rqr, T rho, const DevParams<T>&
 }
 
 // compute_limited_flux_x (moist.jl:850-892) for the face between cells "0" and "p1", with
-// the four scalar values s = scalar_rho / rho already formed
+// the four scalar values s = scalar_rho / rho already formed. Written without branches: the
+// upwind operands are selected first and one limiter evaluation follows, so the four face
+// fluxes of a tracer cell overlap instead of running one after another. The selected operands
+// go through the same operations as the reference's branches, so the result is identical.
 template <class T>
 __device__ __forceinline__ T limited_flux_x(T vel, T s_m1, T s_0, T s_p1, T s_p2, T EPS) {
-    T s_face;
-    if (vel > EPS) {
-        const T r_num = s_p1 - s_0;
-        const T r_den = s_0 - s_m1;
-        const T r = mm::mabs(r_den) < EPS ? T(1.0) : r_num / r_den;
-        s_face = s_0 + T(0.5) * koren(r) * r_den;
-    } else if (vel < -EPS) {
-        const T r_num = s_0 - s_p1;
-        const T r_den = s_p1 - s_p2;
-        const T r = mm::mabs(r_den) < EPS ? T(1.0) : r_num / r_den;
-        s_face = s_p1 + T(0.5) * koren(r) * r_den;
-    } else {
-        s_face = T(0.5) * (s_0 + s_p1);
-    }
-    return s_face * vel;
+    const bool pos = vel > EPS, neg = vel < -EPS;
+    const T r_num = pos ? (s_p1 - s_0) : (s_0 - s_p1);
+    const T r_den = pos ? (s_0 - s_m1) : (s_p1 - s_p2);
+    const T q = r_num / r_den;
+    const T r = mm::mabs(r_den) < EPS ? T(1.0) : q;
+    const T lim = (pos ? s_0 : s_p1) + T(0.5) * koren(r) * r_den;
+    const T cen = T(0.5) * (s_0 + s_p1);
+    return ((pos || neg) ? lim : cen) * vel;
 }
 
 // compute_limited_flux_z (moist.jl:895-945) for face k+1/2 between cells k ("0") and k+1.
 // lin_k / lin_kp1 are the reference's linear-index reads scalar_rho[k] / scalar_rho[k+1]
-// (column 1 of the full array); dt_big is the large step p.dt.
+// (column 1 of the full array); dt_big is the large step p.dt. Branch-free like
+// limited_flux_x; the downward limited value keeps the reference's minus sign.
 template <class T>
 __device__ __forceinline__ T limited_flux_z(T vel, T s_m1, T s_0, T s_p1, T s_p2, int k, int nz,
                                             T dz_k, T dz_kp1, T lin_k, T lin_kp1, T dt_big, T EPS) {
-    T s_face;
-    if (vel > EPS) {
-        if (k == 0) {
-            s_face = f2h(s_0, s_p1, dz_k, dz_kp1);
-            s_face = jmin(s_face, lin_k / (vel * dt_big));
-        } else {
-            const T r_num = s_p1 - s_0;
-            const T r_den = s_0 - s_m1;
-            const T r = mm::mabs(r_den) < EPS ? T(1.0) : r_num / r_den;
-            s_face = s_0 + T(0.5) * koren(r) * r_den;
-        }
-    } else if (vel < -EPS) {
-        if (k == nz - 2) {
-            s_face = f2h(s_0, s_p1, dz_k, dz_kp1);
-            s_face = jmin(s_face, lin_kp1 / (-vel * dt_big));
-        } else {
-            const T r_num = s_0 - s_p1;
-            const T r_den = s_p1 - s_p2;
-            const T r = mm::mabs(r_den) < EPS ? T(1.0) : r_num / r_den;
-            s_face = s_p1 - T(0.5) * koren(r) * r_den;
-        }
-    } else {
-        s_face = f2h(s_0, s_p1, dz_k, dz_kp1);
-    }
-    return s_face * vel;
+    const bool pos = vel > EPS, neg = vel < -EPS;
+    const T f2 = f2h(s_0, s_p1, dz_k, dz_kp1);
+    const T clamp = jmin(f2, (pos ? lin_k : lin_kp1) / (pos ? (vel * dt_big) : (-vel * dt_big)));
+    const T r_num = pos ? (s_p1 - s_0) : (s_0 - s_p1);
+    const T r_den = pos ? (s_0 - s_m1) : (s_p1 - s_p2);
+    const T q = r_num / r_den;
+    const T r = mm::mabs(r_den) < EPS ? T(1.0) : q;
+    const T half = T(0.5) * koren(r) * r_den;
+    const T lim = pos ? (s_0 + half) : (s_p1 - half);
+    const T face = pos ? ((k == 0) ? clamp : lim) : (neg ? ((k == nz - 2) ? clamp : lim) : f2);
+    return face * vel;
 }
 
 // third-order upwind face value times the face mass flux, the (-1, 5, 2)/6 form of

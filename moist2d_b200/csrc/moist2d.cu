@@ -15,6 +15,7 @@
 
 #include "../../include/moist2d.h"
 #include "kernels.cuh"
+#include "tracer_tiles.cuh"
 
 using namespace moist;
 
@@ -32,6 +33,7 @@ struct CtxBase {
     virtual int time_steps(int nsteps, float* ms) = 0;
     virtual int profile(int nsteps, float* total_ms, float* group_ms, long long* group_launches) = 0;
     virtual int rk3_host(moist_state_host* s, int nsteps) = 0;
+    virtual int pass_counts(int* counts, int n) = 0;
 };
 
 }  // namespace
@@ -152,6 +154,12 @@ struct Ctx : CtxBase {
     T* staging;
     int* err;
     bool rd_dirty = true;
+    // tiled tracer sweep (tracer_tiles.cuh)
+    bool use_tiles = false;
+    TileCtl tctl{};
+    T* strips = nullptr;
+    int* pass_hist = nullptr;  // [64] sweeps that converged after p passes
+    size_t tile_smem = 0;
     // profiling: events recorded before each kernel group when active
     bool prof_on = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -230,29 +238,64 @@ struct Ctx : CtxBase {
         AL(g_z, (size_t)nz);
         AL(g_zf, (size_t)nz);
         AL(staging, (size_t)nz * (nx + 2 * halo) + 32);
-        AL(err, 2);
+        AL(err, 4);  // [0] halt (NaN field), [1] pending NaN field, [2] timeout, [3] spare
         CK(cudaMemcpyAsync(g_dz, c->dz, nz * sizeof(T), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(g_z, c->z, nz * sizeof(T), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(g_zf, c->zf, nz * sizeof(T), cudaMemcpyHostToDevice, st));
         dp.dz = g_dz;
         dp.z = g_z;
         dp.zf = g_zf;
+        if (int r = init_tiles()) return r;
         CK(reset_err());
         CK(cudaStreamSynchronize(st));
         return MOIST_OK;
     }
 
     cudaError_t reset_err() {
-        const int v[2] = {INT_MAX, INT_MAX};
+        const int v[4] = {INT_MAX, INT_MAX, 0, 0};
         return cudaMemcpyAsync(err, v, sizeof v, cudaMemcpyHostToDevice, st);
+    }
+
+    // The tiled sweep needs every tile resident at once (its passes meet at grid barriers);
+    // otherwise, or when MOIST_FLAG_TRACER_WAVEFRONT is set, the exact wavefront runs instead.
+    int init_tiles() {
+        tctl.tiles_x = (nx + TT_W - 1) / TT_W;
+        tctl.tiles_z = (nz + TT_W - 1) / TT_W;
+        tctl.ntiles = tctl.tiles_x * tctl.tiles_z;
+        tctl.max_pass = tctl.tiles_x + tctl.tiles_z + 2;
+        tile_smem = sizeof(TileSmem<T>);
+        if (owner->flags & MOIST_FLAG_TRACER_WAVEFRONT) return MOIST_OK;
+        int dev = 0, nsm = 0, coop = 0, nb = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        CK(cudaFuncSetAttribute(k_tracer_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tracer_tiles<T>, 96, tile_smem));
+        if (!coop || (long)nb * nsm < tctl.ntiles) return MOIST_OK;
+        AL(strips, (size_t)2 * 3 * tctl.ntiles * 4 * TT_W);
+        AL(tctl.bar, 2);
+        AL(tctl.changed, (size_t)2 * 3 * tctl.ntiles);
+        AL(tctl.any_changed, (size_t)tctl.max_pass + 2);
+        AL(tctl.passes, 1);
+        AL(pass_hist, 64);
+        tctl.pass_ts = nullptr;
+        tctl.pass_work = nullptr;
+        tctl.timeout = err + 2;
+        int clk = 0;
+        CK(cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, dev));  // kHz
+        tctl.spin_limit = (long long)clk * 1000LL * 2;                 // about two seconds
+        use_tiles = true;
+        return MOIST_OK;
     }
 
     // finish: wait for the stream, read the NaN word
     int finish() {
-        int h[2];
+        int h[4];
         CK(cudaMemcpyAsync(h, err, sizeof h, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         CKL();
+        if (h[2] != 0)
+            return set_err(owner, MOIST_ERR_TIMEOUT, "a grid barrier of the tiled tracer sweep timed out");
         if (h[0] != INT_MAX) {
             owner->nan_field = h[0];
             static const char* names[12] = {"rho", "rho_u", "rho_w", "rho_theta", "rho_qv", "rho_qc", "rho_qr",
@@ -457,10 +500,21 @@ struct Ctx : CtxBase {
         tr.mfx = mfx;
         tr.mfz = mfz;
         tr.dt = dt_stage;
-        const int nthr = (nz + 31) / 32 * 32;
         MARK(MOIST_KGROUP_TRACER, 1);
-        k_tracer_wavefront<T><<<3, nthr, 3 * nz * sizeof(T), st>>>(dp, tr, err);
-        CKL();
+        if (use_tiles) {
+            CK(cudaMemsetAsync(tctl.any_changed, 0, (tctl.max_pass + 2) * sizeof(int), st));
+            TileCtl c = tctl;
+            T* sp = strips;
+            int* e = err;
+            void* args[] = {&dp, &tr, &c, &sp, &e};
+            CK(cudaLaunchCooperativeKernel((void*)k_tracer_tiles<T>, dim3(tctl.ntiles), dim3(96), args, tile_smem, st));
+            k_pass_count<<<1, 1, 0, st>>>(tctl.passes, pass_hist);
+            CKL();
+        } else {
+            const int nthr = (nz + 31) / 32 * 32;
+            k_tracer_wavefront<T><<<3, nthr, 3 * nz * sizeof(T), st>>>(dp, tr, err);
+            CKL();
+        }
         MARK(MOIST_KGROUP_UPDATE, 2);
         UpdArgs<T> ua{s_in, s_out, rho_p, ru_p[ns_s % 2], rw_p, rt_p[ns_s % 3], ph};
         k_update<T><<<g2, b2, 0, st>>>(dp, ua, err);
@@ -555,6 +609,17 @@ struct Ctx : CtxBase {
         }
         if (total_ms) *total_ms = tot;
         return finish();
+    }
+
+    int pass_counts(int* counts, int n) override {
+        int h[64] = {0};
+        if (use_tiles) {
+            CK(cudaMemcpyAsync(h, pass_hist, sizeof h, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemsetAsync(pass_hist, 0, sizeof h, st));
+            CK(cudaStreamSynchronize(st));
+        }
+        for (int j = 0; j < n; j++) counts[j] = j < 64 ? h[j] : 0;
+        return use_tiles ? MOIST_OK : set_err(owner, MOIST_ERR_UNSUPPORTED, "the tiled tracer sweep is not in use");
     }
 
     int rk3_host(moist_state_host* s, int nsteps) override {
@@ -887,6 +952,12 @@ int moist_rk3_step_host(moist_ctx* c, moist_state_host* s, int nsteps) {
     if (!c || !s || nsteps < 0) return MOIST_ERR_ARG;
     CTX_DEVICE(c);
     return c->impl->rk3_host(s, nsteps);
+}
+
+int moist_tracer_pass_counts(moist_ctx* c, int* counts, int n) {
+    if (!c || !counts || n < 0) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
+    return c->impl->pass_counts(counts, n);
 }
 
 int moist_step_profile(moist_ctx* c, int nsteps, float* total_ms, float* group_ms, long long* group_launches) {

@@ -1,0 +1,439 @@
+// tracer_tiles.cuh - the reference's in-place Gauss-Seidel tracer sweep, computed in parallel
+// tiles and repaired to a bitwise fixed point.
+//
+// The reference updates rho_q in place in lexicographic order (moist.jl:1469-1518), so cell
+// (k, i) reads the updated values at (k, i-1), (k, i-2), (k-1, i), (k-2, i) and the
+// stage-start values everywhere else. Write F for the map "recompute every cell from the
+// current values of its predecessors": the reference result is the unique fixed point of F
+// (unique by induction along the dependency order). Here the domain is cut into 32x32 tiles.
+// Inside a tile the order is exact: one warp per tracer, lane r owns row z0+r and processes
+// column c at wavefront step c + r, receiving the row below through warp shuffles. Across tile
+// boundaries each tile starts from speculative values of its left and bottom neighbours'
+// boundary strips (the stage-start values), publishes its own right and top strips after
+// every pass, and is recomputed only when a neighbour's strip changed. A pass in which no
+// strip changes leaves every tile computed from its neighbours' final values: a fixed point,
+// hence the reference's result bit for bit. Influence between cells decays roughly like the
+// Courant number per cell, so two or three passes suffice; the pass count is bounded by
+// tiles_x + tiles_z + 1 (information crosses one tile per pass).
+//
+// The kernel is persistent (cooperative launch, all tiles resident); passes are separated by
+// a grid barrier whose wait is bounded: on timeout it records MOIST_ERR_TIMEOUT and returns.
+#pragma once
+
+#include "fastdiv.cuh"
+#include "kernels.cuh"
+
+namespace moist {
+
+constexpr int TT_W = 32;       // tile width (columns) = tile height (rows) = warp size
+constexpr int TT_S = TT_W + 2; // staged extent with a two-cell halo
+
+struct TileCtl {
+    int tiles_x, tiles_z, ntiles, max_pass;
+    unsigned* bar;      // [0] arrival counter, [1] generation
+    int* changed;       // [2][3][ntiles] per pass parity: bit 0 right strip changed, bit 1 top strip
+    int* any_changed;   // [max_pass + 1]
+    int* passes;        // out: passes run
+    int* timeout;       // out: barrier timeout flag
+    long long spin_limit;
+    unsigned long long* pass_ts;  // optional diagnostic: globaltimer at the start of each pass
+    int* pass_work;               // optional diagnostic: [pass] warps that recomputed their tile
+};
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// bounded grid barrier; every block must call it the same number of times
+__device__ __forceinline__ bool grid_barrier(const TileCtl& c, unsigned nblocks) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vb = c.bar;
+        const unsigned gen = vb[1];
+        __threadfence();
+        const unsigned arrived = atomicAdd(c.bar, 1u);
+        int ok = 1;
+        if (arrived == nblocks - 1) {
+            c.bar[0] = 0;
+            __threadfence();
+            atomicAdd(c.bar + 1, 1u);
+        } else {
+            const long long t0 = clock64();
+            while (vb[1] == gen) {
+                if (clock64() - t0 > c.spin_limit) {
+                    ok = 0;
+                    atomicExch(c.timeout, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok && (*(volatile int*)c.timeout == 0);
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Per-row reciprocals RN(1/b) of the sweep-constant denominators of the tracer update (used by
+// DivMarkstein; ignored by DivIEEE).
+template <class T>
+struct RowRcp {
+    T dx, dz_k, sum_kp, sum_km, zd_kp, zd_km;
+};
+
+template <class D, class T>
+__device__ __forceinline__ T koren_d(T r, bool& bad) {  // moist.jl:846
+    return jmax(T(0.0), jmin(T(2.0) * r, jmin(D::divr(T(1.0) + T(2.0) * r, T(3.0), T(1.0) / T(3.0), bad), T(2.0))));
+}
+
+template <class D, class T>
+__device__ __forceinline__ T f2h_d(T vf1, T vf2, T dz1, T dz2, T r_sum, bool& bad) {  // moist.jl:249
+    return D::divr(vf1 * dz2 + vf2 * dz1, dz1 + dz2, r_sum, bad);
+}
+
+// limited_flux_x / limited_flux_z of model.cuh with the division policy D
+template <class D, class T>
+__device__ __forceinline__ T lflux_x(T vel, T s_m1, T s_0, T s_p1, T s_p2, T EPS, bool& bad) {
+    const bool pos = vel > EPS, neg = vel < -EPS;
+    const T r_num = pos ? (s_p1 - s_0) : (s_0 - s_p1);
+    const T r_den = pos ? (s_0 - s_m1) : (s_p1 - s_p2);
+    const T q = D::div(r_num, r_den, bad);
+    const T r = mm::mabs(r_den) < EPS ? T(1.0) : q;
+    const T lim = (pos ? s_0 : s_p1) + T(0.5) * koren_d<D>(r, bad) * r_den;
+    const T cen = T(0.5) * (s_0 + s_p1);
+    return ((pos || neg) ? lim : cen) * vel;
+}
+
+template <class D, class T>
+__device__ __forceinline__ T lflux_z(T vel, T s_m1, T s_0, T s_p1, T s_p2, int k, int nz, T dz_k, T dz_kp1,
+                                     T r_sum, T lin_k, T lin_kp1, T dt_big, T EPS, bool& bad) {
+    const bool pos = vel > EPS, neg = vel < -EPS;
+    const T f2 = f2h_d<D>(s_0, s_p1, dz_k, dz_kp1, r_sum, bad);
+    const T clamp = jmin(f2, D::div(pos ? lin_k : lin_kp1, pos ? (vel * dt_big) : (-vel * dt_big), bad));
+    const T r_num = pos ? (s_p1 - s_0) : (s_0 - s_p1);
+    const T r_den = pos ? (s_0 - s_m1) : (s_p1 - s_p2);
+    const T q = D::div(r_num, r_den, bad);
+    const T r = mm::mabs(r_den) < EPS ? T(1.0) : q;
+    const T half = T(0.5) * koren_d<D>(r, bad) * r_den;
+    const T lim = pos ? (s_0 + half) : (s_p1 - half);
+    const T face = pos ? ((k == 0) ? clamp : lim) : (neg ? ((k == nz - 2) ? clamp : lim) : f2);
+    return face * vel;
+}
+
+// The tracer update of one cell (moist.jl:1479-1515) from values already gathered: the same
+// operations, in the same order, as tracer_cell in kernels.cuh, with the division policy D
+// (DivIEEE, or DivMarkstein which sets `bad` when a quotient might differ from IEEE division).
+template <class D, class T>
+__device__ __forceinline__ T tracer_cell_t(const DevParams<T>& p, int k, T dt_stage, T s_c, T s_ip1, T s_ip2,
+                                           T s_kp1, T s_kp2, T s_im1, T s_im2, T s_km1, T s_km2, T lin_km1,
+                                           T lin_k, T lin_kp1, T mfx_i, T mfx_im, T mfz_k, T mfz_km, T rho_c,
+                                           T rho_ip, T rho_im, T rho_kp, T rho_km, T dz_k, T dz_kp1, T dz_km1,
+                                           T z_k, T z_kp1, T z_km1, T q0, T dph, const RowRcp<T>& rr, bool& bad) {
+    const int nz = p.nz, ke = nz - 1;
+    const T EPS = p.EPS, dx = p.dx;
+    const T fx_ip = lflux_x<D>(mfx_i, s_im1, s_c, s_ip1, s_ip2, EPS, bad);
+    const T fx_im = lflux_x<D>(mfx_im, s_im2, s_im1, s_c, s_ip1, EPS, bad);
+    const T adv_x = D::divr(fx_ip - fx_im, dx, rr.dx, bad);
+    const T fz_kp = k == ke ? T(0.0)
+                            : lflux_z<D>(mfz_k, s_km1, s_c, s_kp1, s_kp2, k, nz, dz_k, dz_kp1, rr.sum_kp, lin_k,
+                                         lin_kp1, p.dt, EPS, bad);
+    const T fz_km = k == 0 ? T(0.0)
+                           : lflux_z<D>(mfz_km, s_km2, s_km1, s_c, s_kp1, k - 1, nz, dz_km1, dz_k, rr.sum_km,
+                                        lin_km1, lin_k, p.dt, EPS, bad);
+    const T adv_z = D::divr(fz_kp - fz_km, dz_k, rr.dz_k, bad);
+    const T advection = -(adv_x + adv_z);
+    const T scalar_kp = k == ke ? T(0.0) : s_kp1;
+    const T scalar_km = k == 0 ? T(0.0) : s_km1;
+    const T dsdx_ip = D::divr((rho_ip + rho_c) * T(0.5) * (s_ip1 - s_c), dx, rr.dx, bad);
+    const T dsdx_im = D::divr((rho_c + rho_im) * T(0.5) * (s_c - s_im1), dx, rr.dx, bad);
+    const T diff_x = D::divr(p.kappa * (dsdx_ip - dsdx_im), dx, rr.dx, bad);
+    const T dsdz_kp = k == ke ? T(0.0)
+                              : D::divr(f2h_d<D>(rho_kp, rho_c, dz_kp1, dz_k, rr.sum_kp, bad) * (scalar_kp - s_c),
+                                        z_kp1 - z_k, rr.zd_kp, bad);
+    const T dsdz_km = k == 0 ? T(0.0)
+                             : D::divr(f2h_d<D>(rho_c, rho_km, dz_k, dz_km1, rr.sum_km, bad) * (s_c - scalar_km),
+                                       z_k - z_km1, rr.zd_km, bad);
+    const T diff_z = D::divr(p.kappa * (dsdz_kp - dsdz_km), dz_k, rr.dz_k, bad);
+    const T diffusion = diff_x + diff_z;
+    return q0 + dt_stage * (advection + diffusion + dph);
+}
+
+// q0, the phys tendency and the results are staged in shared memory for Float32; Float64
+// reads and writes them in global memory so that enough tiles stay resident
+template <class T>
+struct TileQ {
+    T rrho[TT_W][TT_W + 2];    // RN(1/rho) of the tile cells
+    T q0[3][TT_W][TT_W + 2];   // row stride 34: lane r reads column step - r, conflict-free
+    T dph[3][TT_W][TT_W + 2];
+    T qn[3][TT_W][TT_W + 2];
+};
+template <>
+struct TileQ<double> {};
+template <class T>
+constexpr bool kStageQ = sizeof(T) == 4;
+
+template <class T>
+struct TileSmem {
+    TileQ<T> q;
+    T bot[3][2][TT_W];       // per tracer: the lower tile's top strip for the current pass
+    T rho[TT_S][TT_S];       // rows z0-1 .. z0+32, cols x0-1 .. x0+32 (row stride 34: conflict-free wavefront reads)
+    T mx[TT_W][TT_S];        // mfx faces x0-1 .. x0+31 (index c+1), rows z0 .. z0+31
+    T mz[TT_W + 1][TT_S];    // mfz faces z0-1 .. z0+31 (index r+1), cols x0 .. x0+31
+    T s[3][TT_S][TT_S];      // per tracer: stage-start s = q/rho, rows z0 .. z0+33, cols x0 .. x0+33
+    T lin[3][TT_S + 1];      // per tracer: column 1 of the reference array (interior nx-2), rows z0-1 .. z0+33
+    T strip_out[3][4][TT_W]; // per tracer: right strip cols x0+30, x0+31 (0, 1), top strip rows z0+30, z0+31 (2, 3)
+};
+
+// strips in global memory: [parity][tracer][tile][4][32]
+template <class T>
+__device__ __forceinline__ T* strip_ptr(T* strips, int parity, int t, int tile, int ntiles) {
+    return strips + ((((size_t)parity * 3 + t) * ntiles + tile) * 4) * TT_W;
+}
+
+template <class T>
+__global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<T> a, TileCtl ctl, T* strips,
+                                                     const int* err) {
+    extern __shared__ unsigned char smem_raw[];
+    TileSmem<T>& sm = *reinterpret_cast<TileSmem<T>*>(smem_raw);
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    const int tile = blockIdx.x;
+    const int tx = tile % ctl.tiles_x, tz = tile / ctl.tiles_x;
+    const int x0 = tx * TT_W, z0 = tz * TT_W;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned nblocks = gridDim.x;
+    const bool halt = halted(err);  // uniform across the grid: every block still meets every barrier
+
+    // ---- stage the stage-start values this tile reads (coalesced rows)
+    for (int j = threadIdx.x; j < TT_S * TT_S; j += blockDim.x) {
+        const int rr = j / TT_S, cc = j % TT_S;
+        const int k = z0 - 1 + rr, i = wrapx(x0 - 1 + cc, nx);
+        // columns beyond nx+1 are never read; the bound also keeps wrapx within one period
+        sm.rho[rr][cc] = (k >= 0 && k < nz && x0 - 1 + cc < nx + 2) ? a.rho[MOIST_IDX(k, i)] : T(1);
+    }
+    for (int j = threadIdx.x; j < TT_W * (TT_W + 1); j += blockDim.x) {
+        const int rr = j / (TT_W + 1), cc = j % (TT_W + 1);
+        const int k = z0 + rr, i = wrapx(x0 - 1 + cc, nx);
+        // faces x0-1 .. nx-1 only: face i-1 and i of the cells i < nx
+        sm.mx[rr][cc] = (k < nz && x0 - 1 + cc < nx) ? a.mfx[MOIST_IDX(k, i)] : T(0);
+    }
+    for (int j = threadIdx.x; j < (TT_W + 1) * TT_W; j += blockDim.x) {
+        const int rr = j / TT_W, cc = j % TT_W;
+        const int k = z0 - 1 + rr, i = x0 + cc;
+        sm.mz[rr][cc] = (k >= 0 && k < nz && i < nx) ? a.mfz[MOIST_IDX(k, i)] : T(0);
+    }
+    for (int t = 0; t < 3; t++) {
+        const T* qo = a.q_old[t];
+        for (int j = threadIdx.x; j < TT_S * TT_S; j += blockDim.x) {
+            const int rr = j / TT_S, cc = j % TT_S;
+            const int k = z0 + rr, i = wrapx(x0 + cc, nx);
+            T v = T(0);
+            if (k < nz && x0 + cc < nx + 2) {
+                const size_t c = MOIST_IDX(k, i);
+                v = qo[c] / a.rho[c];
+            }
+            sm.s[t][rr][cc] = v;
+        }
+        for (int j = threadIdx.x; j < TT_S + 1; j += blockDim.x) {
+            const int k = z0 - 1 + j;
+            sm.lin[t][j] = (k >= 0 && k < nz) ? qo[MOIST_IDX(k, nx - 2)] : T(0);
+        }
+        if constexpr (kStageQ<T>) {
+            for (int j = threadIdx.x; j < TT_W * TT_W; j += blockDim.x) {
+                const int rr = j / TT_W, cc = j % TT_W;
+                const int k = z0 + rr, i = x0 + cc;
+                const bool ok = k < nz && i < nx;
+                sm.q.q0[t][rr][cc] = ok ? a.q0[t][MOIST_IDX(k, i)] : T(0);
+                sm.q.dph[t][rr][cc] = ok ? a.dphys[t][MOIST_IDX(k, i)] : T(0);
+                if (t == 0) sm.q.rrho[rr][cc] = ok ? T(1) / a.rho[MOIST_IDX(k, i)] : T(1);
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- pass-0 strips: the stage-start values (the speculation)
+    const int t = warp;  // this warp's tracer
+    {
+        T* out = strip_ptr(strips, 0, t, tile, ctl.ntiles);
+        const int r = lane;
+        __stcg(out + 0 * TT_W + r, sm.s[t][r][TT_W - 2]);
+        __stcg(out + 1 * TT_W + r, sm.s[t][r][TT_W - 1]);
+        __stcg(out + 2 * TT_W + r, sm.s[t][TT_W - 2][r]);
+        __stcg(out + 3 * TT_W + r, sm.s[t][TT_W - 1][r]);
+    }
+    if (!grid_barrier(ctl, nblocks)) return;
+
+    // lane-constant row data
+    const int r = lane;
+    const int k = z0 + r;
+    const bool row_ok = k < nz;
+    const int ke = nz - 1;
+    const T dz_k = row_ok ? p.dz[k] : T(1);
+    const T dz_kp1 = (row_ok && k < ke) ? p.dz[k + 1] : T(1);
+    const T dz_km1 = (row_ok && k > 0) ? p.dz[k - 1] : T(1);
+    const T z_k = row_ok ? p.z[k] : T(0);
+    const T z_kp1 = (row_ok && k < ke) ? p.z[k + 1] : T(1);
+    const T z_km1 = (row_ok && k > 0) ? p.z[k - 1] : T(-1);
+    RowRcp<T> rr;  // IEEE reciprocals, correctly rounded
+    rr.dx = T(1) / p.dx;
+    rr.dz_k = T(1) / dz_k;
+    rr.sum_kp = T(1) / (dz_k + dz_kp1);
+    rr.sum_km = T(1) / (dz_km1 + dz_k);
+    rr.zd_kp = T(1) / (z_kp1 - z_k);
+    rr.zd_km = T(1) / (z_k - z_km1);
+    const int width = min(TT_W, nx - x0);
+    const T* q0 = a.q0[t];
+    const T* dph = a.dphys[t];
+    T* qn = a.q_new[t];
+
+    int pass = 1;
+    for (; pass <= ctl.max_pass; pass++) {
+        const int cur = pass & 1, prv = cur ^ 1;
+        const int* chg_prev = ctl.changed + (size_t)prv * 3 * ctl.ntiles + (size_t)t * ctl.ntiles;
+        int* chg_cur = ctl.changed + (size_t)cur * 3 * ctl.ntiles + (size_t)t * ctl.ntiles;
+        const int left = tx > 0 ? tile - 1 : -1;
+        const int below = tz > 0 ? tile - ctl.tiles_x : -1;
+        // neighbours' strips and flags are written by other SMs: read them through L2 (__ldcg)
+        const bool compute = !halt && (pass == 1 || (left >= 0 && (__ldcg(chg_prev + left) & 1)) ||
+                                       (below >= 0 && (__ldcg(chg_prev + below) & 2)));
+        if (ctl.pass_ts && blockIdx.x == 0 && threadIdx.x == 0) ctl.pass_ts[pass] = globaltimer_ns();
+        if (ctl.pass_work && compute && lane == 0) atomicAdd(ctl.pass_work + pass, 1);
+        const T* sp_prev = strip_ptr(strips, prv, t, tile, ctl.ntiles);
+        T* sp_cur = strip_ptr(strips, cur, t, tile, ctl.ntiles);
+        int my_changed = 0;
+        if (compute) {
+            // left inputs: the left tile's right strip, or at the periodic seam the halo columns'
+            // stage-start values; bottom inputs: the lower tile's top strip (none at k = 0)
+            T prev1, prev2;
+            if (left >= 0) {
+                const T* ls = strip_ptr(strips, prv, t, left, ctl.ntiles);
+                prev2 = __ldcg(ls + 0 * TT_W + r);
+                prev1 = __ldcg(ls + 1 * TT_W + r);
+            } else {
+                prev1 = row_ok ? a.q_old[t][MOIST_IDX(k, nx - 1)] / a.rho[MOIST_IDX(k, nx - 1)] : T(0);
+                prev2 = row_ok ? a.q_old[t][MOIST_IDX(k, nx - 2)] / a.rho[MOIST_IDX(k, nx - 2)] : T(0);
+            }
+            const T* bs = below >= 0 ? strip_ptr(strips, prv, t, below, ctl.ntiles) : nullptr;
+            sm.bot[t][0][r] = bs ? __ldcg(bs + 2 * TT_W + r) : T(0);  // row z0-2
+            sm.bot[t][1][r] = bs ? __ldcg(bs + 3 * TT_W + r) : T(0);  // row z0-1
+            __syncwarp();
+            T sn_last = T(0), km1_used = T(0);
+            const int nsteps = width + TT_W - 1;
+            // Float64: q0 and the phys tendency of this lane's next cell, loaded one step ahead
+            T q0_next = T(0), dph_next = T(0);
+            if constexpr (!kStageQ<T>) {
+                if (row_ok) {  // every active lane starts at column x0 (c = 0); width >= 1
+                    q0_next = q0[MOIST_IDX(k, x0)];
+                    dph_next = dph[MOIST_IDX(k, x0)];
+                }
+            }
+            for (int step = 0; step < nsteps; step++) {
+                const int c = step - r;
+                // row-below values: lane r-1's result of the previous step and the value it used
+                const T up_sn = __shfl_up_sync(0xffffffffu, sn_last, 1);
+                const T up_km1 = __shfl_up_sync(0xffffffffu, km1_used, 1);
+                if (row_ok && c >= 0 && c < width) {
+                    T s_km1, s_km2;
+                    if (r == 0) {
+                        s_km1 = sm.bot[t][1][c];
+                        s_km2 = sm.bot[t][0][c];
+                    } else if (r == 1) {
+                        s_km1 = up_sn;
+                        s_km2 = sm.bot[t][1][c];
+                    } else {
+                        s_km1 = up_sn;
+                        s_km2 = up_km1;
+                    }
+                    const int i = x0 + c;
+                    const size_t cix = MOIST_IDX(k, i);
+                    T q0_c, dph_c;
+                    if constexpr (kStageQ<T>) {
+                        q0_c = sm.q.q0[t][r][c];
+                        dph_c = sm.q.dph[t][r][c];
+                    } else {
+                        q0_c = q0_next;
+                        dph_c = dph_next;
+                        if (c + 1 < width) {
+                            q0_next = q0[cix + 1];
+                            dph_next = dph[cix + 1];
+                        }
+                    }
+#define MOIST_TILE_CELL(D, flag)                                                                          \
+    tracer_cell_t<D>(p, k, a.dt, sm.s[t][r][c], sm.s[t][r][c + 1], sm.s[t][r][c + 2], sm.s[t][r + 1][c],        \
+                     sm.s[t][r + 2][c], prev1, prev2, s_km1, s_km2, sm.lin[t][r], sm.lin[t][r + 1],             \
+                     sm.lin[t][r + 2], sm.mx[r][c + 1], sm.mx[r][c], sm.mz[r + 1][c], sm.mz[r][c],              \
+                     sm.rho[r + 1][c + 1], sm.rho[r + 1][c + 2], sm.rho[r + 1][c], sm.rho[r + 2][c + 1],        \
+                     sm.rho[r][c + 1], dz_k, dz_kp1, dz_km1, z_k, z_kp1, z_km1, q0_c, dph_c, rr, flag)
+                    const T rho_c = sm.rho[r + 1][c + 1];
+                    T qn_v, sn;
+                    if constexpr (sizeof(T) == 4) {
+                        // sweep-constant denominators through Markstein's correction; a cell whose
+                        // operands leave its proven range is recomputed with IEEE division (fastdiv.cuh)
+                        bool bad = false;
+                        qn_v = MOIST_TILE_CELL(DivMarkstein, bad);
+                        sn = mdiv_r(qn_v, rho_c, sm.q.rrho[r][c], bad);
+                        if (bad) {
+                            bool unused = false;
+                            qn_v = MOIST_TILE_CELL(DivIEEE<T>, unused);
+                            sn = qn_v / rho_c;
+                        }
+                    } else {
+                        bool unused = false;
+                        qn_v = MOIST_TILE_CELL(DivIEEE<T>, unused);
+                        sn = qn_v / rho_c;
+                    }
+#undef MOIST_TILE_CELL
+                    if constexpr (kStageQ<T>)
+                        sm.q.qn[t][r][c] = qn_v;
+                    else
+                        qn[cix] = qn_v;
+                    if (c == TT_W - 2) sm.strip_out[t][0][r] = sn;
+                    if (c == TT_W - 1) sm.strip_out[t][1][r] = sn;
+                    if (r == TT_W - 2) sm.strip_out[t][2][c] = sn;
+                    if (r == TT_W - 1) sm.strip_out[t][3][c] = sn;
+                    prev2 = prev1;
+                    prev1 = sn;
+                    sn_last = sn;
+                    km1_used = s_km1;
+                }
+            }
+            __syncwarp();
+            if constexpr (kStageQ<T>) {  // coalesced write of the tile's results
+                for (int rr = 0; rr < TT_W; rr++) {
+                    const int kk = z0 + rr;
+                    if (kk < nz && r < width) qn[MOIST_IDX(kk, x0 + r)] = sm.q.qn[t][rr][r];
+                }
+            }
+            // publish this pass's strips; a strip entry the tile does not own (partial tile)
+            // keeps the speculative value so it never registers a change
+            for (int q = 0; q < 4; q++) {
+                const bool owned = (q < 2) ? (row_ok && width == TT_W) : ((z0 + 30 + (q - 2)) < nz && r < width);
+                const T old = __ldcg(sp_prev + q * TT_W + r);
+                const T v = owned ? sm.strip_out[t][q][r] : old;
+                __stcg(sp_cur + q * TT_W + r, v);
+                if (!(v == old || (v != v && old != old))) my_changed |= (q < 2) ? 1 : 2;
+            }
+        } else {
+            for (int q = 0; q < 4; q++) __stcg(sp_cur + q * TT_W + r, __ldcg(sp_prev + q * TT_W + r));
+        }
+        my_changed = (__any_sync(0xffffffffu, my_changed & 1) ? 1 : 0) | (__any_sync(0xffffffffu, my_changed & 2) ? 2 : 0);
+        if (lane == 0) {
+            __stcg(chg_cur + tile, my_changed);
+            if (my_changed) atomicAdd(ctl.any_changed + pass, 1);
+        }
+        if (!grid_barrier(ctl, nblocks)) return;
+        if (__ldcg(ctl.any_changed + pass) == 0) break;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *ctl.passes = pass;
+}
+
+// histogram of pass counts (diagnostic)
+__global__ void k_pass_count(const int* passes, int* hist) {
+    const int p = *passes;
+    atomicAdd(hist + (p < 63 ? p : 63), 1);
+}
+
+}  // namespace moist
