@@ -587,6 +587,241 @@ __global__ void k_substep(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T, doub
     }
 }
 
+// ----------------------------------------------------------------------------- column strips
+//
+// Strip form of the per-stage factorisation and of the acoustic substep. A block of
+// STRIP_THREADS threads owns wc adjacent columns (wc = 1, 2, 4 or 8) over all levels: the work
+// that is independent per cell runs over all cells of the strip in parallel with coalesced
+// loads, and only the Thomas recurrences run one thread per column, out of shared memory. The
+// per-column kernels above put every load of a column on the recurrence's critical path; here
+// a substep costs about one recurrence of FP64 latencies. Each value goes through the same
+// operations as in k_thomas_factors / k_substep, so the results agree bit for bit.
+
+constexpr int STRIP_THREADS = 256;
+
+// shared memory of one strip block (bytes), laid out by StripSmem
+template <class T, class TT>
+__host__ __device__ inline size_t strip_smem_bytes(int nz, int wc) {
+    const size_t n = (size_t)(nz - 1) * wc;
+    return 3 * n * sizeof(TT) + (2 * n + 2 * (size_t)nz * wc + (size_t)nz * (wc + 1)) * sizeof(T);
+}
+
+template <class T, class TT>
+struct StripSmem {
+    TT *D, *piv, *cp;      // [n][wc]: right-hand side then d', pivots, modified super-diagonal
+    T *a, *w;              // [n][wc]: sub-diagonal, new rho_w_p
+    T *rho_tp, *rt_tp;     // [nz][wc]: off-centred rho_p, rho_theta_p
+    T* u;                  // [nz][wc+1]: rho_u_p at faces i0-1/2 .. i0+wc-1/2
+    __device__ StripSmem(unsigned char* base, int nz, int wc) {
+        const size_t n = (size_t)(nz - 1) * wc;
+        D = (TT*)base;
+        piv = D + n;
+        cp = piv + n;
+        a = (T*)(cp + n);
+        w = a + n;
+        rho_tp = w + n;
+        rt_tp = rho_tp + (size_t)nz * wc;
+        u = rt_tp + (size_t)nz * wc;
+    }
+};
+
+// k_thomas_factors over a strip: the coefficients of all rows in parallel, then the pivot
+// recurrence per column
+template <class T, class TT>
+__global__ void __launch_bounds__(STRIP_THREADS) k_thomas_strip(DevParams<T> p, const T* theta, const T* rt2pres,
+                                                                 T dt_s, int wc, T* ta, T* tb, T* tc, TT* tcp,
+                                                                 TT* tpiv, const int* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (halted(err)) return;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    const int i0 = blockIdx.x * wc, ncol = min(wc, nx - i0);
+    const int ke = nz - 1, n = nz - 1;
+    const T* dz = p.dz;
+    const T* z = p.z;
+    StripSmem<T, TT> sm(smem_raw, nz, wc);
+    T* th_h = sm.rho_tp;  // [n][wc] half-level theta, f2h of the two cells around face j+1/2
+    const int col = threadIdx.x % wc, r0 = threadIdx.x / wc, rs = STRIP_THREADS / wc;
+    const bool own = col < ncol;
+    const int i = i0 + col;
+    const T fact_tp = T(0.5) * (T(1.0) + p.beta);
+    const T dt_tp2 = (dt_s * fact_tp) * (dt_s * fact_tp);
+    for (int j = r0; j < n && own; j += rs)
+        th_h[j * wc + col] = f2h(theta[MOIST_IDX(j, i)], theta[MOIST_IDX(j + 1, i)], dz[j], dz[j + 1]);
+    __syncthreads();
+    for (int j = r0; j < n && own; j += rs) {
+        const int k = j;
+        const T th_cur = th_h[j * wc + col];
+        const T th_prev = k > 0 ? th_h[(j - 1) * wc + col] : T(0);
+        const T th_next = (k + 1 <= ke - 1) ? th_h[(j + 1) * wc + col] : T(0);
+        const T r_k = rt2pres[MOIST_IDX(k, i)], r_kp = rt2pres[MOIST_IDX(k + 1, i)];
+        const T b = dt_tp2 * (r_k / dz[k] + r_kp / dz[k + 1]) * th_cur / (z[k + 1] - z[k]);
+        const T a = (k > 0) ? -dt_tp2 * (r_k * th_prev / ((z[k + 1] - z[k]) * dz[k]) - p.GRAV / (dz[k] + dz[k + 1])) : T(0);
+        const T c = (k < ke - 1) ? -dt_tp2 * (r_kp * th_next / ((z[k + 1] - z[k]) * dz[k + 1]) + p.GRAV / (dz[k] + dz[k + 1])) : T(0);
+        ta[MOIST_IDX(j, i)] = a;
+        tb[MOIST_IDX(j, i)] = b;
+        tc[MOIST_IDX(j, i)] = c;
+        sm.D[j * wc + col] = (TT)(b + T(1.0));
+        sm.a[j * wc + col] = a;
+        sm.cp[j * wc + col] = (TT)c;
+    }
+    __syncthreads();
+    if (threadIdx.x < ncol) {
+        const int cc = threadIdx.x;
+        TT cp_prev = TT(0);
+        for (int j = 0; j < n; j++) {
+            const TT bb = sm.D[j * wc + cc];
+            const TT piv = j == 0 ? bb : bb - (TT)sm.a[j * wc + cc] * cp_prev;
+            const TT cpj = sm.cp[j * wc + cc] / piv;
+            sm.piv[j * wc + cc] = piv;
+            sm.cp[j * wc + cc] = cpj;
+            cp_prev = cpj;
+        }
+    }
+    __syncthreads();
+    for (int j = r0; j < n && own; j += rs) {
+        tcp[MOIST_IDX(j, i)] = sm.cp[j * wc + col];
+        tpiv[MOIST_IDX(j, i)] = sm.piv[j * wc + col];
+    }
+}
+
+// k_substep over a strip (moist.jl:1355-1459)
+template <class T, class TT>
+__global__ void __launch_bounds__(STRIP_THREADS) k_substep_strip(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T,
+                                                                  double fact_tp64, int wc, const int* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (halted(err)) return;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    const int i0 = blockIdx.x * wc, ncol = min(wc, nx - i0);
+    const int ke = nz - 1, n = nz - 1;
+    const T dx = p.dx, EPS = p.EPS;
+    const T* dz = p.dz;
+    const T* z = p.z;
+    StripSmem<T, TT> sm(smem_raw, nz, wc);
+    const int tid = threadIdx.x;
+    const T fact_tpT = T(0.5) * (T(1.0) + p.beta);
+    const T fact_tmT = T(0.5) * (T(1.0) - p.beta);
+    const T fact = fact_tmT / fact_tpT;
+    // (1) horizontal forward step of rho_u_p at the ncol + 1 faces (1355-1366)
+    {
+        const int nf = ncol + 1, wf = wc + 1;
+        for (int e = tid; e < nz * nf; e += STRIP_THREADS) {
+            const int k = e / nf, f = e - k * nf;
+            const int cc = wrapx(i0 + f - 1, nx), cn = wrapx(cc + 1, nx);
+            const size_t a0 = MOIST_IDX(k, cc), a1 = MOIST_IDX(k, cn);
+            T grad_x = (a.rt_in[a1] - a.rt_in[a0]) / dx;
+            const T grad_x_old = (a.rt_old[a1] - a.rt_old[a0]) / dx;
+            grad_x = grad_x + p.gamma_d * (grad_x - grad_x_old);
+            const T rt2pres_h = (a.rt2pres[a0] + a.rt2pres[a1]) * T(0.5);
+            sm.u[k * wf + f] = a.ru_in[a0] + dt_s * (a.R_ru[a0] - rt2pres_h * grad_x);
+        }
+    }
+    __syncthreads();
+    const int col = tid % wc, r0 = tid / wc, rs = STRIP_THREADS / wc;
+    const bool own = col < ncol;
+    const int i = i0 + col;
+    const int im = wrapx(i - 1, nx), ip = wrapx(i + 1, nx);
+    // (2) explicit rho_p, rho_theta_p and their off-centred values (1367-1396)
+    for (int k = r0; k < nz && own; k += rs) {
+        const size_t c = MOIST_IDX(k, i);
+        const T u_m = sm.u[k * (wc + 1) + col], u_p = sm.u[k * (wc + 1) + col + 1];
+        a.ru_out[c] = u_p;
+        a.mfx[c] = a.mfx[c] + u_p / ns_T;
+        T advection = -(u_p - u_m) / dx;
+        T inc = dt_s * (a.R_rho[c] + advection);
+        const T rho_old = a.rho_p[c];
+        sm.rho_tp[k * wc + col] = (T)((double)rho_old + fact_tp64 * (double)inc);
+        a.rho_p[c] = rho_old + inc;
+        const T th_i = a.theta[c], th_ip = a.theta[MOIST_IDX(k, ip)], th_im = a.theta[MOIST_IDX(k, im)];
+        const T flux_ip = (th_ip + th_i) * T(0.5) * u_p;
+        const T flux_im = (th_i + th_im) * T(0.5) * u_m;
+        advection = -(flux_ip - flux_im) / dx;
+        inc = dt_s * (a.R_rt[c] + advection);
+        const T rtp = a.rt_in[c];
+        sm.rt_tp[k * wc + col] = (T)((double)rtp + fact_tp64 * (double)inc);
+        a.rt_out[c] = rtp + inc;
+    }
+    __syncthreads();
+    // (3) right-hand side of the w-p system (1397-1408) and the stage factors
+    for (int j = r0; j < n && own; j += rs) {
+        const int k = j + 1;
+        const size_t c = MOIST_IDX(k, i), cj = c - P;
+        const T buoyancy = (sm.rt_tp[k * wc + col] - sm.rt_tp[j * wc + col]) / (z[k] - z[j]);
+        const T grav = -p.GRAV * T(0.5) * (sm.rho_tp[k * wc + col] + sm.rho_tp[j * wc + col]);
+        const T rt2pres_h = (a.rt2pres[cj] + a.rt2pres[c]) * T(0.5);
+        const T drho_w = dt_s * (a.R_rw[cj] - rt2pres_h * buoyancy + grav);
+        const T w_j = a.rw_p[cj];
+        const T aj = a.ta[cj];
+        T d = w_j + drho_w;
+        if (j > 0) d -= aj * fact * w_j;
+        d -= a.tb[cj] * fact * w_j;
+        if (j < n - 1) d -= a.tc[cj] * fact * a.rw_p[c];
+        sm.D[j * wc + col] = (TT)d;
+        sm.a[j * wc + col] = aj;
+        sm.piv[j * wc + col] = a.tpiv[cj];
+        sm.cp[j * wc + col] = a.tcp[cj];
+    }
+    __syncthreads();
+    // (4) Thomas elimination per column (moist.jl:956-970)
+    if (tid < ncol) {
+        const int cc = tid;
+        TT dprev = sm.D[cc] / sm.piv[cc];
+        sm.D[cc] = dprev;
+        for (int j = 1; j < n; j++) {
+            const TT dp = (sm.D[j * wc + cc] - (TT)sm.a[j * wc + cc] * dprev) / sm.piv[j * wc + cc];
+            sm.D[j * wc + cc] = dp;
+            dprev = dp;
+        }
+        TT x = dprev;
+        sm.w[(n - 1) * wc + cc] = (T)x;
+        for (int j = n - 2; j >= 0; j--) {
+            x = sm.D[j * wc + cc] - sm.cp[j * wc + cc] * x;
+            sm.w[j * wc + cc] = (T)x;
+        }
+    }
+    __syncthreads();
+    // (5) vertical rho_p, rho_theta_p updates (1412-1446), momentum flux averages (1452-1458)
+    const T* th = a.theta;
+    for (int k = r0; k < nz && own; k += rs) {
+        const size_t c = MOIST_IDX(k, i);
+        const T w_k = k < ke ? sm.w[k * wc + col] : T(0.0);
+        const T w_km = k > 0 ? sm.w[(k - 1) * wc + col] : T(0.0);
+        if (k < ke) a.rw_p[c] = w_k;
+        {
+            const T flux_kp = k == ke ? T(0.0) : w_k;
+            const T flux_km = k == 0 ? T(0.0) : w_km;
+            const T advection = -(flux_kp - flux_km) / dz[k];
+            a.rho_p[c] = a.rho_p[c] + dt_s * advection;
+        }
+        T flux_kp, flux_km;
+        if (k == ke) {
+            flux_kp = T(0.0);
+        } else {
+            const T wp = w_k;
+            if (wp > EPS && k > 0)
+                flux_kp = up3(wp, th[c - P], th[c], th[c + P]);
+            else if (a.s_rw[c] < -EPS && k < ke - 1)  // selector on s.rho_w, as written (1426)
+                flux_kp = up3(wp, th[c + 2 * P], th[c + P], th[c]);
+            else
+                flux_kp = wp * f2h(th[c], th[c + P], dz[k], dz[k + 1]);
+        }
+        if (k == 0) {
+            flux_km = T(0.0);
+        } else {
+            const T wp = w_km;
+            const T sw = a.s_rw[c - P];
+            if (sw > EPS && k > 1)
+                flux_km = up3(wp, th[c - 2 * P], th[c - P], th[c]);
+            else if (sw < -EPS && k < ke)
+                flux_km = up3(wp, th[c + P], th[c], th[c - P]);
+            else
+                flux_km = wp * f2h(th[c - P], th[c], dz[k - 1], dz[k]);
+        }
+        const T advection = -(flux_kp - flux_km) / dz[k];
+        a.rt_out[c] = a.rt_out[c] + dt_s * advection;
+        if (k < ke) a.mfz[c] = a.mfz[c] + w_k / ns_T;
+    }
+}
+
 // ----------------------------------------------------------------------------- tracers
 
 template <class T>

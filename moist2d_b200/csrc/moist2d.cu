@@ -160,6 +160,9 @@ struct Ctx : CtxBase {
     T* strips = nullptr;
     int* pass_hist = nullptr;  // [64] sweeps that converged after p passes
     size_t tile_smem = 0;
+    // column strips of the factorisation and the acoustic substeps
+    int strip_wc = 1;
+    size_t strip_smem = 0;
     // profiling: events recorded before each kernel group when active
     bool prof_on = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -245,6 +248,7 @@ struct Ctx : CtxBase {
         dp.dz = g_dz;
         dp.z = g_z;
         dp.zf = g_zf;
+        if (int r = init_strips()) return r;
         if (int r = init_tiles()) return r;
         CK(reset_err());
         CK(cudaStreamSynchronize(st));
@@ -254,6 +258,25 @@ struct Ctx : CtxBase {
     cudaError_t reset_err() {
         const int v[4] = {INT_MAX, INT_MAX, 0, 0};
         return cudaMemcpyAsync(err, v, sizeof v, cudaMemcpyHostToDevice, st);
+    }
+
+    // Strip width: the widest of 8, 4, 2, 1 columns that still gives every SM a block and
+    // keeps two blocks' shared memory on an SM; one column always fits (nz <= 1024).
+    int init_strips() {
+        int dev = 0, nsm = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        strip_wc = 1;
+        for (int w : {8, 4, 2}) {
+            if (cdiv(nx, w) >= nsm && strip_smem_bytes<T, TT>(nz, w) <= 96 * 1024) {
+                strip_wc = w;
+                break;
+            }
+        }
+        strip_smem = strip_smem_bytes<T, TT>(nz, strip_wc);
+        CK(cudaFuncSetAttribute(k_thomas_strip<T, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem));
+        CK(cudaFuncSetAttribute(k_substep_strip<T, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem));
+        return MOIST_OK;
     }
 
     // The tiled sweep needs every tile resident at once (its passes meet at grid barriers);
@@ -446,7 +469,6 @@ struct Ctx : CtxBase {
 
     int run_stage(StateP<T> s_in, StateP<T> s0, T* const qout[3], StateP<T> s_out, T dt_stage, int ns_s) {
         const dim3 b2(32, 8), g2(cdiv(nx, 32), cdiv(nz, 8));
-        const unsigned gc = cdiv(nx, 128);
         MARK(MOIST_KGROUP_PROLOGUE, 3);
         k_diag<T><<<g2, b2, 0, st>>>(dp, s_in, pres, theta, rt2p, uface, wface, err);
         CKL();
@@ -455,7 +477,9 @@ struct Ctx : CtxBase {
         k_tend<T><<<g2, b2, 0, st>>>(dp, ta_, err);
         CKL();
         const T dt_s = dt_stage / T(ns_s);
-        k_thomas_factors<T, TT><<<gc, 128, 0, st>>>(dp, theta, rt2p, dt_s, ta, tb, tc, tcp, tpiv, err);
+        const unsigned gs = cdiv(nx, strip_wc);
+        k_thomas_strip<T, TT><<<gs, STRIP_THREADS, strip_smem, st>>>(dp, theta, rt2p, dt_s, strip_wc, ta, tb, tc, tcp,
+                                                                     tpiv, err);
         CKL();
         const double fact_tp64 = (double)T(0.5) * (1.0 + (double)dp.beta);
         for (int n = 1; n <= ns_s; n++) {
@@ -483,7 +507,8 @@ struct Ctx : CtxBase {
             sa.tcp = tcp;
             sa.tpiv = tpiv;
             sa.dprime = dprime;
-            k_substep<T, TT><<<gc, 128, 0, st>>>(dp, sa, dt_s, T(ns_s), fact_tp64, err);
+            k_substep_strip<T, TT><<<gs, STRIP_THREADS, strip_smem, st>>>(dp, sa, dt_s, T(ns_s), fact_tp64, strip_wc,
+                                                                          err);
             CKL();
         }
         TracerArgs<T> tr;
