@@ -162,11 +162,121 @@ __device__ __forceinline__ T tracer_cell_t(const DevParams<T>& p, int k, T dt_st
     return q0 + dt_stage * (advection + diffusion + dph);
 }
 
+// ---- the Float32 cell without branches (the fast path of the tiled sweep)
+//
+// Same operations and order as tracer_cell_t, with every division done by the branch-free
+// primitives of fastdiv.cuh and every select an explicit selp, so the four face fluxes and the
+// diffusion terms overlap in one basic block instead of waiting on one another. Those
+// primitives equal IEEE division inside stated ranges, which hold when (checked by the caller)
+// the stencil's stage-start mixing ratios are 0 or 2^-48 <= |s| < 2^49 and the densities and
+// grid constants lie in [2^-20, 2^21), and (checked here) the four updated neighbours are in
+// the same range and the five numerators that can still come out tiny or huge do not: then
+// every variable quotient lies in [2^-121, 2^121] and every fixed-denominator numerator in
+// [2^-100, 2^100]. Otherwise `bad` is set and the caller recomputes the cell with IEEE
+// division. The two clamp quotients of the vertical limiter (used on four rows only) come
+// precomputed with IEEE division in cl_kp / cl_km.
+
+template <class D>
+__device__ __forceinline__ float koren_f(float r) {  // moist.jl:846
+    const float t = 2.0f * r;
+    return jmax_f(0.0f, jmin_f(t, jmin_f(D::div3(1.0f + t), 2.0f)));
+}
+
+// (pos || neg) is |vel| > EPS: both are false for a NaN velocity
+template <class D>
+__device__ __forceinline__ float lflux_x_f(float vel, float s_m1, float s_0, float s_p1, float s_p2, float EPS) {
+    const float r_num = sel_gt(vel, EPS, s_p1 - s_0, s_0 - s_p1);
+    const float r_den = sel_gt(vel, EPS, s_0 - s_m1, s_p1 - s_p2);
+    const float r = sel_lt(fabsf(r_den), EPS, 1.0f, D::vdiv(r_num, r_den));
+    const float lim = sel_gt(vel, EPS, s_0, s_p1) + 0.5f * koren_f<D>(r) * r_den;
+    const float cen = 0.5f * (s_0 + s_p1);
+    return sel_gt(fabsf(vel), EPS, lim, cen) * vel;
+}
+
+// face k+1/2 of limited_flux_z with kk = the face's lower cell; at0 / atnm2 are kk == 0 / nz-2
+template <class D>
+__device__ __forceinline__ float lflux_z_f(float vel, float s_m1, float s_0, float s_p1, float s_p2, unsigned at0,
+                                           unsigned atnm2, float dz_a, float dz_b, float sum_ab, typename D::R rsum_ab, float cl,
+                                           float EPS) {
+    const float f2 = D::cdiv(s_0 * dz_b + s_p1 * dz_a, sum_ab, rsum_ab);
+    const float clamp = jmin_f(f2, cl);
+    const float r_num = sel_gt(vel, EPS, s_p1 - s_0, s_0 - s_p1);
+    const float r_den = sel_gt(vel, EPS, s_0 - s_m1, s_p1 - s_p2);
+    const float r = sel_lt(fabsf(r_den), EPS, 1.0f, D::vdiv(r_num, r_den));
+    const float half = 0.5f * koren_f<D>(r) * r_den;
+    const float lim = sel_gt(vel, EPS, s_0 + half, s_p1 - half);
+    // pos: kk == 0 takes the clamp; neg: kk == nz-2 takes it; neither: the face average f2
+    const float pos_face = sel_u(at0, clamp, lim), neg_face = sel_u(atnm2, clamp, lim);
+    const float face = sel_gt(vel, EPS, pos_face, sel_lt(vel, -EPS, neg_face, f2));
+    return face * vel;
+}
+
+// per-lane (row) constants of the fast cell (reciprocals in the policy's type); flags are 0 / 1
+template <class D>
+struct FastRow {
+    using R = typename D::R;
+    float dx, dz_k, dz_kp1, dz_km1, sum_kp, sum_km, zd_kp, zd_km;
+    R rdx, rdz_k, rsum_kp, rsum_km, rzd_kp, rzd_km;
+    float kappa, EPS, dt_stage;
+    unsigned k0, ke, kp_at0, kp_atnm2, km_at0, km_atnm2;
+};
+
+// v is tiny (nonzero, below 2^-100), huge (2^100 or more), infinite or NaN
+__device__ __forceinline__ bool numer_bad(float v) { return tiny_nz(v) | !(fabsf(v) < 0x1p100f); }
+
+template <class D>
+__device__ __forceinline__ float tracer_cell_f(const FastRow<D>& w, float s_c, float s_ip1, float s_ip2, float s_kp1,
+                                               float s_kp2, float s_im1, float s_im2, float s_km1, float s_km2,
+                                               float cl_kp, float cl_km, float mfx_i, float mfx_im, float mfz_k,
+                                               float mfz_km, float rho_c, float rho_ip, float rho_im, float rho_kp,
+                                               float rho_km, float q0, float dph, bool& bad) {
+    const float fx_ip = lflux_x_f<D>(mfx_i, s_im1, s_c, s_ip1, s_ip2, w.EPS);
+    const float fx_im = lflux_x_f<D>(mfx_im, s_im2, s_im1, s_c, s_ip1, w.EPS);
+    const float ndx = fx_ip - fx_im;
+    const float adv_x = D::cdiv(ndx, w.dx, w.rdx);
+    const float fz_kp = sel_u(w.ke, 0.0f,
+                              lflux_z_f<D>(mfz_k, s_km1, s_c, s_kp1, s_kp2, w.kp_at0, w.kp_atnm2, w.dz_k, w.dz_kp1,
+                                        w.sum_kp, w.rsum_kp, cl_kp, w.EPS));
+    const float fz_km = sel_u(w.k0, 0.0f,
+                              lflux_z_f<D>(mfz_km, s_km2, s_km1, s_c, s_kp1, w.km_at0, w.km_atnm2, w.dz_km1, w.dz_k,
+                                        w.sum_km, w.rsum_km, cl_km, w.EPS));
+    const float ndz = fz_kp - fz_km;
+    const float adv_z = D::cdiv(ndz, w.dz_k, w.rdz_k);
+    const float advection = -(adv_x + adv_z);
+    const float scalar_kp = sel_u(w.ke, 0.0f, s_kp1);
+    const float scalar_km = sel_u(w.k0, 0.0f, s_km1);
+    const float dsdx_ip = D::cdiv((rho_ip + rho_c) * 0.5f * (s_ip1 - s_c), w.dx, w.rdx);
+    const float dsdx_im = D::cdiv((rho_c + rho_im) * 0.5f * (s_c - s_im1), w.dx, w.rdx);
+    const float kx = w.kappa * (dsdx_ip - dsdx_im);
+    const float diff_x = D::cdiv(kx, w.dx, w.rdx);
+    const float dsdz_kp = sel_u(w.ke, 0.0f,
+                                D::cdiv(D::cdiv(rho_kp * w.dz_k + rho_c * w.dz_kp1, w.sum_kp, w.rsum_kp) * (scalar_kp - s_c),
+                                    w.zd_kp, w.rzd_kp));
+    const float dsdz_km = sel_u(w.k0, 0.0f,
+                                D::cdiv(D::cdiv(rho_c * w.dz_km1 + rho_km * w.dz_k, w.sum_km, w.rsum_km) * (s_c - scalar_km),
+                                    w.zd_km, w.rzd_km));
+    const float kz = w.kappa * (dsdz_kp - dsdz_km);
+    const float diff_z = D::cdiv(kz, w.dz_k, w.rdz_k);
+    const float diffusion = diff_x + diff_z;
+    const float q = q0 + w.dt_stage * (advection + diffusion + dph);
+    if constexpr (D::kGuarded)
+        bad = !(s_range(s_im1) & s_range(s_im2) & s_range(s_km1) & s_range(s_km2)) | numer_bad(ndx) |
+              numer_bad(ndz) | numer_bad(kx) | numer_bad(kz) | numer_bad(q);
+    else  // exact for every input; a non-finite result is left to IEEE division all the same
+        bad = !(fabsf(q) <= 0x1.fffffep127f);
+    return q;
+}
+
 // q0, the phys tendency and the results are staged in shared memory for Float32; Float64
 // reads and writes them in global memory so that enough tiles stay resident
+#ifndef MOIST_FAST_DIV
+#define MOIST_FAST_DIV Div64
+#endif
+using FastDiv = MOIST_FAST_DIV;  // division policy of the Float32 fast cell (fastdiv.cuh)
+
 template <class T>
 struct TileQ {
-    T rrho[TT_W][TT_W + 2];    // RN(1/rho) of the tile cells
+    typename FastDiv::R rrho[TT_W][TT_W + 2];  // 1/rho of the tile cells in the fast cell's form
     T q0[3][TT_W][TT_W + 2];   // row stride 34: lane r reads column step - r, conflict-free
     T dph[3][TT_W][TT_W + 2];
     T qn[3][TT_W][TT_W + 2];
@@ -186,6 +296,9 @@ struct TileSmem {
     T s[3][TT_S][TT_S];      // per tracer: stage-start s = q/rho, rows z0 .. z0+33, cols x0 .. x0+33
     T lin[3][TT_S + 1];      // per tracer: column 1 of the reference array (interior nx-2), rows z0-1 .. z0+33
     T strip_out[3][4][TT_W]; // per tracer: right strip cols x0+30, x0+31 (0, 1), top strip rows z0+30, z0+31 (2, 3)
+    T cl[3][2][2][TT_W];     // per tracer: clamp quotients of the vertical limiter [kp, km][low, high row][column]
+    unsigned okm[3][TT_W];   // per tracer and row: bit c set when cell c's stage-start stencil allows the fast cell
+    int tile_ok;             // the tile's densities (and EPS > 0) allow the fast cell
 };
 
 // strips in global memory: [parity][tracer][tile][4][32]
@@ -225,6 +338,14 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
         const int k = z0 - 1 + rr, i = x0 + cc;
         sm.mz[rr][cc] = (k >= 0 && k < nz && i < nx) ? a.mfz[MOIST_IDX(k, i)] : T(0);
     }
+    bool rho_ok = true;  // Float32 fast cell: densities inside [2^-20, 2^21)
+    if constexpr (kStageQ<T>) {
+        for (int j = threadIdx.x; j < TT_S * TT_S; j += blockDim.x) rho_ok &= d_range((&sm.rho[0][0])[j]);
+    }
+    if constexpr (kStageQ<T>) {
+        const int all = __syncthreads_and((int)(rho_ok && p.EPS > T(0)));
+        if (threadIdx.x == 0) sm.tile_ok = all;
+    }
     for (int t = 0; t < 3; t++) {
         const T* qo = a.q_old[t];
         for (int j = threadIdx.x; j < TT_S * TT_S; j += blockDim.x) {
@@ -248,14 +369,46 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
                 const bool ok = k < nz && i < nx;
                 sm.q.q0[t][rr][cc] = ok ? a.q0[t][MOIST_IDX(k, i)] : T(0);
                 sm.q.dph[t][rr][cc] = ok ? a.dphys[t][MOIST_IDX(k, i)] : T(0);
-                if (t == 0) sm.q.rrho[rr][cc] = ok ? T(1) / a.rho[MOIST_IDX(k, i)] : T(1);
+                if (t == 0) sm.q.rrho[rr][cc] = FastDiv::rcp(ok ? a.rho[MOIST_IDX(k, i)] : T(1));
             }
         }
     }
     __syncthreads();
+    const int t = warp;  // this warp's tracer
+    if constexpr (kStageQ<T>) {
+        // per-cell stencil check: s at (r, c), (r, c+1), (r, c+2), (r+1, c), (r+2, c)
+        const int r = lane;
+        unsigned m = 0;
+        for (int c = 0; c < TT_W; c++) {
+            const bool ok = s_range(sm.s[t][r][c]) & s_range(sm.s[t][r][c + 1]) & s_range(sm.s[t][r][c + 2]) &
+                            s_range(sm.s[t][r + 1][c]) & s_range(sm.s[t][r + 2][c]);
+            m |= (unsigned)ok << c;
+        }
+        sm.okm[t][r] = m;
+        // the clamp quotients lin / (+-vel dt) of limited_flux_z on the four rows that can use them:
+        // face k+1/2 from rows k = 0 and nz-2, face k-1/2 from rows k = 1 and nz-1 (IEEE division)
+        const int c = lane;
+        for (int slot = 0; slot < 2; slot++) {
+            T vkp = T(0), vkm = T(0);
+            const int kp = slot == 0 ? 0 : nz - 2;  // face kp+1/2 between cells kp, kp+1
+            const int km = slot == 0 ? 1 : nz - 1;  // face km-1/2 between cells km-1, km
+            if (kp >= 0 && kp < nz - 1 && kp >= z0 && kp < z0 + TT_W && x0 + c < nx) {
+                const T vel = sm.mz[kp - z0 + 1][c];
+                const T lin_a = sm.lin[t][kp - z0 + 1], lin_b = sm.lin[t][kp - z0 + 2];
+                vkp = vel > p.EPS ? lin_a / (vel * p.dt) : lin_b / (-vel * p.dt);
+            }
+            if (km >= 1 && km < nz && km >= z0 && km < z0 + TT_W && x0 + c < nx) {
+                const T vel = sm.mz[km - z0][c];
+                const T lin_a = sm.lin[t][km - z0], lin_b = sm.lin[t][km - z0 + 1];
+                vkm = vel > p.EPS ? lin_a / (vel * p.dt) : lin_b / (-vel * p.dt);
+            }
+            sm.cl[t][0][slot][c] = vkp;
+            sm.cl[t][1][slot][c] = vkm;
+        }
+        __syncwarp();
+    }
 
     // ---- pass-0 strips: the stage-start values (the speculation)
-    const int t = warp;  // this warp's tracer
     {
         T* out = strip_ptr(strips, 0, t, tile, ctl.ntiles);
         const int r = lane;
@@ -284,6 +437,37 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
     rr.sum_km = T(1) / (dz_km1 + dz_k);
     rr.zd_kp = T(1) / (z_kp1 - z_k);
     rr.zd_km = T(1) / (z_k - z_km1);
+    FastRow<FastDiv> fw{};
+    bool lane_fast = false;
+    if constexpr (kStageQ<T>) {
+        fw.dx = p.dx;
+        fw.dz_k = dz_k;
+        fw.dz_kp1 = dz_kp1;
+        fw.dz_km1 = dz_km1;
+        fw.sum_kp = dz_k + dz_kp1;
+        fw.sum_km = dz_km1 + dz_k;
+        fw.zd_kp = z_kp1 - z_k;
+        fw.zd_km = z_k - z_km1;
+        fw.rdx = FastDiv::rcp(fw.dx);
+        fw.rdz_k = FastDiv::rcp(fw.dz_k);
+        fw.rsum_kp = FastDiv::rcp(fw.sum_kp);
+        fw.rsum_km = FastDiv::rcp(fw.sum_km);
+        fw.rzd_kp = FastDiv::rcp(fw.zd_kp);
+        fw.rzd_km = FastDiv::rcp(fw.zd_km);
+        fw.kappa = p.kappa;
+        fw.EPS = p.EPS;
+        fw.dt_stage = a.dt;
+        fw.k0 = k == 0;
+        fw.ke = k == ke;
+        fw.kp_at0 = k == 0;
+        fw.kp_atnm2 = k == nz - 2;
+        fw.km_at0 = k - 1 == 0;
+        fw.km_atnm2 = k - 1 == nz - 2;
+        // the constants of the faces this row has (none above the top row, none below row 0)
+        lane_fast = !FastDiv::kGuarded || (sm.tile_ok && d_range(fw.dx) && d_range(fw.dz_k) &&
+                    (fw.ke || (d_range(fw.dz_kp1) && d_range(fw.sum_kp) && d_range(fw.zd_kp))) &&
+                    (fw.k0 || (d_range(fw.dz_km1) && d_range(fw.sum_km) && d_range(fw.zd_km))));
+    }
     const int width = min(TT_W, nx - x0);
     const T* q0 = a.q0[t];
     const T* dph = a.dphys[t];
@@ -330,76 +514,108 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
                     dph_next = dph[MOIST_IDX(k, x0)];
                 }
             }
-            for (int step = 0; step < nsteps; step++) {
-                const int c = step - r;
-                // row-below values: lane r-1's result of the previous step and the value it used
-                const T up_sn = __shfl_up_sync(0xffffffffu, sn_last, 1);
-                const T up_km1 = __shfl_up_sync(0xffffffffu, km1_used, 1);
-                if (row_ok && c >= 0 && c < width) {
-                    T s_km1, s_km2;
-                    if (r == 0) {
-                        s_km1 = sm.bot[t][1][c];
-                        s_km2 = sm.bot[t][0][c];
-                    } else if (r == 1) {
-                        s_km1 = up_sn;
-                        s_km2 = sm.bot[t][1][c];
-                    } else {
-                        s_km1 = up_sn;
-                        s_km2 = up_km1;
-                    }
-                    const int i = x0 + c;
-                    const size_t cix = MOIST_IDX(k, i);
-                    T q0_c, dph_c;
-                    if constexpr (kStageQ<T>) {
-                        q0_c = sm.q.q0[t][r][c];
-                        dph_c = sm.q.dph[t][r][c];
-                    } else {
-                        q0_c = q0_next;
-                        dph_c = dph_next;
-                        if (c + 1 < width) {
-                            q0_next = q0[cix + 1];
-                            dph_next = dph[cix + 1];
-                        }
-                    }
 #define MOIST_TILE_CELL(D, flag)                                                                          \
     tracer_cell_t<D>(p, k, a.dt, sm.s[t][r][c], sm.s[t][r][c + 1], sm.s[t][r][c + 2], sm.s[t][r + 1][c],        \
                      sm.s[t][r + 2][c], prev1, prev2, s_km1, s_km2, sm.lin[t][r], sm.lin[t][r + 1],             \
                      sm.lin[t][r + 2], sm.mx[r][c + 1], sm.mx[r][c], sm.mz[r + 1][c], sm.mz[r][c],              \
                      sm.rho[r + 1][c + 1], sm.rho[r + 1][c + 2], sm.rho[r + 1][c], sm.rho[r + 2][c + 1],        \
                      sm.rho[r][c + 1], dz_k, dz_kp1, dz_km1, z_k, z_kp1, z_km1, q0_c, dph_c, rr, flag)
+            if constexpr (kStageQ<T>) {
+                // Float32: every lane evaluates the branch-free cell at a clamped column each step
+                // (inactive lanes on throw-away values) and only the stores are predicated, so a
+                // step is one basic block; a cell outside the fast cell's proven ranges is
+                // recomputed with IEEE division (fastdiv.cuh). The strips are formed after the loop.
+                const T* bot0 = sm.bot[t][0];
+                const T* bot1 = sm.bot[t][1];
+                const T* cl_kp = sm.cl[t][0][k == 0 ? 0 : 1];
+                const T* cl_km = sm.cl[t][1][k == 1 ? 0 : 1];
+                const unsigned okm = FastDiv::kGuarded ? (lane_fast ? sm.okm[t][r] : 0u) : ~0u;
+                for (int step = 0; step < nsteps; step++) {
+                    const int c_raw = step - r;
+                    const bool active = row_ok && c_raw >= 0 && c_raw < width;
+                    const int c = min(max(c_raw, 0), TT_W - 1);
+                    // row-below values: lane r-1's result of the previous step and the value it used
+                    const T up_sn = __shfl_up_sync(0xffffffffu, sn_last, 1);
+                    const T up_km1 = __shfl_up_sync(0xffffffffu, km1_used, 1);
+                    const T b1 = bot1[c], b0 = bot0[c];
+                    const T s_km1 = r == 0 ? b1 : up_sn;
+                    const T s_km2 = r == 0 ? b0 : (r == 1 ? b1 : up_km1);
+                    const T q0_c = sm.q.q0[t][r][c], dph_c = sm.q.dph[t][r][c];
                     const T rho_c = sm.rho[r + 1][c + 1];
-                    T qn_v, sn;
-                    if constexpr (sizeof(T) == 4) {
-                        // sweep-constant denominators through Markstein's correction; a cell whose
-                        // operands leave its proven range is recomputed with IEEE division (fastdiv.cuh)
-                        bool bad = false;
-                        qn_v = MOIST_TILE_CELL(DivMarkstein, bad);
-                        sn = mdiv_r(qn_v, rho_c, sm.q.rrho[r][c], bad);
-                        if (bad) {
-                            bool unused = false;
-                            qn_v = MOIST_TILE_CELL(DivIEEE<T>, unused);
-                            sn = qn_v / rho_c;
-                        }
-                    } else {
+                    bool bad;
+                    T qn_v = tracer_cell_f<FastDiv>(fw, sm.s[t][r][c], sm.s[t][r][c + 1], sm.s[t][r][c + 2], sm.s[t][r + 1][c],
+                                           sm.s[t][r + 2][c], prev1, prev2, s_km1, s_km2, cl_kp[c], cl_km[c],
+                                           sm.mx[r][c + 1], sm.mx[r][c], sm.mz[r + 1][c], sm.mz[r][c], rho_c,
+                                           sm.rho[r + 1][c + 2], sm.rho[r + 1][c], sm.rho[r + 2][c + 1], sm.rho[r][c + 1],
+                                           q0_c, dph_c, bad);
+                    T sn = FastDiv::cdiv(qn_v, rho_c, sm.q.rrho[r][c]);
+                    if (active && (bad || !((okm >> c) & 1u))) {
                         bool unused = false;
                         qn_v = MOIST_TILE_CELL(DivIEEE<T>, unused);
                         sn = qn_v / rho_c;
                     }
-#undef MOIST_TILE_CELL
-                    if constexpr (kStageQ<T>)
+                    if (active) {
                         sm.q.qn[t][r][c] = qn_v;
-                    else
-                        qn[cix] = qn_v;
-                    if (c == TT_W - 2) sm.strip_out[t][0][r] = sn;
-                    if (c == TT_W - 1) sm.strip_out[t][1][r] = sn;
-                    if (r == TT_W - 2) sm.strip_out[t][2][c] = sn;
-                    if (r == TT_W - 1) sm.strip_out[t][3][c] = sn;
-                    prev2 = prev1;
-                    prev1 = sn;
+                        prev2 = prev1;
+                        prev1 = sn;
+                    }
+                    // lane r+1 reads these next step only for the column it shares with this step
                     sn_last = sn;
                     km1_used = s_km1;
                 }
+                __syncwarp();
+                // the boundary strips s = q / rho of the values just computed (IEEE division, as
+                // every s of the loop: the fast quotient equals it inside its guarded range)
+                if (row_ok && width == TT_W) {
+                    sm.strip_out[t][0][r] = sm.q.qn[t][r][TT_W - 2] / sm.rho[r + 1][TT_W - 1];
+                    sm.strip_out[t][1][r] = sm.q.qn[t][r][TT_W - 1] / sm.rho[r + 1][TT_W];
+                }
+                if (r < width) {
+                    if (z0 + TT_W - 2 < nz) sm.strip_out[t][2][r] = sm.q.qn[t][TT_W - 2][r] / sm.rho[TT_W - 1][r + 1];
+                    if (z0 + TT_W - 1 < nz) sm.strip_out[t][3][r] = sm.q.qn[t][TT_W - 1][r] / sm.rho[TT_W][r + 1];
+                }
+            } else {
+                for (int step = 0; step < nsteps; step++) {
+                    const int c = step - r;
+                    // row-below values: lane r-1's result of the previous step and the value it used
+                    const T up_sn = __shfl_up_sync(0xffffffffu, sn_last, 1);
+                    const T up_km1 = __shfl_up_sync(0xffffffffu, km1_used, 1);
+                    if (row_ok && c >= 0 && c < width) {
+                        T s_km1, s_km2;
+                        if (r == 0) {
+                            s_km1 = sm.bot[t][1][c];
+                            s_km2 = sm.bot[t][0][c];
+                        } else if (r == 1) {
+                            s_km1 = up_sn;
+                            s_km2 = sm.bot[t][1][c];
+                        } else {
+                            s_km1 = up_sn;
+                            s_km2 = up_km1;
+                        }
+                        const int i = x0 + c;
+                        const size_t cix = MOIST_IDX(k, i);
+                        const T q0_c = q0_next, dph_c = dph_next;
+                        if (c + 1 < width) {
+                            q0_next = q0[cix + 1];
+                            dph_next = dph[cix + 1];
+                        }
+                        const T rho_c = sm.rho[r + 1][c + 1];
+                        bool unused = false;
+                        const T qn_v = MOIST_TILE_CELL(DivIEEE<T>, unused);
+                        const T sn = qn_v / rho_c;
+                        qn[cix] = qn_v;
+                        if (c == TT_W - 2) sm.strip_out[t][0][r] = sn;
+                        if (c == TT_W - 1) sm.strip_out[t][1][r] = sn;
+                        if (r == TT_W - 2) sm.strip_out[t][2][c] = sn;
+                        if (r == TT_W - 1) sm.strip_out[t][3][c] = sn;
+                        prev2 = prev1;
+                        prev1 = sn;
+                        sn_last = sn;
+                        km1_used = s_km1;
+                    }
+                }
             }
+#undef MOIST_TILE_CELL
             __syncwarp();
             if constexpr (kStageQ<T>) {  // coalesced write of the tile's results
                 for (int rr = 0; rr < TT_W; rr++) {
