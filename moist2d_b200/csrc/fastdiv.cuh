@@ -1,83 +1,25 @@
-// fastdiv.cuh - branch-free, correctly rounded Float32 division by a known denominator.
+// fastdiv.cuh - branch-free, correctly rounded Float32 division for the tracer sweep.
 //
 // CUDA's IEEE division (div.rn.f32) ends every quotient with a range check and a branch to a
-// slow path, so consecutive divisions cannot overlap: a tracer cell update with ~20 of them
-// costs ~1000 cycles of dependent latency, and the Gauss-Seidel tracer sweep walks long
-// chains of such updates. Most of those divisions have a denominator that is fixed for the
-// whole sweep (dx, dz, z differences, dz sums, 3, the cell density), so its correctly rounded
-// reciprocal y = RN(1/b) can be formed once (with an IEEE division) and each quotient
-// obtained by Markstein's correction (P. Markstein, "Computation of elementary functions on
-// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990; see also the Handbook
-// of Floating-Point Arithmetic, 2nd ed., section 4.7):
-//
-//     q0 = RN(a*y);  r0 = RN(a - b*q0);  q1 = RN(q0 + r0*y)     (q1 is faithful)
-//     r1 = RN(a - b*q1);  q = RN(q1 + r1*y)                    (r1 exact, q = RN(a/b))
-//
-// with the r's and q's formed by fused multiply-adds. The theorem holds when no intermediate
-// underflows or overflows; callers pass a flag that is raised when |a| is outside
-// [2^-100, 2^100] or |b| outside [2^-20, 2^20] (so every quotient and remainder stays normal),
-// and such a cell is recomputed with IEEE division. A zero numerator returns a*y, which has the sign IEEE division gives.
-// tests/test_fastdiv.py checks the routine against IEEE division exhaustively over all finite
-// numerators for the denominators the model uses.
+// slow path (very slow for subnormal results), so consecutive divisions cannot overlap and the
+// code between them cannot be scheduled together: a tracer cell update with ~25 divisions costs
+// ~1800 cycles of dependent latency, and the Gauss-Seidel tracer sweep walks long chains of
+// such updates. Here float division is RN32(RN64(a * y)) with y = 1/b in double precision
+// (proof at div64), which returns the IEEE quotient for every input except ties in the
+// subnormal range; those are reported through a guard word (Div64) or rounded explicitly
+// (Div64X). tests/fastdiv_check.cu checks both against IEEE division on the GPU, exhaustively
+// over all numerators for the model's denominators and on random bit patterns of every class.
 #pragma once
 
 #include <cuda_runtime.h>
 
 namespace moist {
 
-__device__ __forceinline__ float mdiv_r(float a, float b, float y, bool& bad) {
-    const float q0 = a * y;
-    const float r0 = __fmaf_rn(-b, q0, a);
-    const float q1 = __fmaf_rn(r0, y, q0);
-    const float r1 = __fmaf_rn(-b, q1, a);
-    const float q = __fmaf_rn(r1, y, q1);
-    const float aa = fabsf(a), bb = fabsf(b);
-    bad |= ((a != 0.0f) && !(aa >= 0x1p-100f && aa <= 0x1p100f)) || !(bb >= 0x1p-20f && bb <= 0x1p20f);
-    return a == 0.0f ? q0 : q;
-}
-
-// ---- branch-free primitives of the fast tracer cell (no flags; callers guarantee the ranges)
-//
-// rcp_rn(b) = RN(1/b): the hardware approximation rcp.approx (relative error below 1 ulp)
-// refined by one Markstein step y = y0 + y0 (1 - b y0) (Markstein 1990, reciprocal theorem).
-// Checked against IEEE 1/b for every b with 2^-100 <= |b| < 2^101 (tests/fastdiv_check.cu).
-__device__ __forceinline__ float rcp_rn(float b) {
-    float y0;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(b));
-    const float e = __fmaf_rn(-b, y0, 1.0f);
-    return __fmaf_rn(e, y0, y0);
-}
-
-// The corrections of a zero numerator can turn -0 into +0; the sign of q0 = a*y is the sign
-// IEEE division gives, and for a nonzero quotient q0 and q have the same sign, so OR-ing the
-// sign bit of q0 into q restores the zero's sign without a compare.
+// The sign of a zero result: for a nonzero quotient q and q0 (two roundings of the same value)
+// share their sign, so OR-ing the sign bit of q0 into q only changes a zero.
 __device__ __forceinline__ float with_sign_of(float q, float q0) {
     return __int_as_float(__float_as_int(q) | (__float_as_int(q0) & (int)0x80000000));
 }
-
-// two-correction quotient with y = RN(1/b) (the sequence of mdiv_r, without its flag)
-__device__ __forceinline__ float mq2(float a, float b, float y) {
-    const float q0 = a * y;
-    const float r0 = __fmaf_rn(-b, q0, a);
-    const float q1 = __fmaf_rn(r0, y, q0);
-    const float r1 = __fmaf_rn(-b, q1, a);
-    return with_sign_of(__fmaf_rn(r1, y, q1), q0);
-}
-
-// one-correction quotient; equal to IEEE division for b = 3 and every a == 0 or
-// 2^-100 <= |a| <= 2^100 (checked exhaustively)
-__device__ __forceinline__ float mq1(float a, float b, float y) {
-    const float q0 = a * y;
-    const float r0 = __fmaf_rn(-b, q0, a);
-    return with_sign_of(__fmaf_rn(r0, y, q0), q0);
-}
-
-// a / b for a variable denominator: equal to IEEE division when 2^-100 <= |b| < 2^101 and
-// either a == 0 or |a| >= 2^-100 and 2^-125 <= |a/b| <= 2^126. Every pair of significands is
-// checked exhaustively (tests/fastdiv_check.cu); inside these bounds every rounded intermediate
-// is a normal number or a remainder that is exact in both ranges (the remainders are multiples
-// of 2^(e_a - 48) >= 2^-148), so each operation scales exactly with the exponents of a and b.
-__device__ __forceinline__ float vq(float a, float b) { return mq2(a, b, rcp_rn(b)); }
 
 // Selects the compiler cannot turn into branches: both operands are always computed, so the
 // independent parts of a cell update stay in one basic block and overlap.
@@ -112,29 +54,42 @@ __device__ __forceinline__ float jmax_f(float a, float b) {
     return r;
 }
 
-// v != 0 and |v| < 2^-100 (below the range of the Markstein quotients)
-__device__ __forceinline__ bool tiny_nz(float v) { return ((__float_as_uint(v) << 1) - 1u) < ((27u << 24) - 1u); }
-// v == 0 or 2^-48 <= |v| < 2^49: the range of mixing ratios for which the fast cell's variable
-// quotients stay inside the bounds of vq (differences of such values are 0 or in [2^-71, 2^50),
-// so their quotients lie in [2^-121, 2^121])
-__device__ __forceinline__ bool s_range(float v) {
-    const unsigned u2 = __float_as_uint(v) << 1;
-    return (u2 == 0u) | ((u2 - (79u << 24)) < (97u << 24));
-}
-// 2^-20 <= v < 2^21 (positive): the range of the fixed denominators (dx, dz, densities, ...)
-__device__ __forceinline__ bool d_range(float v) { return (__float_as_uint(v) - (107u << 23)) < (41u << 23); }
-
 // ---- FP64-reciprocal division: RN32(a/b) = RN32(RN64(a * y)) for y = 1/b to within 2^-51
 //
-// For floats a, b the quotient a/b is never a float rounding boundary (a midpoint between
-// neighbouring floats, subnormal ones included) and, when it is not a float itself, lies at a
-// relative distance of at least 2^-49 from every boundary: with A, B the 24-bit integer
-// significands, a boundary M near A/B gives |A/B - M| >= 1/(B 2^25) >= 2^-49 |A/B|. The product
-// a*y rounded to double is within 2^-52 + 2^-51 < 2^-49 of a/b, so it lies on the same side of
-// every boundary and rounding it to float gives the IEEE quotient, for every float a and every
-// b with y accurate (zeros, subnormals, infinities and overflow included, since the double
-// product neither underflows nor overflows). No range checks are needed.
+// For floats a, b whose quotient is not a float itself, a/b lies at a relative distance of at
+// least 2^-48 from every float rounding boundary (a midpoint between neighbouring floats, or
+// the overflow threshold): with A, B the integer significands, a boundary M near A/B gives
+// |A/B - M| >= 1/(B 2^25), and in the subnormal range the distance is larger still. A normal
+// quotient is never exactly a boundary (that needs 25 significant bits from a product of
+// B <= 24 bits and A); a subnormal one can be, e.g. (3 * 2^-149) / 6 = 2^-150. The product a*y
+// rounded to double is within 2^-52 + 2^-51 of a/b (the double product neither underflows nor
+// overflows), so it lies on the same side of every boundary and rounding it to float gives the
+// IEEE quotient, except for those exact subnormal ties. Every quotient q in 0 < |q| <= 2^-126
+// is therefore reported through a guard word (subnormal_guard), and the caller recomputes such
+// a cell with IEEE division; zeros, infinities and NaN come out as IEEE division gives them.
 __device__ __forceinline__ float div64(float a, double y) { return __double2float_rn((double)a * y); }
+
+// div64 exact for every input: a quotient below 2^-125 in magnitude (float spacing 2^-149) is
+// rounded explicitly on that grid. w = p 2^149 is the quotient in grid units, within 2^-28 of
+// the exact value; an exact quotient that is not a tie lies at least 2^-25 from every
+// half-integer (the nonzero integer |A 2^e - B (2k+1)| over 2B, with B >= 2^23 since b is
+// normal whenever a/b < 2^-125), so |w - fl - 1/2| < 2^-26 detects the ties, which go to the
+// even neighbour; every other w rounds to its nearest integer. The sign of a zero is p's.
+__device__ __forceinline__ float div64x(float a, double y) {
+    const double p = (double)a * y;
+    const float qn = __double2float_rn(p);
+    const double w = p * 0x1p149;
+    const double fl = floor(w);
+    const bool tie = fabs((w - fl) - 0.5) < 0x1p-26;
+    const double even = (fl - 2.0 * floor(fl * 0.5)) == 0.0 ? fl : fl + 1.0;
+    const float qs = with_sign_of((float)((tie ? even : rint(w)) * 0x1p-149), qn);
+    return fabs(p) < 0x1p-125 ? qs : qn;
+}
+
+// fold q into the guard word g (start from ~0u): afterwards g < 2^24 iff some q had
+// 0 < |q| <= 2^-126 (the doubled bit pattern of 2^-126 is 2^24; zero maps to ~0u)
+__device__ __forceinline__ void subnormal_guard(unsigned& g, float q) { g = min(g, (__float_as_uint(q) << 1) - 1u); }
+__device__ __forceinline__ bool guard_hit(unsigned g) { return g < (1u << 24); }
 
 // 1/b to within 2^-51 relative (b finite and nonzero): the hardware approximation and two
 // Newton steps e = 1 - b y, y += y e in double precision
@@ -148,22 +103,29 @@ __device__ __forceinline__ double rcp64(float b) {
     return __fma_rn(y, e, y);
 }
 
-// division policies of the fast tracer cell: cdiv(a, b, y) with y = 1/b prepared once (type R),
-// vdiv(a, b) for a variable denominator, div3(a) = a / 3
-struct Div32 {  // Markstein on FP32 FMAs: exact inside ranges the caller guards
-    using R = float;
-    static constexpr bool kGuarded = true;
-    __device__ __forceinline__ static R rcp(float b) { return 1.0f / b; }
-    __device__ __forceinline__ static float cdiv(float a, float b, R y) { return mq2(a, b, y); }
-    __device__ __forceinline__ static float vdiv(float a, float b) { return vq(a, b); }
-    __device__ __forceinline__ static float div3(float a) { return mq1(a, 3.0f, 1.0f / 3.0f); }
-};
-struct Div64 {  // FP64 reciprocal: exact for every input
+// division policies of the fast tracer cell: cdiv(a, b, y, g) with y = 1/b prepared once,
+// vdiv(a, b, g) for a variable denominator, div3(a) = a / 3; g is the subnormal guard word
+struct Div64 {  // FP64 reciprocal: exact for every input but subnormal ties, which g reports
     using R = double;
-    static constexpr bool kGuarded = false;
     __device__ __forceinline__ static R rcp(float b) { return 1.0 / (double)b; }
-    __device__ __forceinline__ static float cdiv(float a, float, R y) { return div64(a, y); }
-    __device__ __forceinline__ static float vdiv(float a, float b) { return div64(a, rcp64(b)); }
+    __device__ __forceinline__ static float cdiv(float a, float, R y, unsigned& g) {
+        const float q = div64(a, y);
+        subnormal_guard(g, q);
+        return q;
+    }
+    __device__ __forceinline__ static float vdiv(float a, float b, unsigned& g) {
+        const float q = div64(a, rcp64(b));
+        subnormal_guard(g, q);
+        return q;
+    }
+    // (1 + 2r) / 3: the numerator is 0 or at least 2^-24 in magnitude, so no subnormal quotient
+    __device__ __forceinline__ static float div3(float a) { return div64(a, 1.0 / 3.0); }
+};
+struct Div64X {  // FP64 reciprocal with explicit rounding of subnormal quotients: exact for every input
+    using R = double;
+    __device__ __forceinline__ static R rcp(float b) { return 1.0 / (double)b; }
+    __device__ __forceinline__ static float cdiv(float a, float, R y, unsigned&) { return div64x(a, y); }
+    __device__ __forceinline__ static float vdiv(float a, float b, unsigned&) { return div64x(a, rcp64(b)); }
     __device__ __forceinline__ static float div3(float a) { return div64(a, 1.0 / 3.0); }
 };
 
@@ -175,9 +137,5 @@ struct DivIEEE {
     __device__ __forceinline__ static T divr(T a, T b, T, bool&) { return a / b; }
 };
 
-struct DivMarkstein {
-    __device__ __forceinline__ static float div(float a, float b, bool&) { return a / b; }
-    __device__ __forceinline__ static float divr(float a, float b, float y, bool& bad) { return mdiv_r(a, b, y, bad); }
-};
 
 }  // namespace moist

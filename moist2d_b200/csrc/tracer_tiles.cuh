@@ -78,8 +78,8 @@ __device__ __forceinline__ bool grid_barrier(const TileCtl& c, unsigned nblocks)
     return s_ok != 0;
 }
 
-// Per-row reciprocals RN(1/b) of the sweep-constant denominators of the tracer update (used by
-// DivMarkstein; ignored by DivIEEE).
+// Per-row reciprocals RN(1/b) of the sweep-constant denominators of the tracer update (ignored
+// by DivIEEE, whose divr divides).
 template <class T>
 struct RowRcp {
     T dx, dz_k, sum_kp, sum_km, zd_kp, zd_km;
@@ -126,7 +126,7 @@ __device__ __forceinline__ T lflux_z(T vel, T s_m1, T s_0, T s_p1, T s_p2, int k
 
 // The tracer update of one cell (moist.jl:1479-1515) from values already gathered: the same
 // operations, in the same order, as tracer_cell in kernels.cuh, with the division policy D
-// (DivIEEE, or DivMarkstein which sets `bad` when a quotient might differ from IEEE division).
+// (DivIEEE: plain IEEE division; used for Float64 and for the cells the fast cell leaves).
 template <class D, class T>
 __device__ __forceinline__ T tracer_cell_t(const DevParams<T>& p, int k, T dt_stage, T s_c, T s_ip1, T s_ip2,
                                            T s_kp1, T s_kp2, T s_im1, T s_im2, T s_km1, T s_km2, T lin_km1,
@@ -184,10 +184,10 @@ __device__ __forceinline__ float koren_f(float r) {  // moist.jl:846
 
 // (pos || neg) is |vel| > EPS: both are false for a NaN velocity
 template <class D>
-__device__ __forceinline__ float lflux_x_f(float vel, float s_m1, float s_0, float s_p1, float s_p2, float EPS) {
+__device__ __forceinline__ float lflux_x_f(float vel, float s_m1, float s_0, float s_p1, float s_p2, float EPS, unsigned& g) {
     const float r_num = sel_gt(vel, EPS, s_p1 - s_0, s_0 - s_p1);
     const float r_den = sel_gt(vel, EPS, s_0 - s_m1, s_p1 - s_p2);
-    const float r = sel_lt(fabsf(r_den), EPS, 1.0f, D::vdiv(r_num, r_den));
+    const float r = sel_lt(fabsf(r_den), EPS, 1.0f, D::vdiv(r_num, r_den, g));
     const float lim = sel_gt(vel, EPS, s_0, s_p1) + 0.5f * koren_f<D>(r) * r_den;
     const float cen = 0.5f * (s_0 + s_p1);
     return sel_gt(fabsf(vel), EPS, lim, cen) * vel;
@@ -197,12 +197,12 @@ __device__ __forceinline__ float lflux_x_f(float vel, float s_m1, float s_0, flo
 template <class D>
 __device__ __forceinline__ float lflux_z_f(float vel, float s_m1, float s_0, float s_p1, float s_p2, unsigned at0,
                                            unsigned atnm2, float dz_a, float dz_b, float sum_ab, typename D::R rsum_ab, float cl,
-                                           float EPS) {
-    const float f2 = D::cdiv(s_0 * dz_b + s_p1 * dz_a, sum_ab, rsum_ab);
+                                           float EPS, unsigned& g) {
+    const float f2 = D::cdiv(s_0 * dz_b + s_p1 * dz_a, sum_ab, rsum_ab, g);
     const float clamp = jmin_f(f2, cl);
     const float r_num = sel_gt(vel, EPS, s_p1 - s_0, s_0 - s_p1);
     const float r_den = sel_gt(vel, EPS, s_0 - s_m1, s_p1 - s_p2);
-    const float r = sel_lt(fabsf(r_den), EPS, 1.0f, D::vdiv(r_num, r_den));
+    const float r = sel_lt(fabsf(r_den), EPS, 1.0f, D::vdiv(r_num, r_den, g));
     const float half = 0.5f * koren_f<D>(r) * r_den;
     const float lim = sel_gt(vel, EPS, s_0 + half, s_p1 - half);
     // pos: kk == 0 takes the clamp; neg: kk == nz-2 takes it; neither: the face average f2
@@ -211,68 +211,57 @@ __device__ __forceinline__ float lflux_z_f(float vel, float s_m1, float s_0, flo
     return face * vel;
 }
 
-// per-lane (row) constants of the fast cell (reciprocals in the policy's type); flags are 0 / 1
-template <class D>
+// per-lane (row) constants of the fast cell (reciprocals in the policy's type R); flags are 0 / 1
+template <class R>
 struct FastRow {
-    using R = typename D::R;
     float dx, dz_k, dz_kp1, dz_km1, sum_kp, sum_km, zd_kp, zd_km;
     R rdx, rdz_k, rsum_kp, rsum_km, rzd_kp, rzd_km;
     float kappa, EPS, dt_stage;
     unsigned k0, ke, kp_at0, kp_atnm2, km_at0, km_atnm2;
 };
 
-// v is tiny (nonzero, below 2^-100), huge (2^100 or more), infinite or NaN
-__device__ __forceinline__ bool numer_bad(float v) { return tiny_nz(v) | !(fabsf(v) < 0x1p100f); }
-
 template <class D>
-__device__ __forceinline__ float tracer_cell_f(const FastRow<D>& w, float s_c, float s_ip1, float s_ip2, float s_kp1,
+__device__ __forceinline__ float tracer_cell_f(const FastRow<typename D::R>& w, float s_c, float s_ip1, float s_ip2, float s_kp1,
                                                float s_kp2, float s_im1, float s_im2, float s_km1, float s_km2,
                                                float cl_kp, float cl_km, float mfx_i, float mfx_im, float mfz_k,
                                                float mfz_km, float rho_c, float rho_ip, float rho_im, float rho_kp,
-                                               float rho_km, float q0, float dph, bool& bad) {
-    const float fx_ip = lflux_x_f<D>(mfx_i, s_im1, s_c, s_ip1, s_ip2, w.EPS);
-    const float fx_im = lflux_x_f<D>(mfx_im, s_im2, s_im1, s_c, s_ip1, w.EPS);
+                                               float rho_km, float q0, float dph, unsigned& g, bool& bad) {
+    const float fx_ip = lflux_x_f<D>(mfx_i, s_im1, s_c, s_ip1, s_ip2, w.EPS, g);
+    const float fx_im = lflux_x_f<D>(mfx_im, s_im2, s_im1, s_c, s_ip1, w.EPS, g);
     const float ndx = fx_ip - fx_im;
-    const float adv_x = D::cdiv(ndx, w.dx, w.rdx);
+    const float adv_x = D::cdiv(ndx, w.dx, w.rdx, g);
     const float fz_kp = sel_u(w.ke, 0.0f,
                               lflux_z_f<D>(mfz_k, s_km1, s_c, s_kp1, s_kp2, w.kp_at0, w.kp_atnm2, w.dz_k, w.dz_kp1,
-                                        w.sum_kp, w.rsum_kp, cl_kp, w.EPS));
+                                        w.sum_kp, w.rsum_kp, cl_kp, w.EPS, g));
     const float fz_km = sel_u(w.k0, 0.0f,
                               lflux_z_f<D>(mfz_km, s_km2, s_km1, s_c, s_kp1, w.km_at0, w.km_atnm2, w.dz_km1, w.dz_k,
-                                        w.sum_km, w.rsum_km, cl_km, w.EPS));
+                                        w.sum_km, w.rsum_km, cl_km, w.EPS, g));
     const float ndz = fz_kp - fz_km;
-    const float adv_z = D::cdiv(ndz, w.dz_k, w.rdz_k);
+    const float adv_z = D::cdiv(ndz, w.dz_k, w.rdz_k, g);
     const float advection = -(adv_x + adv_z);
     const float scalar_kp = sel_u(w.ke, 0.0f, s_kp1);
     const float scalar_km = sel_u(w.k0, 0.0f, s_km1);
-    const float dsdx_ip = D::cdiv((rho_ip + rho_c) * 0.5f * (s_ip1 - s_c), w.dx, w.rdx);
-    const float dsdx_im = D::cdiv((rho_c + rho_im) * 0.5f * (s_c - s_im1), w.dx, w.rdx);
+    const float dsdx_ip = D::cdiv((rho_ip + rho_c) * 0.5f * (s_ip1 - s_c), w.dx, w.rdx, g);
+    const float dsdx_im = D::cdiv((rho_c + rho_im) * 0.5f * (s_c - s_im1), w.dx, w.rdx, g);
     const float kx = w.kappa * (dsdx_ip - dsdx_im);
-    const float diff_x = D::cdiv(kx, w.dx, w.rdx);
+    const float diff_x = D::cdiv(kx, w.dx, w.rdx, g);
     const float dsdz_kp = sel_u(w.ke, 0.0f,
-                                D::cdiv(D::cdiv(rho_kp * w.dz_k + rho_c * w.dz_kp1, w.sum_kp, w.rsum_kp) * (scalar_kp - s_c),
-                                    w.zd_kp, w.rzd_kp));
+                                D::cdiv(D::cdiv(rho_kp * w.dz_k + rho_c * w.dz_kp1, w.sum_kp, w.rsum_kp, g) * (scalar_kp - s_c),
+                                        w.zd_kp, w.rzd_kp, g));
     const float dsdz_km = sel_u(w.k0, 0.0f,
-                                D::cdiv(D::cdiv(rho_c * w.dz_km1 + rho_km * w.dz_k, w.sum_km, w.rsum_km) * (s_c - scalar_km),
-                                    w.zd_km, w.rzd_km));
+                                D::cdiv(D::cdiv(rho_c * w.dz_km1 + rho_km * w.dz_k, w.sum_km, w.rsum_km, g) * (s_c - scalar_km),
+                                        w.zd_km, w.rzd_km, g));
     const float kz = w.kappa * (dsdz_kp - dsdz_km);
-    const float diff_z = D::cdiv(kz, w.dz_k, w.rdz_k);
+    const float diff_z = D::cdiv(kz, w.dz_k, w.rdz_k, g);
     const float diffusion = diff_x + diff_z;
     const float q = q0 + w.dt_stage * (advection + diffusion + dph);
-    if constexpr (D::kGuarded)
-        bad = !(s_range(s_im1) & s_range(s_im2) & s_range(s_km1) & s_range(s_km2)) | numer_bad(ndx) |
-              numer_bad(ndz) | numer_bad(kx) | numer_bad(kz) | numer_bad(q);
-    else  // exact for every input; a non-finite result is left to IEEE division all the same
-        bad = !(fabsf(q) <= 0x1.fffffep127f);
+    bad = !(fabsf(q) <= 0x1.fffffep127f);  // non-finite results are left to IEEE division
     return q;
 }
 
 // q0, the phys tendency and the results are staged in shared memory for Float32; Float64
 // reads and writes them in global memory so that enough tiles stay resident
-#ifndef MOIST_FAST_DIV
-#define MOIST_FAST_DIV Div64
-#endif
-using FastDiv = MOIST_FAST_DIV;  // division policy of the Float32 fast cell (fastdiv.cuh)
+using FastDiv = Div64;  // division policy of the Float32 fast cell (fastdiv.cuh); Div64X for its fallback
 
 template <class T>
 struct TileQ {
@@ -297,8 +286,6 @@ struct TileSmem {
     T lin[3][TT_S + 1];      // per tracer: column 1 of the reference array (interior nx-2), rows z0-1 .. z0+33
     T strip_out[3][4][TT_W]; // per tracer: right strip cols x0+30, x0+31 (0, 1), top strip rows z0+30, z0+31 (2, 3)
     T cl[3][2][2][TT_W];     // per tracer: clamp quotients of the vertical limiter [kp, km][low, high row][column]
-    unsigned okm[3][TT_W];   // per tracer and row: bit c set when cell c's stage-start stencil allows the fast cell
-    int tile_ok;             // the tile's densities (and EPS > 0) allow the fast cell
 };
 
 // strips in global memory: [parity][tracer][tile][4][32]
@@ -338,14 +325,6 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
         const int k = z0 - 1 + rr, i = x0 + cc;
         sm.mz[rr][cc] = (k >= 0 && k < nz && i < nx) ? a.mfz[MOIST_IDX(k, i)] : T(0);
     }
-    bool rho_ok = true;  // Float32 fast cell: densities inside [2^-20, 2^21)
-    if constexpr (kStageQ<T>) {
-        for (int j = threadIdx.x; j < TT_S * TT_S; j += blockDim.x) rho_ok &= d_range((&sm.rho[0][0])[j]);
-    }
-    if constexpr (kStageQ<T>) {
-        const int all = __syncthreads_and((int)(rho_ok && p.EPS > T(0)));
-        if (threadIdx.x == 0) sm.tile_ok = all;
-    }
     for (int t = 0; t < 3; t++) {
         const T* qo = a.q_old[t];
         for (int j = threadIdx.x; j < TT_S * TT_S; j += blockDim.x) {
@@ -376,15 +355,6 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
     __syncthreads();
     const int t = warp;  // this warp's tracer
     if constexpr (kStageQ<T>) {
-        // per-cell stencil check: s at (r, c), (r, c+1), (r, c+2), (r+1, c), (r+2, c)
-        const int r = lane;
-        unsigned m = 0;
-        for (int c = 0; c < TT_W; c++) {
-            const bool ok = s_range(sm.s[t][r][c]) & s_range(sm.s[t][r][c + 1]) & s_range(sm.s[t][r][c + 2]) &
-                            s_range(sm.s[t][r + 1][c]) & s_range(sm.s[t][r + 2][c]);
-            m |= (unsigned)ok << c;
-        }
-        sm.okm[t][r] = m;
         // the clamp quotients lin / (+-vel dt) of limited_flux_z on the four rows that can use them:
         // face k+1/2 from rows k = 0 and nz-2, face k-1/2 from rows k = 1 and nz-1 (IEEE division)
         const int c = lane;
@@ -437,8 +407,7 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
     rr.sum_km = T(1) / (dz_km1 + dz_k);
     rr.zd_kp = T(1) / (z_kp1 - z_k);
     rr.zd_km = T(1) / (z_k - z_km1);
-    FastRow<FastDiv> fw{};
-    bool lane_fast = false;
+    FastRow<FastDiv::R> fw{};
     if constexpr (kStageQ<T>) {
         fw.dx = p.dx;
         fw.dz_k = dz_k;
@@ -463,10 +432,6 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
         fw.kp_atnm2 = k == nz - 2;
         fw.km_at0 = k - 1 == 0;
         fw.km_atnm2 = k - 1 == nz - 2;
-        // the constants of the faces this row has (none above the top row, none below row 0)
-        lane_fast = !FastDiv::kGuarded || (sm.tile_ok && d_range(fw.dx) && d_range(fw.dz_k) &&
-                    (fw.ke || (d_range(fw.dz_kp1) && d_range(fw.sum_kp) && d_range(fw.zd_kp))) &&
-                    (fw.k0 || (d_range(fw.dz_km1) && d_range(fw.sum_km) && d_range(fw.zd_km))));
     }
     const int width = min(TT_W, nx - x0);
     const T* q0 = a.q0[t];
@@ -529,7 +494,6 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
                 const T* bot1 = sm.bot[t][1];
                 const T* cl_kp = sm.cl[t][0][k == 0 ? 0 : 1];
                 const T* cl_km = sm.cl[t][1][k == 1 ? 0 : 1];
-                const unsigned okm = FastDiv::kGuarded ? (lane_fast ? sm.okm[t][r] : 0u) : ~0u;
                 for (int step = 0; step < nsteps; step++) {
                     const int c_raw = step - r;
                     const bool active = row_ok && c_raw >= 0 && c_raw < width;
@@ -543,16 +507,31 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
                     const T q0_c = sm.q.q0[t][r][c], dph_c = sm.q.dph[t][r][c];
                     const T rho_c = sm.rho[r + 1][c + 1];
                     bool bad;
+                    unsigned g = ~0u;
                     T qn_v = tracer_cell_f<FastDiv>(fw, sm.s[t][r][c], sm.s[t][r][c + 1], sm.s[t][r][c + 2], sm.s[t][r + 1][c],
                                            sm.s[t][r + 2][c], prev1, prev2, s_km1, s_km2, cl_kp[c], cl_km[c],
                                            sm.mx[r][c + 1], sm.mx[r][c], sm.mz[r + 1][c], sm.mz[r][c], rho_c,
                                            sm.rho[r + 1][c + 2], sm.rho[r + 1][c], sm.rho[r + 2][c + 1], sm.rho[r][c + 1],
-                                           q0_c, dph_c, bad);
-                    T sn = FastDiv::cdiv(qn_v, rho_c, sm.q.rrho[r][c]);
-                    if (active && (bad || !((okm >> c) & 1u))) {
-                        bool unused = false;
-                        qn_v = MOIST_TILE_CELL(DivIEEE<T>, unused);
-                        sn = qn_v / rho_c;
+                                           q0_c, dph_c, g, bad);
+                    T sn = FastDiv::cdiv(qn_v, rho_c, sm.q.rrho[r][c], g);
+                    bad |= guard_hit(g);
+                    if (active && bad) {
+                        // a subnormal-range quotient or a non-finite result: the same cell with
+                        // subnormal quotients rounded explicitly (exact for every input), and
+                        // IEEE division if the result is still not finite
+                        unsigned g2 = ~0u;
+                        bool bad2;
+                        qn_v = tracer_cell_f<Div64X>(fw, sm.s[t][r][c], sm.s[t][r][c + 1], sm.s[t][r][c + 2],
+                                                     sm.s[t][r + 1][c], sm.s[t][r + 2][c], prev1, prev2, s_km1, s_km2,
+                                                     cl_kp[c], cl_km[c], sm.mx[r][c + 1], sm.mx[r][c], sm.mz[r + 1][c],
+                                                     sm.mz[r][c], rho_c, sm.rho[r + 1][c + 2], sm.rho[r + 1][c],
+                                                     sm.rho[r + 2][c + 1], sm.rho[r][c + 1], q0_c, dph_c, g2, bad2);
+                        sn = Div64X::cdiv(qn_v, rho_c, sm.q.rrho[r][c], g2);
+                        if (bad2) {
+                            bool unused = false;
+                            qn_v = MOIST_TILE_CELL(DivIEEE<T>, unused);
+                            sn = qn_v / rho_c;
+                        }
                     }
                     if (active) {
                         sm.q.qn[t][r][c] = qn_v;
