@@ -968,6 +968,95 @@ __global__ void k_prec(DevParams<T> p, T* prec, const T* d_prec, const int* err)
     prec[i] = prec[i] + d_prec[i] * p.dt;
 }
 
+// ----------------------------------------------------------------------------- budgets
+//
+// Domain budgets as compensated FP64 sums (Neumaier's variant of Kahan summation; the library
+// is built with --fmad=false, so the error terms are formed exactly). Per cell: mass rho dz dx,
+// water (rho_qv + rho_qc + rho_qr) dz dx, and total energy (kinetic + potential + internal,
+// each formed in the state precision exactly as output_history forms eng_k, eng_p, eng_i,
+// moist.jl:1797-1841) times dz dx; per column: accumulated rain prec dx. A fixed grid of
+// BUDGET_BLOCKS blocks, a fixed per-thread order, a fixed tree inside each block and a final
+// sequential merge make the result reproducible bit for bit.
+
+constexpr int BUDGET_BLOCKS = 256, BUDGET_THREADS = 256;
+
+struct CSum {
+    double s, c;  // running sum and the accumulated rounding errors
+};
+__device__ __forceinline__ void cs_add(CSum& a, double x) {
+    const double t = a.s + x;
+    a.c += fabs(a.s) >= fabs(x) ? (a.s - t) + x : (x - t) + a.s;
+    a.s = t;
+}
+__device__ __forceinline__ void cs_merge(CSum& a, const CSum& b) {
+    cs_add(a, b.s);
+    a.c += b.c;
+}
+
+// energy density of one cell in the state precision (moist.jl:1799-1841)
+template <class T>
+__device__ __forceinline__ T cell_energy(const DevParams<T>& p, const StateP<T>& s, int k, int i) {
+    const int nx = p.nx, P = p.P;
+    const size_t c = MOIST_IDX(k, i);
+    const T rho = s.rho[c];
+    const T rho_inv = T(1.0) / rho;
+    const T theta = s.rt[c] * rho_inv;
+    const T qv = s.qv[c] * rho_inv, qc = s.qc[c] * rho_inv, qr = s.qr[c] * rho_inv;
+    const T qt = qv + qc + qr;
+    const T qd = T(1.0) - qt;
+    const T r = p.Rd * qd + p.Rv * qv;
+    const T cp = p.Cpd * qd + p.Cpv * qv + p.Cpl * (qc + qr);
+    const T cv = cp - r;
+    const T pi = mm::mpow(r * s.rt[c] / p.P0, r / cv);
+    const T temp = theta * pi;
+    const T u = (s.ru[c] + s.ru[MOIST_IDX(k, wrapx(i - 1, nx))]) * T(0.5) * rho_inv;
+    const T w = k > 0 ? (s.rw[c] + s.rw[c - P]) * T(0.5) * rho_inv : s.rw[c] * T(0.5) * rho_inv;
+    const T eng_k = T(0.5) * rho * (u * u + w * w);
+    const T eng_p = rho * p.GRAV * p.z[k];
+    const T eng_i = rho * (cv * temp + qv * p.Lv);
+    return eng_k + eng_p + eng_i;
+}
+
+// the four sums of one block; out[blockIdx.x][4] pairs
+template <class T>
+__global__ void __launch_bounds__(BUDGET_THREADS) k_budget(DevParams<T> p, StateP<T> s, const T* prec, CSum* out) {
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    CSum acc[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    const double dx = (double)p.dx;
+    const long long n = (long long)nx * nz;
+    for (long long e = blockIdx.x * (long long)BUDGET_THREADS + threadIdx.x; e < n;
+         e += (long long)BUDGET_BLOCKS * BUDGET_THREADS) {
+        const int k = (int)(e / nx), i = (int)(e - (long long)k * nx);
+        const size_t c = MOIST_IDX(k, i);
+        const double vol = (double)p.dz[k] * dx;
+        cs_add(acc[0], (double)s.rho[c] * vol);
+        cs_add(acc[1], ((double)s.qv[c] + (double)s.qc[c] + (double)s.qr[c]) * vol);
+        const T e_kpi = cell_energy(p, s, k, i);
+        cs_add(acc[2], (double)e_kpi * vol);
+    }
+    for (int i = blockIdx.x * BUDGET_THREADS + threadIdx.x; i < nx; i += BUDGET_BLOCKS * BUDGET_THREADS)
+        cs_add(acc[3], (double)prec[i] * dx);
+    __shared__ CSum part[4][BUDGET_THREADS];
+    for (int q = 0; q < 4; q++) part[q][threadIdx.x] = acc[q];
+    __syncthreads();
+    for (int h = BUDGET_THREADS / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h)
+            for (int q = 0; q < 4; q++) cs_merge(part[q][threadIdx.x], part[q][threadIdx.x + h]);
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) out[blockIdx.x * 4 + threadIdx.x] = part[threadIdx.x][0];
+}
+
+// sequential merge of the block sums: res = {mass, water + rain, energy, rain}
+__global__ void k_budget_final(const CSum* part, double* res) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    CSum tot[4] = {{0, 0}, {0, 0}, {0, 0}, {0, 0}};
+    for (int b = 0; b < BUDGET_BLOCKS; b++)
+        for (int q = 0; q < 4; q++) cs_merge(tot[q], part[b * 4 + q]);
+    cs_merge(tot[1], tot[3]);
+    for (int q = 0; q < 4; q++) res[q] = tot[q].s + tot[q].c;
+}
+
 // ----------------------------------------------------------------------------- layout moves
 
 // (ka, ia) column-major host layout <-> [nz][P] interior device layout, through a 32x32 tile

@@ -153,6 +153,8 @@ struct Ctx : CtxBase {
     T *g_dz, *g_z, *g_zf;
     T* staging;
     int* err;
+    CSum* bud_part;   // [BUDGET_BLOCKS][4] block sums of the budgets
+    double* bud_res;  // [4]
     bool rd_dirty = true;
     // tiled tracer sweep (tracer_tiles.cuh)
     bool use_tiles = false;
@@ -242,6 +244,8 @@ struct Ctx : CtxBase {
         AL(g_zf, (size_t)nz);
         AL(staging, (size_t)nz * (nx + 2 * halo) + 32);
         AL(err, 4);  // [0] halt (NaN field), [1] pending NaN field, [2] timeout, [3] spare
+        AL(bud_part, (size_t)BUDGET_BLOCKS * 4);
+        AL(bud_res, 4);
         CK(cudaMemcpyAsync(g_dz, c->dz, nz * sizeof(T), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(g_z, c->z, nz * sizeof(T), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(g_zf, c->zf, nz * sizeof(T), cudaMemcpyHostToDevice, st));
@@ -704,8 +708,15 @@ struct Ctx : CtxBase {
         return finish();
     }
 
+    // compensated FP64 domain budgets of the current state (kernels.cuh, k_budget)
     int budget(double out[4]) override {
-        return set_err(owner, MOIST_ERR_UNSUPPORTED, "budget not available yet");
+        k_budget<T><<<BUDGET_BLOCKS, BUDGET_THREADS, 0, st>>>(dp, cur, prec, bud_part);
+        CKL();
+        k_budget_final<<<1, 32, 0, st>>>(bud_part, bud_res);
+        CKL();
+        CK(cudaMemcpyAsync(out, bud_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return MOIST_OK;
     }
 };
 

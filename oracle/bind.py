@@ -41,6 +41,7 @@ def lib():
         L.oracle_exchange_halo.argtypes = [P, I, V]
         L.oracle_solve_tridiagonal.argtypes = [I, I, V, V, V, V]
         L.oracle_invert_T_for_thetae.argtypes = [P, I, D, D, D, C.POINTER(D)]
+        L.oracle_budget_terms.argtypes = [P, I, S, V, V, V, V]
         for f in ("oracle_exp_d", "oracle_log_d"):
             getattr(L, f).argtypes = [D]
             getattr(L, f).restype = D
@@ -55,6 +56,17 @@ def _check(rc):
         raise ValueError("oracle: invalid argument")
     if rc >= 0:
         raise FloatingPointError("NaN detected in " + NAN_FIELDS[rc])
+
+
+def budget_terms(s, p):
+    """Per-cell budget terms (mass, water, energy; (nz, nx) doubles) and per-column rain (nx,),
+    to be summed exactly (math.fsum) for the compensated sums of moist_budget."""
+    cp = p.to_c()
+    h = s.to_c()
+    out = [np.zeros((p.Nz, p.Nx)) for _ in range(3)] + [np.zeros(p.Nx)]
+    _check(lib().oracle_budget_terms(C.byref(cp), p.precision, C.byref(h),
+                                     *[o.ctypes.data_as(C.c_void_p) for o in out]))
+    return out
 
 
 def rk3_step(s, p, nsteps=1, tri64=False):

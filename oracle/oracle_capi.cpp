@@ -193,9 +193,58 @@ int flux_t(const moist_params* cp, int dir, const void* scalar_rho, const void* 
     return -1;
 }
 
+// per-cell budget terms (the GPU's k_budget, kernels.cuh): mass and water per cell times
+// dz dx, the energy of output_history (moist.jl:1797-1841) formed in T times dz dx, rain per
+// column times dx; all as doubles, for an exactly rounded sum in the test
+template <class T>
+int budget_terms_t(const moist_params* cp, const moist_state_host* hs, double* mass, double* water,
+                   double* energy, double* rain) {
+    const Par<T> p = Par<T>::from_c(*cp);
+    State<T> s(p);
+    load(s, hs);
+    exchange_halo(s.rho_u.a(), p);  // u at the cell centres reads rho_u[k, i-1] (moist.jl:1799)
+    auto rho = s.rho.a(), ru = s.rho_u.a(), rw = s.rho_w.a(), rt = s.rho_theta.a();
+    auto rqv = s.rho_qv.a(), rqc = s.rho_qc.a(), rqr = s.rho_qr.a();
+    const double dx = (double)p.dx;
+    for (int k = 0; k < p.Nz; k++)
+        for (int j = 0; j < p.Nx; j++) {
+            const int i = p.is + j;
+            const size_t o = (size_t)k * p.Nx + j;
+            const double vol = (double)p.dz[k] * dx;
+            mass[o] = (double)rho(k, i) * vol;
+            water[o] = ((double)rqv(k, i) + (double)rqc(k, i) + (double)rqr(k, i)) * vol;
+            const T rho_inv = T(1.0) / rho(k, i);
+            const T theta = rt(k, i) * rho_inv;
+            const T qv = rqv(k, i) * rho_inv, qc = rqc(k, i) * rho_inv, qr = rqr(k, i) * rho_inv;
+            const T qt = qv + qc + qr;
+            const T qd = T(1.0) - qt;
+            const T r = p.Rd * qd + p.Rv * qv;
+            const T cp = p.Cpd * qd + p.Cpv * qv + p.Cpl * (qc + qr);
+            const T cv = cp - r;
+            const T pi = mm::mpow(r * rt(k, i) / p.P0, r / cv);
+            const T temp = theta * pi;
+            const T u = (ru(k, i) + ru(k, i - 1)) * T(0.5) * rho_inv;
+            const T w = k > 0 ? (rw(k, i) + rw(k - 1, i)) * T(0.5) * rho_inv : rw(k, i) * T(0.5) * rho_inv;
+            const T eng_k = T(0.5) * rho(k, i) * (u * u + w * w);
+            const T eng_p = rho(k, i) * p.GRAV * p.z[k];
+            const T eng_i = rho(k, i) * (cv * temp + qv * p.Lv);
+            energy[o] = (double)(eng_k + eng_p + eng_i) * vol;
+        }
+    for (int j = 0; j < p.Nx; j++) rain[j] = (double)s.prec[p.is + j] * dx;
+    return -1;
+}
+
 }  // namespace
 
 extern "C" {
+
+int oracle_budget_terms(const moist_params* cp, int prec, const moist_state_host* s, double* mass, double* water,
+                        double* energy, double* rain) {
+    if (!params_ok(cp) || !s || !mass || !water || !energy || !rain) return -2;
+    return prec == MOIST_F32 ? budget_terms_t<float>(cp, s, mass, water, energy, rain)
+                             : budget_terms_t<double>(cp, s, mass, water, energy, rain);
+}
+
 
 int oracle_rk3_step(const moist_params* cp, int prec, int tri64, moist_state_host* s, int nsteps) {
     if (!params_ok(cp) || !s) return -2;
