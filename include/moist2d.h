@@ -76,7 +76,10 @@ enum {
     MOIST_FLAG_TRI_NATIVE = 1,
     /* Run the tracer transport as one exact wavefront per tracer instead of the tiled sweep
      * (same results bit for bit, much slower; kept for cross-checking). */
-    MOIST_FLAG_TRACER_WAVEFRONT = 2
+    MOIST_FLAG_TRACER_WAVEFRONT = 2,
+    /* Run the tracer transport as one exact row-streaming wavefront per tracer (one thread per
+     * row; no repair passes; same results bit for bit). Needs nz <= 256. */
+    MOIST_FLAG_TRACER_STREAM = 4
 };
 
 /*
@@ -236,6 +239,31 @@ int moist_eval_helper(const moist_params* p, int precision, int helper, int n, c
  * out[2] = total energy (kinetic + potential + internal, the terms of moist.jl:1839-1852)*dx*dz,
  * out[3] = accumulated surface rain sum(prec*dx). */
 int moist_budget(moist_ctx* ctx, double out[4]);
+
+/* ---- Ensembles (no counterpart in the reference, which advances one domain per process).
+ * A batch advances nmembers independent domains together: members[i] are the members'
+ * parameters (each its own nx, nz, grid, dt and physics switches; ns, do_sf and do_rd must
+ * agree; halo = 2, nx >= 2, nz <= 256). Each large step is one launch per kernel of the step
+ * for all members, from a packed (member, block) work list, captured once as a CUDA graph; the
+ * tracer transport runs as the row-streaming wavefront (MOIST_FLAG_TRACER_STREAM). Every
+ * member's results equal those of a context stepping that member alone, bit for bit.
+ * flags: MOIST_FLAG_TRI_NATIVE as for moist_ctx_create. */
+typedef struct moist_batch moist_batch;
+int moist_batch_create(const moist_params* members, int nmembers, int precision, int flags, moist_batch** out);
+int moist_batch_destroy(moist_batch* b);
+/* the member's own context: upload, download, budget and the other per-context calls apply
+ * to it (its moist_rk3_step advances that member alone) */
+moist_ctx* moist_batch_member(moist_batch* b, int member);
+int moist_batch_upload(moist_batch* b, int member, const moist_state_host* s);
+int moist_batch_download(moist_batch* b, int member, moist_state_host* s);
+/* nsteps large steps of every member; a NaN in a member stops that member's work (the others
+ * continue) and returns MOIST_ERR_NAN, with the member in moist_batch_nan_member and the field
+ * in moist_nan_field(moist_batch_member(b, m)) */
+int moist_batch_step(moist_batch* b, int nsteps);
+/* nsteps large steps timed with CUDA events on the batch stream (no error check) */
+int moist_batch_time_steps(moist_batch* b, int nsteps, float* ms);
+const char* moist_batch_last_error(const moist_batch* b);
+int moist_batch_nan_member(const moist_batch* b);
 
 /* Kernel groups of one large step, for moist_step_profile. */
 enum {

@@ -15,7 +15,9 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_rain_sedimentation", "moist_implicit_correction", "moist_eval_helper",
            "moist_budget", "moist_stream", "moist_synchronize", "moist_time_steps",
            "moist_rk3_step_host", "moist_step_profile", "moist_set_device",
-           "moist_implicit_correction_noalloc", "moist_tracer_pass_counts")
+           "moist_implicit_correction_noalloc", "moist_tracer_pass_counts", "moist_batch_create",
+           "moist_batch_destroy", "moist_batch_member", "moist_batch_upload", "moist_batch_download",
+           "moist_batch_step", "moist_batch_time_steps", "moist_batch_last_error", "moist_batch_nan_member")
 
 
 def lib():
@@ -55,5 +57,17 @@ def lib():
                                                         C.c_size_t]
         L.moist_step_profile.argtypes = [Ctx, I, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                          C.POINTER(C.c_longlong)]
+        B = C.c_void_p
+        L.moist_batch_create.argtypes = [P, I, I, I, C.POINTER(B)]
+        L.moist_batch_destroy.argtypes = [B]
+        L.moist_batch_member.argtypes = [B, I]
+        L.moist_batch_member.restype = Ctx
+        L.moist_batch_upload.argtypes = [B, I, S]
+        L.moist_batch_download.argtypes = [B, I, S]
+        L.moist_batch_step.argtypes = [B, I]
+        L.moist_batch_time_steps.argtypes = [B, I, C.POINTER(C.c_float)]
+        L.moist_batch_last_error.argtypes = [B]
+        L.moist_batch_last_error.restype = C.c_char_p
+        L.moist_batch_nan_member.argtypes = [B]
         _lib = L
     return _lib

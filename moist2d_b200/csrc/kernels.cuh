@@ -32,10 +32,10 @@ __device__ __forceinline__ bool halted(const int* err) { return *(volatile const
 // reference's halo reads rho_u[ks, is-1] and rho[ks, ie+1], which hold the values of the
 // last halo exchange (start of the last RK stage), not the current interior.
 template <class T>
-__global__ void k_surface_fluxes(DevParams<T> p, StateP<T> s, const T* ru_left, const T* rho_right,
-                                 T* d_u_sf, T* d_th_sf, T* d_qv_sf, T* mflux, T* shflux, T* lhflux,
-                                 const int* err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_surface_fluxes(DevParams<T> p, StateP<T> s, const T* ru_left, const T* rho_right,
+                                                 T* d_u_sf, T* d_th_sf, T* d_qv_sf, T* mflux, T* shflux, T* lhflux,
+                                                 const int* err, int bx, int by) {
+    const int i = bx * blockDim.x + threadIdx.x;
     const int nx = p.nx;
     if (i >= nx || halted(err)) return;
     const T rho = s.rho[i], qv = s.qv[i] / rho, qc = s.qc[i] / rho, qr = s.qr[i] / rho;
@@ -67,6 +67,10 @@ __global__ void k_surface_fluxes(DevParams<T> p, StateP<T> s, const T* ru_left, 
     d_qv_sf[i] = lh / p.dz[0];
     lhflux[i] = lh * p.Lv;
 }
+template <class T>
+__global__ void k_surface_fluxes(DevParams<T> p, StateP<T> s, const T* ru_left, const T* rho_right,                                  T* d_u_sf, T* d_th_sf, T* d_qv_sf, T* mflux, T* shflux, T* lhflux,                                  const int* err) {
+    b_surface_fluxes(p, s, ru_left, rho_right, d_u_sf, d_th_sf, d_qv_sf, mflux, shflux, lhflux, err, blockIdx.x, blockIdx.y);
+}
 
 template <class T>
 __device__ __forceinline__ T tanh_m(T x) {  // tanh from the shared exp
@@ -76,9 +80,9 @@ __device__ __forceinline__ T tanh_m(T x) {  // tanh from the shared exp
 
 // gray_radiation! (moist.jl:776-840), one thread per column; LW_up / LW_dn scratch [nz+1][P]
 template <class T>
-__global__ void k_gray_radiation(DevParams<T> p, StateP<T> s, const T* theta_ref, T* lw_up,
-                                 T* lw_dn, T* d_th_rd, const int* err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_gray_radiation(DevParams<T> p, StateP<T> s, const T* theta_ref, T* lw_up, T* lw_dn,
+                                                 T* d_th_rd, const int* err, int bx, int by) {
+    const int i = bx * blockDim.x + threadIdx.x;
     const int nx = p.nx, nz = p.nz, P = p.P;
     if (i >= nx || halted(err)) return;
     auto col = [&](int k, T& cpk, T& pik, T& tempk, T& epsk, T& tauk) {
@@ -125,15 +129,19 @@ __global__ void k_gray_radiation(DevParams<T> p, StateP<T> s, const T* theta_ref
         d_th_rd[c] = hr + cr;
     }
 }
+template <class T>
+__global__ void k_gray_radiation(DevParams<T> p, StateP<T> s, const T* theta_ref, T* lw_up,                                  T* lw_dn, T* d_th_rd, const int* err) {
+    b_gray_radiation(p, s, theta_ref, lw_up, lw_dn, d_th_rd, err, blockIdx.x, blockIdx.y);
+}
 
 // Kessler microphysics + rain sedimentation + assembly of the six phys tendencies
 // (moist.jl:1593-1644), one thread per cell.
 template <class T>
-__global__ void k_physics(DevParams<T> p, StateP<T> s, T* d_th_mp, T* d_qv_mp, T* d_qc_mp, T* d_qr_mp,
-                          T* d_qr_sed, T* d_prec, const T* d_th_rd, const T* d_u_sf, const T* d_th_sf,
-                          const T* d_qv_sf, PhysP<T> ph, const int* err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void b_physics(DevParams<T> p, StateP<T> s, T* d_th_mp, T* d_qv_mp, T* d_qc_mp, T* d_qr_mp,
+                                          T* d_qr_sed, T* d_prec, const T* d_th_rd, const T* d_u_sf, const T* d_th_sf,
+                                          const T* d_qv_sf, PhysP<T> ph, const int* err, int bx, int by) {
+    const int i = bx * blockDim.x + threadIdx.x;
+    const int k = by * blockDim.y + threadIdx.y;
     const int nx = p.nx, nz = p.nz, P = p.P;
     if (i >= nx || k >= nz || halted(err)) return;
     const size_t c = MOIST_IDX(k, i);
@@ -172,15 +180,19 @@ __global__ void k_physics(DevParams<T> p, StateP<T> s, T* d_th_mp, T* d_qv_mp, T
     ph.d_qc[c] = dqc;
     ph.d_qr[c] = dqr + sed;
 }
+template <class T>
+__global__ void k_physics(DevParams<T> p, StateP<T> s, T* d_th_mp, T* d_qv_mp, T* d_qc_mp, T* d_qr_mp,                           T* d_qr_sed, T* d_prec, const T* d_th_rd, const T* d_u_sf, const T* d_th_sf,                           const T* d_qv_sf, PhysP<T> ph, const int* err) {
+    b_physics(p, s, d_th_mp, d_qv_mp, d_qc_mp, d_qr_mp, d_qr_sed, d_prec, d_th_rd, d_u_sf, d_th_sf, d_qv_sf, ph, err, blockIdx.x, blockIdx.y);
+}
 
 // ----------------------------------------------------------------------------- stage prologue
 
 // diagnostics (moist.jl:1048-1062) and face velocities u_face, w_face (1091-1097, 1185-1189)
 template <class T>
-__global__ void k_diag(DevParams<T> p, StateP<T> s, T* pres, T* theta, T* rt2pres, T* u_face,
-                       T* w_face, const int* err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void b_diag(DevParams<T> p, StateP<T> s, T* pres, T* theta, T* rt2pres, T* u_face,
+                                       T* w_face, const int* err, int bx, int by) {
+    const int i = bx * blockDim.x + threadIdx.x;
+    const int k = by * blockDim.y + threadIdx.y;
     const int nx = p.nx, nz = p.nz, P = p.P;
     if (i >= nx || k >= nz || halted(err)) return;
     const size_t c = MOIST_IDX(k, i);
@@ -198,6 +210,10 @@ __global__ void k_diag(DevParams<T> p, StateP<T> s, T* pres, T* theta, T* rt2pre
     u_face[c] = s.ru[c] * T(2.0) / (rho + s.rho[MOIST_IDX(k, ip)]);
     if (k < nz - 1) w_face[c] = s.rw[c] / f2h(rho, s.rho[c + P], p.dz[k], p.dz[k + 1]);
 }
+template <class T>
+__global__ void k_diag(DevParams<T> p, StateP<T> s, T* pres, T* theta, T* rt2pres, T* u_face,                        T* w_face, const int* err) {
+    b_diag(p, s, pres, theta, rt2pres, u_face, w_face, err, blockIdx.x, blockIdx.y);
+}
 
 template <class T>
 struct TendArgs {
@@ -212,9 +228,9 @@ struct TendArgs {
 // slow tendencies R_rho, R_rho_u, R_rho_w, R_rho_theta (moist.jl:1079-1332), perturbation
 // initialisation and the saved momentum fluxes (1339-1348)
 template <class T>
-__global__ void k_tend(DevParams<T> p, TendArgs<T> a, const int* err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void b_tend(DevParams<T> p, TendArgs<T> a, const int* err, int bx, int by) {
+    const int i = bx * blockDim.x + threadIdx.x;
+    const int k = by * blockDim.y + threadIdx.y;
     const int nx = p.nx, nz = p.nz, P = p.P;
     if (i >= nx || k >= nz || halted(err)) return;
     const T EPS = p.EPS, dx = p.dx, GRAV = p.GRAV;
@@ -411,6 +427,10 @@ __global__ void k_tend(DevParams<T> p, TendArgs<T> a, const int* err) {
     a.rt_p[c] = a.s0.rt[c] - a.s.rt[c];
     a.mfx[c] = ru[c];
     a.mfz[c] = rw[c];
+}
+template <class T>
+__global__ void k_tend(DevParams<T> p, TendArgs<T> a, const int* err) {
+    b_tend(p, a, err, blockIdx.x, blockIdx.y);
 }
 
 // Per-stage factorisation of the w-p tridiagonal system (implicit_correction!, moist.jl:
@@ -628,13 +648,13 @@ struct StripSmem {
 // k_thomas_factors over a strip: the coefficients of all rows in parallel, then the pivot
 // recurrence per column
 template <class T, class TT>
-__global__ void __launch_bounds__(STRIP_THREADS) k_thomas_strip(DevParams<T> p, const T* theta, const T* rt2pres,
-                                                                 T dt_s, int wc, T* ta, T* tb, T* tc, TT* tcp,
-                                                                 TT* tpiv, const int* err) {
+__device__ __forceinline__ void b_thomas_strip(DevParams<T> p, const T* theta, const T* rt2pres, T dt_s, int wc,
+                                               T* ta, T* tb, T* tc, TT* tcp, TT* tpiv, const int* err, int bx,
+                                               int by) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (halted(err)) return;
     const int nx = p.nx, nz = p.nz, P = p.P;
-    const int i0 = blockIdx.x * wc, ncol = min(wc, nx - i0);
+    const int i0 = bx * wc, ncol = min(wc, nx - i0);
     const int ke = nz - 1, n = nz - 1;
     const T* dz = p.dz;
     const T* z = p.z;
@@ -683,15 +703,19 @@ __global__ void __launch_bounds__(STRIP_THREADS) k_thomas_strip(DevParams<T> p, 
         tpiv[MOIST_IDX(j, i)] = sm.piv[j * wc + col];
     }
 }
+template <class T, class TT>
+__global__ void __launch_bounds__(STRIP_THREADS) k_thomas_strip(DevParams<T> p, const T* theta, const T* rt2pres,                                                                  T dt_s, int wc, T* ta, T* tb, T* tc, TT* tcp,                                                                  TT* tpiv, const int* err) {
+    b_thomas_strip(p, theta, rt2pres, dt_s, wc, ta, tb, tc, tcp, tpiv, err, blockIdx.x, blockIdx.y);
+}
 
 // k_substep over a strip (moist.jl:1355-1459)
 template <class T, class TT>
-__global__ void __launch_bounds__(STRIP_THREADS) k_substep_strip(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T,
-                                                                  double fact_tp64, int wc, const int* err) {
+__device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T, double fact_tp64,
+                                                int wc, const int* err, int bx, int by) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (halted(err)) return;
     const int nx = p.nx, nz = p.nz, P = p.P;
-    const int i0 = blockIdx.x * wc, ncol = min(wc, nx - i0);
+    const int i0 = bx * wc, ncol = min(wc, nx - i0);
     const int ke = nz - 1, n = nz - 1;
     const T dx = p.dx, EPS = p.EPS;
     const T* dz = p.dz;
@@ -821,6 +845,10 @@ __global__ void __launch_bounds__(STRIP_THREADS) k_substep_strip(DevParams<T> p,
         if (k < ke) a.mfz[c] = a.mfz[c] + w_k / ns_T;
     }
 }
+template <class T, class TT>
+__global__ void __launch_bounds__(STRIP_THREADS) k_substep_strip(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T,                                                                   double fact_tp64, int wc, const int* err) {
+    b_substep_strip(p, a, dt_s, ns_T, fact_tp64, wc, err, blockIdx.x, blockIdx.y);
+}
 
 // ----------------------------------------------------------------------------- tracers
 
@@ -932,9 +960,9 @@ struct UpdArgs {
 
 // state update (moist.jl:1522-1539) and NaN checks (1542-1578)
 template <class T>
-__global__ void k_update(DevParams<T> p, UpdArgs<T> a, int* err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void b_update(DevParams<T> p, UpdArgs<T> a, int* err, int bx, int by) {
+    const int i = bx * blockDim.x + threadIdx.x;
+    const int k = by * blockDim.y + threadIdx.y;
     const int nx = p.nx, nz = p.nz, P = p.P;
     if (i >= nx || k >= nz || halted(err)) return;
     const size_t c = MOIST_IDX(k, i);
@@ -955,6 +983,10 @@ __global__ void k_update(DevParams<T> p, UpdArgs<T> a, int* err) {
         if (v[f] != v[f]) bad = f;
     if (bad != INT_MAX) atomicMin(err + 1, bad);  // err[1]: pending, promoted at stage end
 }
+template <class T>
+__global__ void k_update(DevParams<T> p, UpdArgs<T> a, int* err) {
+    b_update(p, a, err, blockIdx.x, blockIdx.y);
+}
 
 // promote the stage's NaN report (err[1]) to the halt word (err[0])
 __global__ void k_stage_end(int* err) {
@@ -962,10 +994,14 @@ __global__ void k_stage_end(int* err) {
 }
 
 template <class T>
-__global__ void k_prec(DevParams<T> p, T* prec, const T* d_prec, const int* err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_prec(DevParams<T> p, T* prec, const T* d_prec, const int* err, int bx, int by) {
+    const int i = bx * blockDim.x + threadIdx.x;
     if (i >= p.nx || halted(err)) return;
     prec[i] = prec[i] + d_prec[i] * p.dt;
+}
+template <class T>
+__global__ void k_prec(DevParams<T> p, T* prec, const T* d_prec, const int* err) {
+    b_prec(p, prec, d_prec, err, blockIdx.x, blockIdx.y);
 }
 
 // ----------------------------------------------------------------------------- budgets

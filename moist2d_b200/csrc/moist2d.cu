@@ -15,11 +15,24 @@
 
 #include "../../include/moist2d.h"
 #include "kernels.cuh"
-#include "tracer_tiles.cuh"
+#include "batch.cuh"
 
 using namespace moist;
 
 namespace {
+
+// the launches of one large step of a context, recorded instead of launched: per slot the
+// launch kind and the bytes of its argument struct (batch.cuh)
+struct StepRecord {
+    std::vector<int> kind;
+    std::vector<std::vector<unsigned char>> args;
+    template <class A>
+    void put(int k, const A& a) {
+        kind.push_back(k);
+        const unsigned char* b = reinterpret_cast<const unsigned char*>(&a);
+        args.emplace_back(b, b + sizeof(A));
+    }
+};
 
 struct CtxBase {
     virtual ~CtxBase() {}
@@ -36,6 +49,12 @@ struct CtxBase {
     virtual int pass_counts(int* counts, int n) = 0;
 };
 
+struct BatchBase {
+    virtual ~BatchBase() {}
+    virtual int step(int nsteps) = 0;
+    virtual int time_steps(int nsteps, float* ms) = 0;
+};
+
 }  // namespace
 
 struct moist_ctx {
@@ -46,6 +65,16 @@ struct moist_ctx {
     std::string err;
     int nan_field = -1;
     CtxBase* impl = nullptr;
+};
+
+struct moist_batch {
+    int device = 0;
+    int precision = MOIST_F32;
+    cudaStream_t stream = nullptr;
+    std::vector<moist_ctx*> members;
+    std::string err;
+    int nan_member = -1, nan_field = -1;
+    BatchBase* impl = nullptr;
 };
 
 namespace {
@@ -75,6 +104,8 @@ int set_err(moist_ctx* c, int code, const char* fmt, ...) {
     } while (0)
 
 inline unsigned cdiv(int a, int b) { return (unsigned)((a + b - 1) / b); }
+
+#define SINGLE_ARG(...) __VA_ARGS__
 
 template <class T>
 DevParams<T> make_params(const moist_params* c, int P) {
@@ -162,6 +193,12 @@ struct Ctx : CtxBase {
     T* strips = nullptr;
     int* pass_hist = nullptr;  // [64] sweeps that converged after p passes
     size_t tile_smem = 0;
+    // when set, launch_step records its launches here instead of launching them
+    StepRecord* rec = nullptr;
+    // row-streaming tracer sweep (MOIST_FLAG_TRACER_STREAM)
+    bool use_stream = false;
+    T* s_old[3] = {nullptr, nullptr, nullptr};
+    double* rrho = nullptr;
     // column strips of the factorisation and the acoustic substeps
     int strip_wc = 1;
     size_t strip_smem = 0;
@@ -253,6 +290,14 @@ struct Ctx : CtxBase {
         dp.z = g_z;
         dp.zf = g_zf;
         if (int r = init_strips()) return r;
+        if (owner->flags & MOIST_FLAG_TRACER_STREAM) {
+            if (nz > STREAM_MAX_ROWS)
+                return set_err(owner, MOIST_ERR_UNSUPPORTED, "the streaming tracer sweep needs nz <= %d (got %d)",
+                               STREAM_MAX_ROWS, nz);
+            for (int t = 0; t < 3; t++) AL(s_old[t], fsz);
+            AL(rrho, fsz);
+            use_stream = true;
+        }
         if (int r = init_tiles()) return r;
         CK(reset_err());
         CK(cudaStreamSynchronize(st));
@@ -291,7 +336,7 @@ struct Ctx : CtxBase {
         tctl.ntiles = tctl.tiles_x * tctl.tiles_z;
         tctl.max_pass = tctl.tiles_x + tctl.tiles_z + 2;
         tile_smem = sizeof(TileSmem<T>);
-        if (owner->flags & MOIST_FLAG_TRACER_WAVEFRONT) return MOIST_OK;
+        if (owner->flags & (MOIST_FLAG_TRACER_WAVEFRONT | MOIST_FLAG_TRACER_STREAM)) return MOIST_OK;
         int dev = 0, nsm = 0, coop = 0, nb = 0;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -444,17 +489,32 @@ struct Ctx : CtxBase {
         MARK(MOIST_KGROUP_PHYSICS, 1 + (full && dp.do_sf) + (full && dp.do_rd));
         if (full) {
             if (dp.do_sf) {
-                k_surface_fluxes<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, cur, halo_vals, halo_vals + 1, d_u_sf, d_th_sf,
-                                                                  d_qv_sf, mflux, shflux, lhflux, err);
-                CKL();
+                if (rec) {
+                    rec->put(BK_SF, BSf<T>{dp, cur, halo_vals, halo_vals + 1, d_u_sf, d_th_sf, d_qv_sf, mflux, shflux,
+                                           lhflux, err});
+                } else {
+                    k_surface_fluxes<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, cur, halo_vals, halo_vals + 1, d_u_sf,
+                                                                      d_th_sf, d_qv_sf, mflux, shflux, lhflux, err);
+                    CKL();
+                }
             } else {
-                for (T* f : {d_u_sf, d_th_sf, d_qv_sf, mflux, shflux, lhflux})
-                    CK(cudaMemsetAsync(f, 0, P * sizeof(T), st));
+                for (T* f : {d_u_sf, d_th_sf, d_qv_sf, mflux, shflux, lhflux}) {
+                    if (rec)
+                        rec->put(BK_MEMSET, BMemset{f, P * sizeof(T)});
+                    else
+                        CK(cudaMemsetAsync(f, 0, P * sizeof(T), st));
+                }
             }
             if (dp.do_rd) {
-                k_gray_radiation<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, cur, theta_ref, lw_up, lw_dn, d_th_rd, err);
-                CKL();
+                if (rec) {
+                    rec->put(BK_RD, BRd<T>{dp, cur, theta_ref, lw_up, lw_dn, d_th_rd, err});
+                } else {
+                    k_gray_radiation<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, cur, theta_ref, lw_up, lw_dn, d_th_rd, err);
+                    CKL();
+                }
                 rd_dirty = true;
+            } else if (rec) {  // a recorded step clears every time: uploads may come between steps
+                rec->put(BK_MEMSET, BMemset{d_th_rd, fsz * sizeof(T)});
             } else if (rd_dirty) {
                 CK(cudaMemsetAsync(d_th_rd, 0, fsz * sizeof(T), st));
                 rd_dirty = false;
@@ -465,6 +525,11 @@ struct Ctx : CtxBase {
             q.do_mp = 1;
             q.do_sed = 1;
         }
+        if (rec) {
+            rec->put(BK_PHYS, BPhys<T>{q, cur, d_th_mp, d_qv_mp, d_qc_mp, d_qr_mp, d_qr_sed, d_prec, d_th_rd, d_u_sf,
+                                       d_th_sf, d_qv_sf, ph, err});
+            return MOIST_OK;
+        }
         k_physics<T><<<g, b, 0, st>>>(q, cur, d_th_mp, d_qv_mp, d_qc_mp, d_qr_mp, d_qr_sed, d_prec, d_th_rd, d_u_sf,
                                       d_th_sf, d_qv_sf, ph, err);
         CKL();
@@ -474,17 +539,23 @@ struct Ctx : CtxBase {
     int run_stage(StateP<T> s_in, StateP<T> s0, T* const qout[3], StateP<T> s_out, T dt_stage, int ns_s) {
         const dim3 b2(32, 8), g2(cdiv(nx, 32), cdiv(nz, 8));
         MARK(MOIST_KGROUP_PROLOGUE, 3);
-        k_diag<T><<<g2, b2, 0, st>>>(dp, s_in, pres, theta, rt2p, uface, wface, err);
-        CKL();
         TendArgs<T> ta_{s_in, s0, ph, pres, theta, uface, wface, R_rho, R_ru, R_rw, R_rt, rho_p, ru_p[0], rw_p,
                         rt_p[0], mfx, mfz, halo_vals, halo_vals + 1};
-        k_tend<T><<<g2, b2, 0, st>>>(dp, ta_, err);
-        CKL();
         const T dt_s = dt_stage / T(ns_s);
         const unsigned gs = cdiv(nx, strip_wc);
-        k_thomas_strip<T, TT><<<gs, STRIP_THREADS, strip_smem, st>>>(dp, theta, rt2p, dt_s, strip_wc, ta, tb, tc, tcp,
-                                                                     tpiv, err);
-        CKL();
+        if (rec) {
+            rec->put(BK_DIAG, BDiag<T>{dp, s_in, pres, theta, rt2p, uface, wface, err});
+            rec->put(BK_TEND, BTend<T>{dp, ta_, err});
+            rec->put(BK_THOMAS, BThomas<T, TT>{dp, theta, rt2p, dt_s, strip_wc, ta, tb, tc, tcp, tpiv, err});
+        } else {
+            k_diag<T><<<g2, b2, 0, st>>>(dp, s_in, pres, theta, rt2p, uface, wface, err);
+            CKL();
+            k_tend<T><<<g2, b2, 0, st>>>(dp, ta_, err);
+            CKL();
+            k_thomas_strip<T, TT><<<gs, STRIP_THREADS, strip_smem, st>>>(dp, theta, rt2p, dt_s, strip_wc, ta, tb, tc,
+                                                                         tcp, tpiv, err);
+            CKL();
+        }
         const double fact_tp64 = (double)T(0.5) * (1.0 + (double)dp.beta);
         for (int n = 1; n <= ns_s; n++) {
             MARK(MOIST_KGROUP_SUBSTEP, 1);
@@ -511,6 +582,10 @@ struct Ctx : CtxBase {
             sa.tcp = tcp;
             sa.tpiv = tpiv;
             sa.dprime = dprime;
+            if (rec) {
+                rec->put(BK_SUB, BSub<T, TT>{dp, sa, dt_s, T(ns_s), fact_tp64, strip_wc, err});
+                continue;
+            }
             k_substep_strip<T, TT><<<gs, STRIP_THREADS, strip_smem, st>>>(dp, sa, dt_s, T(ns_s), fact_tp64, strip_wc,
                                                                           err);
             CKL();
@@ -529,8 +604,21 @@ struct Ctx : CtxBase {
         tr.mfx = mfx;
         tr.mfz = mfz;
         tr.dt = dt_stage;
-        MARK(MOIST_KGROUP_TRACER, 1);
-        if (use_tiles) {
+        MARK(MOIST_KGROUP_TRACER, (use_stream || use_tiles) ? 2 : 1);
+        if (use_stream) {
+            StreamArgs<T> sa{tr, {s_old[0], s_old[1], s_old[2]}, rrho};
+            if (rec) {
+                rec->put(BK_PREP, BPrep<T>{dp, tr, s_old[0], s_old[1], s_old[2], rrho, err});
+                rec->put(BK_STREAM, BStream<T>{dp, sa, err});
+            } else {
+                k_stream_prep<T><<<g2, b2, 0, st>>>(dp, tr, s_old[0], s_old[1], s_old[2], rrho, err);
+                CKL();
+                k_tracer_stream<T><<<3, (nz + 31) / 32 * 32, 0, st>>>(dp, sa, err);
+                CKL();
+            }
+        } else if (rec) {
+            return set_err(owner, MOIST_ERR_UNSUPPORTED, "a recorded step needs the streaming tracer sweep");
+        } else if (use_tiles) {
             CK(cudaMemsetAsync(tctl.any_changed, 0, (tctl.max_pass + 2) * sizeof(int), st));
             TileCtl c = tctl;
             T* sp = strips;
@@ -546,6 +634,11 @@ struct Ctx : CtxBase {
         }
         MARK(MOIST_KGROUP_UPDATE, 2);
         UpdArgs<T> ua{s_in, s_out, rho_p, ru_p[ns_s % 2], rw_p, rt_p[ns_s % 3], ph};
+        if (rec) {
+            rec->put(BK_UPD, BUpd<T>{dp, ua, err});
+            rec->put(BK_STAGE_END, BStageEnd{err});
+            return MOIST_OK;
+        }
         k_update<T><<<g2, b2, 0, st>>>(dp, ua, err);
         CKL();
         k_stage_end<<<1, 1, 0, st>>>(err);
@@ -571,8 +664,12 @@ struct Ctx : CtxBase {
         if ((r = run_stage(nxt, cur, tmpq, with_q(nxt, tmpq), dt / T(2), ns2)) != MOIST_OK) return r;
         if ((r = run_stage(with_q(nxt, tmpq), cur, nq, nxt, dt, ns)) != MOIST_OK) return r;
         MARK(MOIST_KGROUP_OTHER, 1);
-        k_prec<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, prec, d_prec, err);
-        CKL();
+        if (rec) {
+            rec->put(BK_PREC, BPrec<T>{dp, prec, d_prec, err});
+        } else {
+            k_prec<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, prec, d_prec, err);
+            CKL();
+        }
         std::swap(cur, nxt);
         return MOIST_OK;
     }
@@ -851,6 +948,264 @@ int implicit_t(const moist_params* c, void* rho_w, const void* drho_w, const voi
     return MOIST_OK;
 }
 
+
+// ---------------------------------------------------------------------------- ensembles
+
+int set_berr(moist_batch* b, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (b) b->err = buf;
+    return code;
+}
+
+#define BCK(call)                                                                                    \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess)                                                                       \
+            return set_berr(owner, MOIST_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));  \
+    } while (0)
+
+// The members' recorded steps turned into packed launches (batch.cuh). Two steps are recorded
+// because the current and next States swap every step; each is captured as a CUDA graph.
+template <class T, class TT>
+struct BatchImpl : BatchBase {
+    moist_batch* owner;
+    cudaStream_t st;
+    std::vector<Ctx<T, TT>*> m;
+    struct Slot {
+        int kind;
+        unsigned nitems;
+        dim3 block;
+        size_t smem;
+        const BItem* items;
+        const void* args;
+    };
+    std::vector<Slot> slots[2];
+    std::vector<void*> allocs;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    int parity = 0;
+    int** errs = nullptr;  // device: the members' error words
+    int* err_all = nullptr;
+    size_t max_strip_smem = 0;
+    int max_rows = 32;
+
+    BatchImpl(moist_batch* o, std::vector<Ctx<T, TT>*> members) : owner(o), st(o->stream), m(std::move(members)) {}
+    ~BatchImpl() override {
+        if (st) cudaStreamSynchronize(st);
+        for (auto& e : exec)
+            if (e) cudaGraphExecDestroy(e);
+        for (void* a : allocs) cudaFree(a);
+    }
+
+    template <class U>
+    int dalloc(U** p, size_t n) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(U));
+        if (e != cudaSuccess) return set_berr(owner, MOIST_ERR_NOMEM, "cudaMalloc of %zu bytes failed", n * sizeof(U));
+        allocs.push_back(q);
+        *p = (U*)q;
+        return MOIST_OK;
+    }
+
+    // (member, block) items of one launch kind
+    void items_of(int kind, std::vector<BItem>& it, dim3& block, size_t& smem) {
+        const int n = (int)m.size();
+        smem = 0;
+        auto cells = [&](int i) {
+            for (unsigned by = 0; by < cdiv(m[i]->nz, 8); by++)
+                for (unsigned bx = 0; bx < cdiv(m[i]->nx, 32); bx++) it.push_back({i, (int)bx, (int)by});
+        };
+        switch (kind) {
+            case BK_MEMSET:
+                block = dim3(256);
+                for (int i = 0; i < n; i++) it.push_back({i, 0, 0});
+                break;
+            case BK_SF:
+            case BK_RD:
+            case BK_PREC:
+                block = dim3(128);
+                for (int i = 0; i < n; i++)
+                    for (unsigned bx = 0; bx < cdiv(m[i]->nx, 128); bx++) it.push_back({i, (int)bx, 0});
+                break;
+            case BK_PHYS:
+            case BK_DIAG:
+            case BK_TEND:
+            case BK_UPD:
+            case BK_PREP:
+                block = dim3(32, 8);
+                for (int i = 0; i < n; i++) cells(i);
+                break;
+            case BK_THOMAS:
+            case BK_SUB:
+                block = dim3(STRIP_THREADS);
+                smem = max_strip_smem;
+                for (int i = 0; i < n; i++)
+                    for (unsigned bx = 0; bx < cdiv(m[i]->nx, m[i]->strip_wc); bx++) it.push_back({i, (int)bx, 0});
+                break;
+            case BK_STREAM: {
+                // the longest sweeps (nx + nz steps) first, so that the short ones fill the tail
+                block = dim3(max_rows);
+                std::vector<int> order(n);
+                for (int i = 0; i < n; i++) order[i] = i;
+                std::stable_sort(order.begin(), order.end(),
+                                 [&](int a, int b) { return m[a]->nx + m[a]->nz > m[b]->nx + m[b]->nz; });
+                for (int i : order)
+                    for (int t = 0; t < 3; t++) it.push_back({i, t, 0});
+                break;
+            }
+            case BK_STAGE_END:
+                block = dim3(32);
+                for (int i = 0; i < n; i++) it.push_back({i, 0, 0});
+                break;
+        }
+    }
+
+#define BATCH_LAUNCH(KIND, A, F)                                                                        \
+    case KIND:                                                                                          \
+        k_batched<A, F><<<s.nitems, s.block, s.smem, st>>>(s.items, (const A*)s.args, F{});            \
+        break;
+    int launch(const Slot& s) {
+        switch (s.kind) {
+            BATCH_LAUNCH(BK_MEMSET, BMemset, FMemset)
+            BATCH_LAUNCH(BK_SF, BSf<T>, FSf<T>)
+            BATCH_LAUNCH(BK_RD, BRd<T>, FRd<T>)
+            BATCH_LAUNCH(BK_PHYS, BPhys<T>, FPhys<T>)
+            BATCH_LAUNCH(BK_DIAG, BDiag<T>, FDiag<T>)
+            BATCH_LAUNCH(BK_TEND, BTend<T>, FTend<T>)
+            BATCH_LAUNCH(BK_THOMAS, SINGLE_ARG(BThomas<T, TT>), SINGLE_ARG(FThomas<T, TT>))
+            BATCH_LAUNCH(BK_SUB, SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSub<T, TT>))
+            BATCH_LAUNCH(BK_PREP, BPrep<T>, FPrep<T>)
+            BATCH_LAUNCH(BK_STREAM, BStream<T>, FStream<T>)
+            BATCH_LAUNCH(BK_UPD, BUpd<T>, FUpd<T>)
+            BATCH_LAUNCH(BK_STAGE_END, BStageEnd, FStageEnd)
+            BATCH_LAUNCH(BK_PREC, BPrec<T>, FPrec<T>)
+            default:
+                return set_berr(owner, MOIST_ERR_ARG, "unknown launch kind %d", s.kind);
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return set_berr(owner, MOIST_ERR_CUDA, "batched launch failed: %s", cudaGetErrorString(e));
+        return MOIST_OK;
+    }
+#undef BATCH_LAUNCH
+
+    int build() {
+        const int n = (int)m.size();
+        for (auto* c : m) {
+            max_strip_smem = std::max(max_strip_smem, c->strip_smem);
+            max_rows = std::max(max_rows, (c->nz + 31) / 32 * 32);
+        }
+        BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BThomas<T, TT>), SINGLE_ARG(FThomas<T, TT>)>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_strip_smem));
+        BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSub<T, TT>)>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_strip_smem));
+        for (int q = 0; q < 2; q++) {
+            std::vector<StepRecord> rec(n);
+            for (int i = 0; i < n; i++) {
+                m[i]->rec = &rec[i];
+                const int r = m[i]->launch_step();  // records; swaps the member's current and next State
+                m[i]->rec = nullptr;
+                if (r != MOIST_OK)
+                    return set_berr(owner, r, "member %d: %s", i, m[i]->owner->err.c_str());
+            }
+            for (int i = 1; i < n; i++)
+                if (rec[i].kind != rec[0].kind)
+                    return set_berr(owner, MOIST_ERR_ARG,
+                                    "member %d takes other launches than member 0 (ns, do_sf and do_rd must agree)", i);
+            for (size_t j = 0; j < rec[0].kind.size(); j++) {
+                Slot sl{};
+                sl.kind = rec[0].kind[j];
+                const size_t sz = rec[0].args[j].size();
+                std::vector<unsigned char> packed(sz * n);
+                for (int i = 0; i < n; i++) std::memcpy(packed.data() + sz * i, rec[i].args[j].data(), sz);
+                std::vector<BItem> it;
+                items_of(sl.kind, it, sl.block, sl.smem);
+                sl.nitems = (unsigned)it.size();
+                unsigned char* dargs;
+                BItem* ditems;
+                if (int r = dalloc(&dargs, packed.size())) return r;
+                if (int r = dalloc(&ditems, it.size())) return r;
+                BCK(cudaMemcpy(dargs, packed.data(), packed.size(), cudaMemcpyHostToDevice));
+                BCK(cudaMemcpy(ditems, it.data(), it.size() * sizeof(BItem), cudaMemcpyHostToDevice));
+                sl.items = ditems;
+                sl.args = dargs;
+                slots[q].push_back(sl);
+            }
+        }
+        std::vector<int*> ev(n);
+        for (int i = 0; i < n; i++) ev[i] = m[i]->err;
+        if (int r = dalloc(&errs, n)) return r;
+        if (int r = dalloc(&err_all, 4 * n)) return r;
+        BCK(cudaMemcpy(errs, ev.data(), n * sizeof(int*), cudaMemcpyHostToDevice));
+        for (int q = 0; q < 2; q++) {
+            cudaGraph_t g;
+            BCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            int r = MOIST_OK;
+            for (const Slot& sl : slots[q])
+                if ((r = launch(sl)) != MOIST_OK) break;
+            cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (r != MOIST_OK) return r;
+            if (e != cudaSuccess) return set_berr(owner, MOIST_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&exec[q], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return set_berr(owner, MOIST_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+        }
+        return MOIST_OK;
+    }
+
+    int launch_steps(int nsteps) {
+        for (int j = 0; j < nsteps; j++) {
+            BCK(cudaGraphLaunch(exec[parity], st));
+            parity ^= 1;
+            for (auto* c : m) std::swap(c->cur, c->nxt);
+        }
+        return MOIST_OK;
+    }
+
+    int step(int nsteps) override {
+        const int n = (int)m.size();
+        k_reset_err<<<cdiv(n, 128), 128, 0, st>>>(errs, n);
+        if (int r = launch_steps(nsteps)) return r;
+        k_gather_err<<<cdiv(n, 128), 128, 0, st>>>(errs, n, err_all);
+        std::vector<int> h(4 * (size_t)n);
+        BCK(cudaMemcpyAsync(h.data(), err_all, h.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+        BCK(cudaStreamSynchronize(st));
+        BCK(cudaGetLastError());
+        owner->nan_member = -1;
+        owner->nan_field = -1;
+        for (int i = 0; i < n; i++) {
+            if (h[4 * i] != INT_MAX) {
+                static const char* names[12] = {"rho", "rho_u", "rho_w", "rho_theta", "rho_qv", "rho_qc", "rho_qr",
+                                                "d_rho_u_phys", "d_rho_theta_phys", "d_rho_qv_phys", "d_rho_qc_phys",
+                                                "d_rho_qr_phys"};
+                owner->nan_member = i;
+                owner->nan_field = h[4 * i];
+                m[i]->owner->nan_field = h[4 * i];
+                const char* nm = h[4 * i] >= 0 && h[4 * i] < 12 ? names[h[4 * i]] : "?";
+                m[i]->owner->err = std::string("NaN detected in ") + nm;
+                return set_berr(owner, MOIST_ERR_NAN, "member %d: NaN detected in %s", i, nm);
+            }
+        }
+        return MOIST_OK;
+    }
+
+    int time_steps(int nsteps, float* ms) override {
+        cudaEvent_t e0, e1;
+        BCK(cudaEventCreate(&e0));
+        BCK(cudaEventCreate(&e1));
+        BCK(cudaEventRecord(e0, st));
+        int r = launch_steps(nsteps);
+        BCK(cudaEventRecord(e1, st));
+        BCK(cudaEventSynchronize(e1));
+        BCK(cudaEventElapsedTime(ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return r;
+    }
+};
+
 }  // namespace
 
 // ============================================================================ C-ABI
@@ -926,6 +1281,102 @@ int moist_ctx_destroy(moist_ctx* c) {
 }
 
 const char* moist_last_error(const moist_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+// ------------------------------------------------------------------------- ensembles
+
+int moist_batch_destroy(moist_batch* b) {
+    if (!b) return MOIST_ERR_ARG;
+    cudaSetDevice(b->device);
+    delete b->impl;
+    for (moist_ctx* c : b->members) moist_ctx_destroy(c);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return MOIST_OK;
+}
+
+int moist_batch_create(const moist_params* members, int nmembers, int precision, int flags, moist_batch** out) {
+    if (!out) return MOIST_ERR_ARG;
+    *out = nullptr;
+    if (!members || nmembers < 1 || (precision != MOIST_F32 && precision != MOIST_F64)) return MOIST_ERR_ARG;
+    for (int i = 0; i < nmembers; i++) {
+        if (members[i].halo != 2 || members[i].nx < 2) return MOIST_ERR_ARG;
+        if (members[i].nz > STREAM_MAX_ROWS) return MOIST_ERR_UNSUPPORTED;
+        if (members[i].ns != members[0].ns) return MOIST_ERR_ARG;
+    }
+    moist_batch* b = new moist_batch();
+    b->precision = precision;
+    if (cudaGetDevice(&b->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete b;
+        return MOIST_ERR_CUDA;
+    }
+    const int mflags = (flags & MOIST_FLAG_TRI_NATIVE) | MOIST_FLAG_TRACER_STREAM;
+    for (int i = 0; i < nmembers; i++) {
+        moist_ctx* c = nullptr;
+        const int r = moist_ctx_create(&members[i], precision, mflags, &c);
+        if (r != MOIST_OK) {
+            moist_batch_destroy(b);
+            return r;
+        }
+        b->members.push_back(c);
+    }
+    int r;
+    if (precision == MOIST_F64) {
+        std::vector<Ctx<double, double>*> v;
+        for (auto* c : b->members) v.push_back(static_cast<Ctx<double, double>*>(c->impl));
+        auto* x = new BatchImpl<double, double>(b, v);
+        b->impl = x;
+        r = x->build();
+    } else if (flags & MOIST_FLAG_TRI_NATIVE) {
+        std::vector<Ctx<float, float>*> v;
+        for (auto* c : b->members) v.push_back(static_cast<Ctx<float, float>*>(c->impl));
+        auto* x = new BatchImpl<float, float>(b, v);
+        b->impl = x;
+        r = x->build();
+    } else {
+        std::vector<Ctx<float, double>*> v;
+        for (auto* c : b->members) v.push_back(static_cast<Ctx<float, double>*>(c->impl));
+        auto* x = new BatchImpl<float, double>(b, v);
+        b->impl = x;
+        r = x->build();
+    }
+    if (r != MOIST_OK) {
+        moist_batch_destroy(b);
+        return r;
+    }
+    *out = b;
+    return MOIST_OK;
+}
+
+moist_ctx* moist_batch_member(moist_batch* b, int member) {
+    return (b && member >= 0 && member < (int)b->members.size()) ? b->members[member] : nullptr;
+}
+
+int moist_batch_upload(moist_batch* b, int member, const moist_state_host* s) {
+    moist_ctx* c = moist_batch_member(b, member);
+    return c ? moist_upload_state(c, s) : MOIST_ERR_ARG;
+}
+
+int moist_batch_download(moist_batch* b, int member, moist_state_host* s) {
+    moist_ctx* c = moist_batch_member(b, member);
+    return c ? moist_download_state(c, s) : MOIST_ERR_ARG;
+}
+
+int moist_batch_step(moist_batch* b, int nsteps) {
+    if (!b || nsteps < 0) return MOIST_ERR_ARG;
+    if (cudaSetDevice(b->device) != cudaSuccess) return MOIST_ERR_CUDA;
+    return b->impl->step(nsteps);
+}
+
+int moist_batch_time_steps(moist_batch* b, int nsteps, float* ms) {
+    if (!b || nsteps < 0 || !ms) return MOIST_ERR_ARG;
+    if (cudaSetDevice(b->device) != cudaSuccess) return MOIST_ERR_CUDA;
+    return b->impl->time_steps(nsteps, ms);
+}
+
+const char* moist_batch_last_error(const moist_batch* b) { return b ? b->err.c_str() : "null batch"; }
+int moist_batch_nan_member(const moist_batch* b) { return b ? b->nan_member : -1; }
+
 int moist_nan_field(const moist_ctx* c) { return c ? c->nan_field : -1; }
 
 // the context's device is made current for the calling thread at every entry point

@@ -157,3 +157,78 @@ def eval_helper(p, helper, inputs, nout):
                                    out.ctypes.data_as(C.POINTER(C.c_double))), None,
            "moist_eval_helper")
     return out.reshape(n, nout) if nout > 1 else out
+
+
+class Ensemble:
+    """Independent domains advanced together (moist_batch_*): one launch per kernel of the large
+    step for all members, each step a CUDA graph. `params` are the members' Params (one
+    precision; ns, do_sf and do_rd equal; nz <= 256). Every member's results equal those of a
+    Model stepping that member alone, bit for bit."""
+
+    def __init__(self, params, flags=0):
+        self.params = list(params)
+        precs = {p.precision for p in self.params}
+        if len(precs) != 1:
+            raise ValueError("Ensemble: members of one precision")
+        self._cps = [p.to_c() for p in self.params]
+        arr = (abi.moist_params * len(self._cps))(*self._cps)
+        self.b = C.c_void_p()
+        rc = lib().moist_batch_create(arr, len(self._cps), precs.pop(), flags, C.byref(self.b))
+        _raise(rc, None, "moist_batch_create")
+
+    def close(self):
+        if self.b:
+            lib().moist_batch_destroy(self.b)
+            self.b = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc == abi.MOIST_OK:
+            return
+        msg = lib().moist_batch_last_error(self.b).decode()
+        if rc == abi.MOIST_ERR_NAN:
+            raise FloatingPointError(msg)
+        raise RuntimeError("%s failed (%s): %s" % (what, lib().moist_status_string(rc).decode(), msg))
+
+    def member(self, i):
+        return lib().moist_batch_member(self.b, int(i))
+
+    def upload(self, i, s):
+        h = s.to_c()
+        ctx = self.member(i)
+        _raise(lib().moist_batch_upload(self.b, int(i), C.byref(h)), ctx, "moist_batch_upload")
+
+    def download(self, i, s):
+        h = s.to_c()
+        ctx = self.member(i)
+        _raise(lib().moist_batch_download(self.b, int(i), C.byref(h)), ctx, "moist_batch_download")
+        return s
+
+    def step(self, nsteps=1):
+        self._check(lib().moist_batch_step(self.b, int(nsteps)), "moist_batch_step")
+
+    def time_steps(self, nsteps):
+        ms = C.c_float()
+        self._check(lib().moist_batch_time_steps(self.b, int(nsteps), C.byref(ms)), "moist_batch_time_steps")
+        return ms.value
+
+    @property
+    def nan_member(self):
+        return lib().moist_batch_nan_member(self.b)
+
+    def budget(self, i):
+        out = (C.c_double * 4)()
+        ctx = self.member(i)
+        _raise(lib().moist_budget(ctx, out), ctx, "moist_budget")
+        return np.array(out[:])

@@ -133,11 +133,27 @@ def test_tiled_tracer_sweep_matches_wavefront_and_oracle(T, tri_native):
     from states import perturb
     p, s = sounding_bubbles(T, nx=256, nz=72, nbub=2)
     perturb(s, p, 21, wind=6.0, w=2.0)
-    a, b, c = s.copy(), s.copy(), s.copy()
+    a, b, c, d = s.copy(), s.copy(), s.copy(), s.copy()
     model.rk3_step(a, p, 3, flags=_flags(tri_native))
     model.rk3_step(b, p, 3, flags=_flags(tri_native) | abi.MOIST_FLAG_TRACER_WAVEFRONT)
+    model.rk3_step(d, p, 3, flags=_flags(tri_native) | abi.MOIST_FLAG_TRACER_STREAM)
     bind.rk3_step(c, p, 3, tri64=_tri64(T, tri_native))
     compare(a, b, p)
+    compare(a, c, p)
+    compare(d, c, p)
+
+
+@pytest.mark.parametrize("T,tri_native", MODES, ids=MODE_IDS)
+@pytest.mark.parametrize("nx,nz", [(2, 2), (3, 5), (7, 33), (40, 31), (33, 64), (64, 97), (19, 256)])
+def test_streaming_tracer_sweep_small_shapes(T, tri_native, nx, nz):
+    """The row-streaming sweep against the oracle on shapes that put rows on both sides of warp
+    boundaries, partial last warps, the largest supported height and the narrowest domain."""
+    from states import perturb
+    p, s = small_case(T, nx, nz)
+    perturb(s, p, 5, wind=4.0, w=1.0)
+    a, c = s.copy(), s.copy()
+    model.rk3_step(a, p, 2, flags=_flags(tri_native) | abi.MOIST_FLAG_TRACER_STREAM)
+    bind.rk3_step(c, p, 2, tri64=_tri64(T, tri_native))
     compare(a, c, p)
 
 
