@@ -262,6 +262,9 @@ int moist_batch_download(moist_batch* b, int member, moist_state_host* s);
 int moist_batch_step(moist_batch* b, int nsteps);
 /* nsteps large steps timed with CUDA events on the batch stream (no error check) */
 int moist_batch_time_steps(moist_batch* b, int nsteps, float* ms);
+/* nsteps large steps launched without the graphs, with CUDA events around every packed launch:
+ * total device time and its split over the MOIST_KGROUP_* groups (group_ms[MOIST_NGROUPS]) */
+int moist_batch_profile(moist_batch* b, int nsteps, float* total_ms, float* group_ms);
 const char* moist_batch_last_error(const moist_batch* b);
 int moist_batch_nan_member(const moist_batch* b);
 

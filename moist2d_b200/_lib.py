@@ -17,7 +17,8 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_rk3_step_host", "moist_step_profile", "moist_set_device",
            "moist_implicit_correction_noalloc", "moist_tracer_pass_counts", "moist_batch_create",
            "moist_batch_destroy", "moist_batch_member", "moist_batch_upload", "moist_batch_download",
-           "moist_batch_step", "moist_batch_time_steps", "moist_batch_last_error", "moist_batch_nan_member")
+           "moist_batch_step", "moist_batch_time_steps", "moist_batch_last_error", "moist_batch_nan_member",
+           "moist_batch_profile")
 
 
 def lib():
@@ -69,5 +70,6 @@ def lib():
         L.moist_batch_last_error.argtypes = [B]
         L.moist_batch_last_error.restype = C.c_char_p
         L.moist_batch_nan_member.argtypes = [B]
+        L.moist_batch_profile.argtypes = [B, I, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         _lib = L
     return _lib

@@ -204,9 +204,11 @@ struct FPrec {
     }
 };
 
-// one launch for all members: block b runs item b with its member's arguments
-template <class A, class F>
-__global__ void __launch_bounds__(256) k_batched(const BItem* __restrict__ items, const A* __restrict__ args, F f) {
+// one launch for all members: block b runs item b with its member's arguments. MINB bounds
+// the registers so that MINB blocks of 256 threads fit on an SM.
+template <class A, class F, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_batched(const BItem* __restrict__ items, const A* __restrict__ args,
+                                                        F f) {
     const BItem it = items[blockIdx.x];
     f(args[it.m], it.bx, it.by);
 }

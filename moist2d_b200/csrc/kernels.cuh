@@ -665,9 +665,11 @@ __device__ __forceinline__ void b_thomas_strip(DevParams<T> p, const T* theta, c
     const int i = i0 + col;
     const T fact_tp = T(0.5) * (T(1.0) + p.beta);
     const T dt_tp2 = (dt_s * fact_tp) * (dt_s * fact_tp);
+    #pragma unroll 4
     for (int j = r0; j < n && own; j += rs)
         th_h[j * wc + col] = f2h(theta[MOIST_IDX(j, i)], theta[MOIST_IDX(j + 1, i)], dz[j], dz[j + 1]);
     __syncthreads();
+    #pragma unroll 4
     for (int j = r0; j < n && own; j += rs) {
         const int k = j;
         const T th_cur = th_h[j * wc + col];
@@ -698,6 +700,7 @@ __device__ __forceinline__ void b_thomas_strip(DevParams<T> p, const T* theta, c
         }
     }
     __syncthreads();
+    #pragma unroll 4
     for (int j = r0; j < n && own; j += rs) {
         tcp[MOIST_IDX(j, i)] = sm.cp[j * wc + col];
         tpiv[MOIST_IDX(j, i)] = sm.piv[j * wc + col];
@@ -728,6 +731,7 @@ __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a
     // (1) horizontal forward step of rho_u_p at the ncol + 1 faces (1355-1366)
     {
         const int nf = ncol + 1, wf = wc + 1;
+        #pragma unroll 4
         for (int e = tid; e < nz * nf; e += STRIP_THREADS) {
             const int k = e / nf, f = e - k * nf;
             const int cc = wrapx(i0 + f - 1, nx), cn = wrapx(cc + 1, nx);
@@ -745,6 +749,7 @@ __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a
     const int i = i0 + col;
     const int im = wrapx(i - 1, nx), ip = wrapx(i + 1, nx);
     // (2) explicit rho_p, rho_theta_p and their off-centred values (1367-1396)
+    #pragma unroll 4
     for (int k = r0; k < nz && own; k += rs) {
         const size_t c = MOIST_IDX(k, i);
         const T u_m = sm.u[k * (wc + 1) + col], u_p = sm.u[k * (wc + 1) + col + 1];
@@ -766,6 +771,7 @@ __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a
     }
     __syncthreads();
     // (3) right-hand side of the w-p system (1397-1408) and the stage factors
+    #pragma unroll 4
     for (int j = r0; j < n && own; j += rs) {
         const int k = j + 1;
         const size_t c = MOIST_IDX(k, i), cj = c - P;
@@ -805,6 +811,7 @@ __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a
     __syncthreads();
     // (5) vertical rho_p, rho_theta_p updates (1412-1446), momentum flux averages (1452-1458)
     const T* th = a.theta;
+    #pragma unroll 4
     for (int k = r0; k < nz && own; k += rs) {
         const size_t c = MOIST_IDX(k, i);
         const T w_k = k < ke ? sm.w[k * wc + col] : T(0.0);

@@ -53,6 +53,7 @@ struct BatchBase {
     virtual ~BatchBase() {}
     virtual int step(int nsteps) = 0;
     virtual int time_steps(int nsteps, float* ms) = 0;
+    virtual int profile(int nsteps, float* total_ms, float* group_ms) = 0;
 };
 
 }  // namespace
@@ -1063,25 +1064,25 @@ struct BatchImpl : BatchBase {
         }
     }
 
-#define BATCH_LAUNCH(KIND, A, F)                                                                        \
-    case KIND:                                                                                          \
-        k_batched<A, F><<<s.nitems, s.block, s.smem, st>>>(s.items, (const A*)s.args, F{});            \
+#define BATCH_LAUNCH(KIND, A, F, MINB)                                                                 \
+    case KIND:                                                                                         \
+        k_batched<A, F, MINB><<<s.nitems, s.block, s.smem, st>>>(s.items, (const A*)s.args, F{});     \
         break;
     int launch(const Slot& s) {
         switch (s.kind) {
-            BATCH_LAUNCH(BK_MEMSET, BMemset, FMemset)
-            BATCH_LAUNCH(BK_SF, BSf<T>, FSf<T>)
-            BATCH_LAUNCH(BK_RD, BRd<T>, FRd<T>)
-            BATCH_LAUNCH(BK_PHYS, BPhys<T>, FPhys<T>)
-            BATCH_LAUNCH(BK_DIAG, BDiag<T>, FDiag<T>)
-            BATCH_LAUNCH(BK_TEND, BTend<T>, FTend<T>)
-            BATCH_LAUNCH(BK_THOMAS, SINGLE_ARG(BThomas<T, TT>), SINGLE_ARG(FThomas<T, TT>))
-            BATCH_LAUNCH(BK_SUB, SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSub<T, TT>))
-            BATCH_LAUNCH(BK_PREP, BPrep<T>, FPrep<T>)
-            BATCH_LAUNCH(BK_STREAM, BStream<T>, FStream<T>)
-            BATCH_LAUNCH(BK_UPD, BUpd<T>, FUpd<T>)
-            BATCH_LAUNCH(BK_STAGE_END, BStageEnd, FStageEnd)
-            BATCH_LAUNCH(BK_PREC, BPrec<T>, FPrec<T>)
+            BATCH_LAUNCH(BK_MEMSET, BMemset, FMemset, 1)
+            BATCH_LAUNCH(BK_SF, BSf<T>, FSf<T>, 1)
+            BATCH_LAUNCH(BK_RD, BRd<T>, FRd<T>, 1)
+            BATCH_LAUNCH(BK_PHYS, BPhys<T>, FPhys<T>, 1)
+            BATCH_LAUNCH(BK_DIAG, BDiag<T>, FDiag<T>, 1)
+            BATCH_LAUNCH(BK_TEND, BTend<T>, FTend<T>, 1)
+            BATCH_LAUNCH(BK_THOMAS, SINGLE_ARG(BThomas<T, TT>), SINGLE_ARG(FThomas<T, TT>), 4)
+            BATCH_LAUNCH(BK_SUB, SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSub<T, TT>), 4)
+            BATCH_LAUNCH(BK_PREP, BPrep<T>, FPrep<T>, 1)
+            BATCH_LAUNCH(BK_STREAM, BStream<T>, FStream<T>, 1)
+            BATCH_LAUNCH(BK_UPD, BUpd<T>, FUpd<T>, 1)
+            BATCH_LAUNCH(BK_STAGE_END, BStageEnd, FStageEnd, 1)
+            BATCH_LAUNCH(BK_PREC, BPrec<T>, FPrec<T>, 1)
             default:
                 return set_berr(owner, MOIST_ERR_ARG, "unknown launch kind %d", s.kind);
         }
@@ -1094,12 +1095,21 @@ struct BatchImpl : BatchBase {
     int build() {
         const int n = (int)m.size();
         for (auto* c : m) {
+            // a batch has blocks enough for every SM without narrow strips: take the widest
+            // strip whose shared memory leaves room for several blocks per SM
+            for (int w : {8, 4, 2, 1}) {
+                if (w == 1 || strip_smem_bytes<T, TT>(c->nz, w) <= 64 * 1024) {
+                    c->strip_wc = w;
+                    c->strip_smem = strip_smem_bytes<T, TT>(c->nz, w);
+                    break;
+                }
+            }
             max_strip_smem = std::max(max_strip_smem, c->strip_smem);
             max_rows = std::max(max_rows, (c->nz + 31) / 32 * 32);
         }
-        BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BThomas<T, TT>), SINGLE_ARG(FThomas<T, TT>)>,
+        BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BThomas<T, TT>), SINGLE_ARG(FThomas<T, TT>), 4>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_strip_smem));
-        BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSub<T, TT>)>,
+        BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSub<T, TT>), 4>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_strip_smem));
         for (int q = 0; q < 2; q++) {
             std::vector<StepRecord> rec(n);
@@ -1188,6 +1198,40 @@ struct BatchImpl : BatchBase {
                 return set_berr(owner, MOIST_ERR_NAN, "member %d: NaN detected in %s", i, nm);
             }
         }
+        return MOIST_OK;
+    }
+
+    // nsteps without the graphs: events around every packed launch, summed per kernel group
+    int profile(int nsteps, float* total_ms, float* group_ms) override {
+        static const int group_of[BK_NKINDS] = {MOIST_KGROUP_PHYSICS,  MOIST_KGROUP_PHYSICS, MOIST_KGROUP_PHYSICS,
+                                                MOIST_KGROUP_PHYSICS,  MOIST_KGROUP_PROLOGUE, MOIST_KGROUP_PROLOGUE,
+                                                MOIST_KGROUP_PROLOGUE, MOIST_KGROUP_SUBSTEP, MOIST_KGROUP_TRACER,
+                                                MOIST_KGROUP_TRACER,   MOIST_KGROUP_UPDATE,  MOIST_KGROUP_UPDATE,
+                                                MOIST_KGROUP_OTHER};
+        size_t per = slots[0].size() + slots[1].size();
+        std::vector<cudaEvent_t> ev(nsteps * (per + 2) + 1);
+        for (auto& e : ev) BCK(cudaEventCreate(&e));
+        std::vector<int> kinds;
+        size_t j = 0;
+        BCK(cudaEventRecord(ev[j++], st));
+        for (int n = 0; n < nsteps; n++) {
+            for (const Slot& sl : slots[parity]) {
+                if (int r = launch(sl)) return r;
+                kinds.push_back(sl.kind);
+                BCK(cudaEventRecord(ev[j++], st));
+            }
+            parity ^= 1;
+            for (auto* c : m) std::swap(c->cur, c->nxt);
+        }
+        BCK(cudaEventSynchronize(ev[j - 1]));
+        for (int g = 0; g < MOIST_NGROUPS; g++) group_ms[g] = 0.f;
+        for (size_t q = 0; q < kinds.size(); q++) {
+            float t;
+            BCK(cudaEventElapsedTime(&t, ev[q], ev[q + 1]));
+            group_ms[group_of[kinds[q]]] += t;
+        }
+        BCK(cudaEventElapsedTime(total_ms, ev[0], ev[j - 1]));
+        for (auto& e : ev) cudaEventDestroy(e);
         return MOIST_OK;
     }
 
@@ -1372,6 +1416,12 @@ int moist_batch_time_steps(moist_batch* b, int nsteps, float* ms) {
     if (!b || nsteps < 0 || !ms) return MOIST_ERR_ARG;
     if (cudaSetDevice(b->device) != cudaSuccess) return MOIST_ERR_CUDA;
     return b->impl->time_steps(nsteps, ms);
+}
+
+int moist_batch_profile(moist_batch* b, int nsteps, float* total_ms, float* group_ms) {
+    if (!b || nsteps < 1 || !total_ms || !group_ms) return MOIST_ERR_ARG;
+    if (cudaSetDevice(b->device) != cudaSuccess) return MOIST_ERR_CUDA;
+    return b->impl->profile(nsteps, total_ms, group_ms);
 }
 
 const char* moist_batch_last_error(const moist_batch* b) { return b ? b->err.c_str() : "null batch"; }

@@ -277,8 +277,11 @@ def _sounding_u(z):
     return 12.0 * np.tanh(np.asarray(z, dtype=np.float64) / 3e3)
 
 
-def _bubbles_state(p, base, bubbles):
-    """Apply warm bubbles [(xc, zc, r, amp)] at constant pressure to the base columns."""
+def _bubbles_state(p, base, bubbles, distinct_columns=False):
+    """Apply warm bubbles [(xc, zc, r, amp)] at constant pressure to the base columns.
+    distinct_columns: solve only the columns a bubble touches plus one environment column and
+    copy that one to the other columns (the solve is elementwise, so the untouched columns are
+    the same environment column)."""
     c = p.c
     rho0, qv0, th0, pr = base
     nx, nz = p.Nx, p.Nz
@@ -297,7 +300,18 @@ def _bubbles_state(p, base, bubbles):
     rh = np.repeat(np.array([[1.0 - 0.75 * min(zk / 12e3, 1.0) ** 1.25] for zk in zz]), nx, axis=1)
     th_env = np.repeat(th0, nx, axis=1)
     # environmental theta at fixed pressure plus the perturbation
-    rho, qv, th = _state_at_pressure(P, lambda Pi: th_env + thp, rh, c)
+    if distinct_columns:
+        touched = np.flatnonzero(np.any(thp != 0.0, axis=0))
+        env = np.flatnonzero(~np.any(thp != 0.0, axis=0))
+        cols = np.concatenate([touched, env[:1]])
+        r_, q_, t_ = _state_at_pressure(P[:, cols], lambda Pi: th_env[:, cols] + thp[:, cols], rh[:, cols], c)
+        rho, qv, th = (np.empty((nz, nx)) for _ in range(3))
+        for full, part in ((rho, r_), (qv, q_), (th, t_)):
+            if len(env):
+                full[:, env] = part[:, -1:]
+            full[:, touched] = part[:, :len(touched)]
+    else:
+        rho, qv, th = _state_at_pressure(P, lambda Pi: th_env + thp, rh, c)
     u = np.repeat(_sounding_u(zz)[:, None], nx, axis=1)
     s = State(p)
     s.theta_ref[:] = th0[:, 0].astype(p.T)
@@ -327,6 +341,9 @@ def single_bubble(T=np.float32, seed=4, nx=512, nz=96, amp=2.0, radius=2e3, ns=8
     return p, _bubbles_state(p, base, [(float(p.Lx) / 2.0, 1.5e3, radius, amp)])
 
 
+_SOUNDING_CACHE = {}
+
+
 def ensemble_member(T=np.float32, seed=3, member=0, nx_choices=tuple(range(256, 2049, 256)),
                     nz_choices=(64, 96, 128), ns=8, dt=2.0, amp=(1.0, 3.0), rad=(1e3, 3e3)):
     """Member m of an ensemble of uneven domains: nx, nz drawn from the choices, one bubble at
@@ -335,7 +352,10 @@ def ensemble_member(T=np.float32, seed=3, member=0, nx_choices=tuple(range(256, 
     nx = int(nx_choices[min(int(u[0] * len(nx_choices)), len(nx_choices) - 1)])
     nz = int(nz_choices[min(int(u[1] * len(nz_choices)), len(nz_choices) - 1)])
     p = _grid_params(T, nx, nz, 250.0, 125.0, ns, dt)
-    base = sounding_columns(p.z, p.c)
+    key = (np.dtype(T).str, p.z.tobytes())
+    if key not in _SOUNDING_CACHE:  # the hydrostatic march depends on the grid only
+        _SOUNDING_CACHE[key] = sounding_columns(p.z, p.c)
+    base = _SOUNDING_CACHE[key]
     bub = [(u[2] * float(p.Lx), 1.5e3, rad[0] + (rad[1] - rad[0]) * u[4],
             amp[0] + (amp[1] - amp[0]) * u[3])]
-    return p, _bubbles_state(p, base, bub)
+    return p, _bubbles_state(p, base, bub, distinct_columns=True)

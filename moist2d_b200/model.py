@@ -223,6 +223,13 @@ class Ensemble:
         self._check(lib().moist_batch_time_steps(self.b, int(nsteps), C.byref(ms)), "moist_batch_time_steps")
         return ms.value
 
+    def profile(self, nsteps):
+        """(total ms, per-group ms) of nsteps launched without the graphs (MOIST_KGROUP_* order)."""
+        tot = C.c_float()
+        g = (C.c_float * abi.MOIST_NGROUPS)()
+        self._check(lib().moist_batch_profile(self.b, int(nsteps), C.byref(tot), g), "moist_batch_profile")
+        return tot.value, list(g)
+
     @property
     def nan_member(self):
         return lib().moist_batch_nan_member(self.b)
