@@ -347,7 +347,7 @@ struct Ctx : CtxBase {
         if (!coop || (long)nb * nsm < tctl.ntiles) return MOIST_OK;
         AL(strips, (size_t)2 * 3 * tctl.ntiles * 4 * TT_W);
         AL(tctl.bar, 2);
-        AL(tctl.changed, (size_t)2 * 3 * tctl.ntiles);
+        AL(tctl.changed, (size_t)2 * 3 * tctl.ntiles * 2);
         AL(tctl.any_changed, (size_t)tctl.max_pass + 2);
         AL(tctl.passes, 1);
         AL(pass_hist, 64);

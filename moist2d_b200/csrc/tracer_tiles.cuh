@@ -31,7 +31,7 @@ constexpr int TT_S = TT_W + 2; // staged extent with a two-cell halo
 struct TileCtl {
     int tiles_x, tiles_z, ntiles, max_pass;
     unsigned* bar;      // [0] arrival counter, [1] generation
-    int* changed;       // [2][3][ntiles] per pass parity: bit 0 right strip changed, bit 1 top strip
+    int* changed;       // [2][3][ntiles][2] per pass parity: rows whose right-strip entries changed, columns whose top-strip entries changed (bit masks)
     int* any_changed;   // [max_pass + 1]
     int* passes;        // out: passes run
     int* timeout;       // out: barrier timeout flag
@@ -266,6 +266,7 @@ using FastDiv = Div64;  // division policy of the Float32 fast cell (fastdiv.cuh
 template <class T>
 struct TileQ {
     typename FastDiv::R rrho[TT_W][TT_W + 2];  // 1/rho of the tile cells in the fast cell's form
+    T snp[3][TT_W][TT_W + 2];  // per tracer: s = q / rho of the last pass (the rows a repair pass replays)
     T q0[3][TT_W][TT_W + 2];   // row stride 34: lane r reads column step - r, conflict-free
     T dph[3][TT_W][TT_W + 2];
     T qn[3][TT_W][TT_W + 2];
@@ -441,18 +442,22 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
     int pass = 1;
     for (; pass <= ctl.max_pass; pass++) {
         const int cur = pass & 1, prv = cur ^ 1;
-        const int* chg_prev = ctl.changed + (size_t)prv * 3 * ctl.ntiles + (size_t)t * ctl.ntiles;
-        int* chg_cur = ctl.changed + (size_t)cur * 3 * ctl.ntiles + (size_t)t * ctl.ntiles;
+        const int* chg_prev = ctl.changed + ((size_t)prv * 3 * ctl.ntiles + (size_t)t * ctl.ntiles) * 2;
+        int* chg_cur = ctl.changed + ((size_t)cur * 3 * ctl.ntiles + (size_t)t * ctl.ntiles) * 2;
         const int left = tx > 0 ? tile - 1 : -1;
         const int below = tz > 0 ? tile - ctl.tiles_x : -1;
-        // neighbours' strips and flags are written by other SMs: read them through L2 (__ldcg)
-        const bool compute = !halt && (pass == 1 || (left >= 0 && (__ldcg(chg_prev + left) & 1)) ||
-                                       (below >= 0 && (__ldcg(chg_prev + below) & 2)));
+        // neighbours' strips and masks are written by other SMs: read them through L2 (__ldcg)
+        const unsigned lmask = left >= 0 ? (unsigned)__ldcg(chg_prev + 2 * left) : 0u;
+        const unsigned bmask = below >= 0 ? (unsigned)__ldcg(chg_prev + 2 * below + 1) : 0u;
+        const bool compute = !halt && (pass == 1 || lmask != 0u || bmask != 0u);
+        // Rows below the lowest changed row of the left strip have unchanged inputs when the
+        // lower strip did not change: a repair pass replays their last values (Float32)
+        const int rmin = (pass == 1 || bmask != 0u || !kStageQ<T>) ? 0 : __ffs((int)lmask) - 1;
         if (ctl.pass_ts && blockIdx.x == 0 && threadIdx.x == 0) ctl.pass_ts[pass] = globaltimer_ns();
         if (ctl.pass_work && compute && lane == 0) atomicAdd(ctl.pass_work + pass, 1);
         const T* sp_prev = strip_ptr(strips, prv, t, tile, ctl.ntiles);
         T* sp_cur = strip_ptr(strips, cur, t, tile, ctl.ntiles);
-        int my_changed = 0;
+        bool right_changed = false, top_changed = false;
         if (compute) {
             // left inputs: the left tile's right strip, or at the periodic seam the halo columns'
             // stage-start values; bottom inputs: the lower tile's top strip (none at k = 0)
@@ -494,53 +499,85 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
                 const T* bot1 = sm.bot[t][1];
                 const T* cl_kp = sm.cl[t][0][k == 0 ? 0 : 1];
                 const T* cl_km = sm.cl[t][1][k == 1 ? 0 : 1];
-                for (int step = 0; step < nsteps; step++) {
+                // Repair passes recompute only where an input changed. A cell reads four updated
+                // values: (k, i-1), (k, i-2) of its own row and (k-1, i), (k-2, i) from the rows
+                // below; each lane carries, with every value it passes on, whether that value
+                // changed in this pass. The stage-start values never change, so a cell whose
+                // four updated inputs are all unchanged returns its last value. A step in which
+                // no lane has a changed input replays the stored values only.
+                const bool all_dirty = pass == 1;
+                const bool left_chg = ((lmask >> r) & 1u) != 0u;  // this row's left-strip inputs
+                bool c1 = left_chg, c2 = left_chg;                // prev1, prev2 changed
+                bool chg_last = false, km1_chg_used = false;
+                // replayed rows start two steps early: the first recomputed row reads the two below
+                for (int step = rmin >= 2 ? rmin - 2 : 0; step < nsteps; step++) {
                     const int c_raw = step - r;
                     const bool active = row_ok && c_raw >= 0 && c_raw < width;
                     const int c = min(max(c_raw, 0), TT_W - 1);
                     // row-below values: lane r-1's result of the previous step and the value it used
                     const T up_sn = __shfl_up_sync(0xffffffffu, sn_last, 1);
                     const T up_km1 = __shfl_up_sync(0xffffffffu, km1_used, 1);
+                    const bool up_chg = __shfl_up_sync(0xffffffffu, chg_last, 1);
+                    const bool up_km1_chg = __shfl_up_sync(0xffffffffu, km1_chg_used, 1);
                     const T b1 = bot1[c], b0 = bot0[c];
+                    const bool bchg = ((bmask >> c) & 1u) != 0u;  // the lower tile's top strip at column c
                     const T s_km1 = r == 0 ? b1 : up_sn;
                     const T s_km2 = r == 0 ? b0 : (r == 1 ? b1 : up_km1);
-                    const T q0_c = sm.q.q0[t][r][c], dph_c = sm.q.dph[t][r][c];
-                    const T rho_c = sm.rho[r + 1][c + 1];
-                    bool bad;
-                    unsigned g = ~0u;
-                    T qn_v = tracer_cell_f<FastDiv>(fw, sm.s[t][r][c], sm.s[t][r][c + 1], sm.s[t][r][c + 2], sm.s[t][r + 1][c],
-                                           sm.s[t][r + 2][c], prev1, prev2, s_km1, s_km2, cl_kp[c], cl_km[c],
-                                           sm.mx[r][c + 1], sm.mx[r][c], sm.mz[r + 1][c], sm.mz[r][c], rho_c,
-                                           sm.rho[r + 1][c + 2], sm.rho[r + 1][c], sm.rho[r + 2][c + 1], sm.rho[r][c + 1],
-                                           q0_c, dph_c, g, bad);
-                    T sn = FastDiv::cdiv(qn_v, rho_c, sm.q.rrho[r][c], g);
-                    bad |= guard_hit(g);
-                    if (active && bad) {
-                        // a subnormal-range quotient or a non-finite result: the same cell with
-                        // subnormal quotients rounded explicitly (exact for every input), and
-                        // IEEE division if the result is still not finite
-                        unsigned g2 = ~0u;
-                        bool bad2;
-                        qn_v = tracer_cell_f<Div64X>(fw, sm.s[t][r][c], sm.s[t][r][c + 1], sm.s[t][r][c + 2],
-                                                     sm.s[t][r + 1][c], sm.s[t][r + 2][c], prev1, prev2, s_km1, s_km2,
-                                                     cl_kp[c], cl_km[c], sm.mx[r][c + 1], sm.mx[r][c], sm.mz[r + 1][c],
-                                                     sm.mz[r][c], rho_c, sm.rho[r + 1][c + 2], sm.rho[r + 1][c],
-                                                     sm.rho[r + 2][c + 1], sm.rho[r][c + 1], q0_c, dph_c, g2, bad2);
-                        sn = Div64X::cdiv(qn_v, rho_c, sm.q.rrho[r][c], g2);
-                        if (bad2) {
-                            bool unused = false;
-                            qn_v = MOIST_TILE_CELL(DivIEEE<T>, unused);
-                            sn = qn_v / rho_c;
+                    const bool km1_chg = r == 0 ? bchg : up_chg;
+                    const bool km2_chg = r == 0 ? bchg : (r == 1 ? bchg : up_km1_chg);
+                    const bool dirty = active && (all_dirty || c1 || c2 || km1_chg || km2_chg);
+                    T qn_v = T(0), sn = sm.q.snp[t][r][c];
+                    bool changed = false;
+                    if (__any_sync(0xffffffffu, dirty)) {
+                        const T q0_c = sm.q.q0[t][r][c], dph_c = sm.q.dph[t][r][c];
+                        const T rho_c = sm.rho[r + 1][c + 1];
+                        bool bad;
+                        unsigned g = ~0u;
+                        qn_v = tracer_cell_f<FastDiv>(fw, sm.s[t][r][c], sm.s[t][r][c + 1], sm.s[t][r][c + 2],
+                                                      sm.s[t][r + 1][c], sm.s[t][r + 2][c], prev1, prev2, s_km1,
+                                                      s_km2, cl_kp[c], cl_km[c], sm.mx[r][c + 1], sm.mx[r][c],
+                                                      sm.mz[r + 1][c], sm.mz[r][c], rho_c, sm.rho[r + 1][c + 2],
+                                                      sm.rho[r + 1][c], sm.rho[r + 2][c + 1], sm.rho[r][c + 1], q0_c,
+                                                      dph_c, g, bad);
+                        T snc = FastDiv::cdiv(qn_v, rho_c, sm.q.rrho[r][c], g);
+                        bad |= guard_hit(g);
+                        if (dirty && bad) {
+                            // a subnormal-range quotient or a non-finite result: the same cell with
+                            // subnormal quotients rounded explicitly (exact for every input), and
+                            // IEEE division if the result is still not finite
+                            unsigned g2 = ~0u;
+                            bool bad2;
+                            qn_v = tracer_cell_f<Div64X>(fw, sm.s[t][r][c], sm.s[t][r][c + 1], sm.s[t][r][c + 2],
+                                                         sm.s[t][r + 1][c], sm.s[t][r + 2][c], prev1, prev2, s_km1,
+                                                         s_km2, cl_kp[c], cl_km[c], sm.mx[r][c + 1], sm.mx[r][c],
+                                                         sm.mz[r + 1][c], sm.mz[r][c], rho_c, sm.rho[r + 1][c + 2],
+                                                         sm.rho[r + 1][c], sm.rho[r + 2][c + 1], sm.rho[r][c + 1],
+                                                         q0_c, dph_c, g2, bad2);
+                            snc = Div64X::cdiv(qn_v, rho_c, sm.q.rrho[r][c], g2);
+                            if (bad2) {
+                                bool unused = false;
+                                qn_v = MOIST_TILE_CELL(DivIEEE<T>, unused);
+                                snc = qn_v / rho_c;
+                            }
+                        }
+                        if (dirty) {
+                            changed = !all_dirty && !(__float_as_uint(snc) == __float_as_uint(sn));
+                            sn = snc;
+                            sm.q.qn[t][r][c] = qn_v;
+                            sm.q.snp[t][r][c] = snc;
                         }
                     }
                     if (active) {
-                        sm.q.qn[t][r][c] = qn_v;
                         prev2 = prev1;
                         prev1 = sn;
+                        c2 = c1;
+                        c1 = changed;
                     }
                     // lane r+1 reads these next step only for the column it shares with this step
                     sn_last = sn;
                     km1_used = s_km1;
+                    chg_last = changed;
+                    km1_chg_used = km1_chg;
                 }
                 __syncwarp();
                 // the boundary strips s = q / rho of the values just computed (IEEE division, as
@@ -609,15 +646,18 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
                 const T old = __ldcg(sp_prev + q * TT_W + r);
                 const T v = owned ? sm.strip_out[t][q][r] : old;
                 __stcg(sp_cur + q * TT_W + r, v);
-                if (!(v == old || (v != v && old != old))) my_changed |= (q < 2) ? 1 : 2;
+                if (!(v == old || (v != v && old != old))) (q < 2 ? right_changed : top_changed) = true;
             }
         } else {
             for (int q = 0; q < 4; q++) __stcg(sp_cur + q * TT_W + r, __ldcg(sp_prev + q * TT_W + r));
         }
-        my_changed = (__any_sync(0xffffffffu, my_changed & 1) ? 1 : 0) | (__any_sync(0xffffffffu, my_changed & 2) ? 2 : 0);
+        // lane r: row r of the right strip, column r of the top strip
+        const unsigned rmask = __ballot_sync(0xffffffffu, right_changed);
+        const unsigned tmask = __ballot_sync(0xffffffffu, top_changed);
         if (lane == 0) {
-            __stcg(chg_cur + tile, my_changed);
-            if (my_changed) atomicAdd(ctl.any_changed + pass, 1);
+            __stcg(chg_cur + 2 * tile, (int)rmask);
+            __stcg(chg_cur + 2 * tile + 1, (int)tmask);
+            if (rmask | tmask) atomicAdd(ctl.any_changed + pass, 1);
         }
         if (!grid_barrier(ctl, nblocks)) return;
         if (__ldcg(ctl.any_changed + pass) == 0) break;
