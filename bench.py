@@ -16,6 +16,9 @@ e2e:    the same metric through the reference-facing call rk3_step!(s, p) on a h
         wall clock around each call.
 roofline: the kernel group with the largest device time; achieved = its algorithmic bytes per
         launch (words per cell below x cells) / its mean launch time from the same events.
+ensemble: (1 GPU, Float32) the batched forward: 256 uneven members advanced together (one packed
+        launch per kernel of the step, one CUDA graph per step), device time per step, its
+        cell-steps/s, HBM fraction of the whole step's algorithmic bytes and ratio to `value`.
 Multi-GPU: independent replicas (the domain does not shard; ensemble members would).
 """
 import argparse
@@ -154,6 +157,35 @@ def cpu_baseline(workload, T, budget_s=12.0, max_steps=40):
                       "C++ restatement of rk3_step! (OpenMP over columns)" % (n, p.Nx, p.Nz, dt)}
 
 
+def measure_ensemble(nmem, steps, warmup, peak, plain_value):
+    """Ensemble of nmem uneven Float32 members (nx in {256, ..., 2048}, nz in {64, 96, 128},
+    seeded bubbles on the analytic sounding), one packed launch per kernel of the step for all
+    members, each step one CUDA graph; device time of `steps` steps from CUDA events. The
+    members' fields (113 MB each for 256 members) exceed L2, so no flush is needed."""
+    from moist2d_b200 import model
+    from moist2d_b200.init import ensemble_member
+    t0 = time.perf_counter()
+    mem = [ensemble_member(np.float32, member=m) for m in range(nmem)]
+    cells = sum(p.Nx * p.Nz for p, _ in mem)
+    words = words_per_cell_step(mem[0][0].ns)
+    with model.Ensemble([p for p, _ in mem]) as e:
+        for i, (_, s) in enumerate(mem):
+            e.upload(i, s)
+        setup_s = time.perf_counter() - t0
+        e.step(warmup)
+        ms = e.time_steps(steps) / steps
+        tot, g = e.profile(2)
+    value = cells / (ms / 1e3)
+    return {"members": nmem, "cells": cells, "steps": steps, "warmup": warmup, "ms_per_step": ms,
+            "value": value, "unit": "cell-steps/s", "vs_plain": value / plain_value,
+            "hbm_frac": cells * words * 4 / (ms / 1e3) / 1e9 / peak,
+            "group_ms_per_step": {k: float(x) / 2 for k, x in zip(GROUPS, g)},
+            "setup_s": setup_s,
+            "workload": "%d members, nx in {256,...,2048}, nz in {64,96,128}, dx=250 m, dz=125 m, "
+                        "dt=2 s, ns=8, one seeded bubble each on the analytic sounding, Float32 "
+                        "state with fp64 w-p elimination" % nmem}
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's CPU path (no Julia here: the threaded oracle port)."""
     if rank != 0:
@@ -201,6 +233,8 @@ def main():
     ap.add_argument("--precision", default="f32", choices=("f32", "f64"))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end measurement")
+    ap.add_argument("--ensemble", type=int, default=256,
+                    help="members of the batched-ensemble measurement (0 skips it)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -323,6 +357,14 @@ def main():
                 "peak_kind": peak_kind,
                 "step_frac": cells * words_per_cell_step(p.ns) * bpw / (t_max / 1e3) / 1e9 / peak}
 
+    m.close()
+    ens = None
+    if rank == 0 and world == 1 and args.ensemble > 0 and args.precision == "f32":
+        try:
+            ens = measure_ensemble(args.ensemble, max(3, min(args.steps, 10)), args.warmup, peak, value)
+        except Exception as e:  # the ensemble must not hide the single-domain number
+            ens = {"value": None, "error": str(e)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -347,10 +389,10 @@ def main():
             "gpu_launches": int(launches.sum()),
             "kernel_ms_per_step": {g: float(group_ms[j] / args.steps) for j, g in enumerate(gnames)},
             "clocks": clk,
+            "ensemble": ens,
         }
         print(json.dumps(line), flush=True)
 
-    m.close()
     if world > 1:
         dist.destroy_process_group()
 

@@ -268,6 +268,37 @@ int moist_batch_profile(moist_batch* b, int nsteps, float* total_ms, float* grou
 const char* moist_batch_last_error(const moist_batch* b);
 int moist_batch_nan_member(const moist_batch* b);
 
+/* ---- Adjoint (no counterpart in the reference, which has no derivatives; a Julia caller
+ * exposes it as the pullback of a ChainRulesCore.rrule around rk3_step!).
+ *
+ * moist_adjoint_run advances the context State nsteps large steps (as moist_rk3_step does, the
+ * context is left at the final State) and returns the gradient of the objective
+ *   J = sum_i prec_weight[i] * prec_final[i] + sum_f sum_(k,i) state[f](k,i) * S_final_f(k,i)
+ * with respect to the initial State's seven prognostic fields, the initial prec and the Kessler
+ * parameters K_auto and Qc_threshold. The gradient is the discrete adjoint of the computed step:
+ * the reverse sweep goes step by step from the last step, each step recomputed from its input
+ * State (kept every ckpt_every steps and recomputed in between) with its stage internals
+ * taped, and adjoint variables in double whatever the context precision. Branch points
+ * (upwind and limiter switches, Kessler clamps) contribute the derivative of the branch taken.
+ * Needs do_sf = do_rd = 0 (MOIST_ERR_UNSUPPORTED otherwise). Device memory: about
+ * (nsteps / ckpt_every + ckpt_every) States plus 3*ns + 40 fields of one step. */
+typedef struct moist_adjoint_seed {
+    const double* prec_weight; /* (ia) d J / d prec_final, or NULL */
+    const double* state[7];    /* (ka, ia) d J / d S_final of rho, rho_u, rho_w, rho_theta,
+                                  rho_qv, rho_qc, rho_qr, or NULL */
+} moist_adjoint_seed;
+typedef struct moist_adjoint_grad {
+    double* state[7];          /* (ka, ia) d J / d S_initial (halo columns 0), or NULL to skip */
+    double* prec;              /* (ia) d J / d prec_initial, or NULL */
+    double k_auto;             /* d J / d K_auto */
+    double qc_threshold;       /* d J / d Qc_threshold */
+    double objective;          /* J */
+    double forward_ms;         /* wall time of the forward run */
+    double reverse_ms;         /* wall time of the reverse sweep (recomputation included) */
+} moist_adjoint_grad;
+int moist_adjoint_run(moist_ctx* ctx, int nsteps, int ckpt_every, const moist_adjoint_seed* seed,
+                      moist_adjoint_grad* out);
+
 /* Kernel groups of one large step, for moist_step_profile. */
 enum {
     MOIST_KGROUP_PHYSICS = 0,   /* surface fluxes, radiation, Kessler + sedimentation + phys assembly */

@@ -3,7 +3,7 @@ library or a CUDA device is missing, calls raise."""
 import ctypes as C
 import os
 
-from .abi import moist_params, moist_state_host
+from .abi import moist_adjoint_grad, moist_adjoint_seed, moist_params, moist_state_host
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 SO_PATH = os.path.join(_HERE, "libmoist2d_sm100a.so")
@@ -18,7 +18,7 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_implicit_correction_noalloc", "moist_tracer_pass_counts", "moist_batch_create",
            "moist_batch_destroy", "moist_batch_member", "moist_batch_upload", "moist_batch_download",
            "moist_batch_step", "moist_batch_time_steps", "moist_batch_last_error", "moist_batch_nan_member",
-           "moist_batch_profile")
+           "moist_batch_profile", "moist_adjoint_run")
 
 
 def lib():
@@ -71,5 +71,6 @@ def lib():
         L.moist_batch_last_error.restype = C.c_char_p
         L.moist_batch_nan_member.argtypes = [B]
         L.moist_batch_profile.argtypes = [B, I, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.moist_adjoint_run.argtypes = [Ctx, I, I, C.POINTER(moist_adjoint_seed), C.POINTER(moist_adjoint_grad)]
         _lib = L
     return _lib

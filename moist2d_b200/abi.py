@@ -34,6 +34,9 @@ MOIST_HELPER_SAT_Q = 3
 MOIST_HELPER_EXP = 4
 MOIST_HELPER_POW = 5
 
+# the seven prognostic fields of State (moist.jl:296-302), in the order of the adjoint's arrays
+PROGNOSTIC = ("rho", "rho_u", "rho_w", "rho_theta", "rho_qv", "rho_qc", "rho_qr")
+
 # field names in the order compute_step! checks them for NaN (moist.jl:1543-1577)
 NAN_FIELDS = ("rho", "rho_u", "rho_w", "rho_theta", "rho_qv", "rho_qc", "rho_qr",
               "d_rho_u_phys", "d_rho_theta_phys", "d_rho_qv_phys", "d_rho_qc_phys",
@@ -74,3 +77,13 @@ STATE_FIELDS = ("rho", "rho_u", "rho_w", "rho_theta", "rho_qv", "rho_qc", "rho_q
 
 class moist_state_host(C.Structure):
     _fields_ = [(f, C.c_void_p) for f in STATE_FIELDS]
+
+
+class moist_adjoint_seed(C.Structure):
+    _fields_ = [("prec_weight", C.c_void_p), ("state", C.c_void_p * 7)]
+
+
+class moist_adjoint_grad(C.Structure):
+    _fields_ = [("state", C.c_void_p * 7), ("prec", C.c_void_p), ("k_auto", C.c_double),
+                ("qc_threshold", C.c_double), ("objective", C.c_double), ("forward_ms", C.c_double),
+                ("reverse_ms", C.c_double)]

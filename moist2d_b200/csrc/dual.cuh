@@ -1,0 +1,174 @@
+// dual.cuh - forward-mode dual numbers for the local Jacobians of the adjoint (adjoint.cuh).
+//
+// Dual<N> carries a value and N directional derivatives, all in double. The device building
+// blocks of the large step (model.cuh) are templates over their scalar type, so instantiating
+// them with Dual<N> gives the partial derivatives of a cell's outputs with respect to N seeded
+// inputs in one evaluation. Branches and min/max select on the value, so a derivative is the
+// derivative of the branch the forward step took (the one-sided derivative at a kink).
+//
+// The mm:: overloads must be declared before model.cuh is parsed: its templates call mm::mpow
+// and friends by qualified name, which binds to the overloads visible at the template's
+// definition.
+#pragma once
+
+#include "moist_math.h"
+
+namespace mm {
+
+template <int N>
+struct Dual {
+    double v;
+    double d[N];
+    MM_HD Dual() : v(0.0) {
+#pragma unroll
+        for (int j = 0; j < N; j++) d[j] = 0.0;
+    }
+    MM_HD Dual(double x) : v(x) {
+#pragma unroll
+        for (int j = 0; j < N; j++) d[j] = 0.0;
+    }
+    // a value seeded in direction j
+    MM_HD static Dual seed(double x, int j) {
+        Dual r(x);
+#pragma unroll
+        for (int q = 0; q < N; q++) r.d[q] = (q == j) ? 1.0 : 0.0;
+        return r;
+    }
+};
+
+template <int N>
+MM_HD Dual<N> operator+(const Dual<N>& a, const Dual<N>& b) {
+    Dual<N> r;
+    r.v = a.v + b.v;
+#pragma unroll
+    for (int j = 0; j < N; j++) r.d[j] = a.d[j] + b.d[j];
+    return r;
+}
+template <int N>
+MM_HD Dual<N> operator-(const Dual<N>& a, const Dual<N>& b) {
+    Dual<N> r;
+    r.v = a.v - b.v;
+#pragma unroll
+    for (int j = 0; j < N; j++) r.d[j] = a.d[j] - b.d[j];
+    return r;
+}
+template <int N>
+MM_HD Dual<N> operator-(const Dual<N>& a) {
+    Dual<N> r;
+    r.v = -a.v;
+#pragma unroll
+    for (int j = 0; j < N; j++) r.d[j] = -a.d[j];
+    return r;
+}
+template <int N>
+MM_HD Dual<N> operator*(const Dual<N>& a, const Dual<N>& b) {
+    Dual<N> r;
+    r.v = a.v * b.v;
+#pragma unroll
+    for (int j = 0; j < N; j++) r.d[j] = a.d[j] * b.v + a.v * b.d[j];
+    return r;
+}
+template <int N>
+MM_HD Dual<N> operator/(const Dual<N>& a, const Dual<N>& b) {
+    Dual<N> r;
+    const double q = a.v / b.v;
+    r.v = q;
+#pragma unroll
+    for (int j = 0; j < N; j++) r.d[j] = (a.d[j] - q * b.d[j]) / b.v;
+    return r;
+}
+template <int N>
+MM_HD Dual<N>& operator+=(Dual<N>& a, const Dual<N>& b) {
+    a = a + b;
+    return a;
+}
+template <int N>
+MM_HD Dual<N>& operator-=(Dual<N>& a, const Dual<N>& b) {
+    a = a - b;
+    return a;
+}
+template <int N>
+MM_HD Dual<N>& operator*=(Dual<N>& a, const Dual<N>& b) {
+    a = a * b;
+    return a;
+}
+
+// mixed forms (template deduction does not apply the converting constructor)
+#define MM_DUAL_MIXED(op)                                                                  \
+    template <int N>                                                                       \
+    MM_HD Dual<N> operator op(const Dual<N>& a, double b) { return a op Dual<N>(b); }      \
+    template <int N>                                                                       \
+    MM_HD Dual<N> operator op(double a, const Dual<N>& b) { return Dual<N>(a) op b; }
+MM_DUAL_MIXED(+)
+MM_DUAL_MIXED(-)
+MM_DUAL_MIXED(*)
+MM_DUAL_MIXED(/)
+#undef MM_DUAL_MIXED
+
+#define MM_DUAL_CMP(op)                                                                    \
+    template <int N>                                                                       \
+    MM_HD bool operator op(const Dual<N>& a, const Dual<N>& b) { return a.v op b.v; }     \
+    template <int N>                                                                       \
+    MM_HD bool operator op(const Dual<N>& a, double b) { return a.v op b; }               \
+    template <int N>                                                                       \
+    MM_HD bool operator op(double a, const Dual<N>& b) { return a op b.v; }
+MM_DUAL_CMP(<)
+MM_DUAL_CMP(>)
+MM_DUAL_CMP(<=)
+MM_DUAL_CMP(>=)
+MM_DUAL_CMP(==)
+MM_DUAL_CMP(!=)
+#undef MM_DUAL_CMP
+
+template <int N>
+MM_HD bool signbit_(const Dual<N>& x) {
+    return signbit_(x.v);
+}
+
+template <int N>
+MM_HD Dual<N> mexp(const Dual<N>& x) {
+    Dual<N> r;
+    const double e = exp_d(x.v);
+    r.v = e;
+#pragma unroll
+    for (int j = 0; j < N; j++) r.d[j] = e * x.d[j];
+    return r;
+}
+
+// x^y for x > 0: d(x^y) = x^y (y dx / x + log(x) dy)
+template <int N>
+MM_HD Dual<N> mpow(const Dual<N>& x, const Dual<N>& y) {
+    Dual<N> r;
+    const double p = pow_d(x.v, y.v);
+    r.v = p;
+    bool dy = false;
+#pragma unroll
+    for (int j = 0; j < N; j++) dy = dy || (y.d[j] != 0.0);
+    const double lx = (dy && x.v > 0.0) ? log_d(x.v) : 0.0;
+    const double gx = x.v != 0.0 ? p * y.v / x.v : 0.0;
+#pragma unroll
+    for (int j = 0; j < N; j++) r.d[j] = gx * x.d[j] + p * lx * y.d[j];
+    return r;
+}
+template <int N>
+MM_HD Dual<N> mpow(const Dual<N>& x, double y) {
+    return mpow(x, Dual<N>(y));
+}
+
+template <int N>
+MM_HD Dual<N> msqrt(const Dual<N>& x) {
+    Dual<N> r;
+    const double s = sqrt(x.v);
+    r.v = s;
+    const double g = s > 0.0 ? 0.5 / s : 0.0;
+#pragma unroll
+    for (int j = 0; j < N; j++) r.d[j] = g * x.d[j];
+    return r;
+}
+
+template <int N>
+MM_HD Dual<N> mabs(const Dual<N>& x) {
+    return x.v < 0.0 ? -x : x;
+}
+
+}  // namespace mm

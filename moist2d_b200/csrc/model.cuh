@@ -14,6 +14,7 @@
 #include <stdint.h>
 
 #include "moist_math.h"
+#include "dual.cuh"  // the templates below also instantiate over dual numbers (adjoint.cuh)
 
 namespace moist {
 

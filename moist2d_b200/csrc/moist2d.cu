@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -16,6 +18,7 @@
 #include "../../include/moist2d.h"
 #include "kernels.cuh"
 #include "batch.cuh"
+#include "adjoint.cuh"
 
 using namespace moist;
 
@@ -47,6 +50,7 @@ struct CtxBase {
     virtual int profile(int nsteps, float* total_ms, float* group_ms, long long* group_launches) = 0;
     virtual int rk3_host(moist_state_host* s, int nsteps) = 0;
     virtual int pass_counts(int* counts, int n) = 0;
+    virtual int adjoint_run(int nsteps, int ckpt, const moist_adjoint_seed* seed, moist_adjoint_grad* out) = 0;
 };
 
 struct BatchBase {
@@ -164,6 +168,30 @@ DevParams<T> make_params(const moist_params* c, int P) {
     return p;
 }
 
+// the parameters in double, each scalar as the context precision holds it (grid pointers unset)
+template <class T>
+DevParams<double> params_to_double(const DevParams<T>& q) {
+    DevParams<double> p{};
+    p.nx = q.nx;
+    p.nz = q.nz;
+    p.P = q.P;
+#define PC(f) p.f = (double)q.f;
+    PC(dx) PC(dt) PC(H) PC(nu) PC(kappa) PC(gamma_d) PC(beta) PC(zf_sponge)
+    PC(EPS) PC(GRAV) PC(Rd) PC(Rv) PC(Cpd) PC(Cpv) PC(Cpl) PC(P0) PC(Lv) PC(SIGMA) PC(EPSvap)
+    PC(K_auto) PC(Qc_threshold) PC(K_accr) PC(K_evap) PC(A_term) PC(B_term) PC(T0) PC(ES0) PC(A_SAT) PC(B_SAT)
+    PC(Cd) PC(Ch) PC(Ce) PC(uabs_min) PC(temp_surf) PC(k_abs_qv) PC(k_abs_qc) PC(k_abs_qr) PC(surf_emissivity)
+    PC(tau_cooling) PC(z_trop)
+#undef PC
+    p.do_mp = q.do_mp;
+    p.do_auto = q.do_auto;
+    p.do_accr = q.do_accr;
+    p.do_revap = q.do_revap;
+    p.do_sed = q.do_sed;
+    p.do_rd = q.do_rd;
+    p.do_sf = q.do_sf;
+    return p;
+}
+
 template <class T, class TT>
 struct Ctx : CtxBase {
     moist_ctx* owner;
@@ -203,6 +231,31 @@ struct Ctx : CtxBase {
     // column strips of the factorisation and the acoustic substeps
     int strip_wc = 1;
     size_t strip_smem = 0;
+    // adjoint tape: when set, run_stage copies the stage internals the reverse sweep needs
+    struct Tape {
+        T* in[3][7];                           // stage inputs
+        std::vector<std::array<T*, 4>> sub[3]; // rho_p, rho_u_p, rho_w_p, rho_theta_p after substep n (0: start)
+        T* rrt[3];                             // R_rho_theta
+        T* mf[3][2];                           // momentum fluxes after the substeps
+        T* qout[3][3];                         // tracer sweep results
+    };
+    Tape* tape = nullptr;
+    int tape_stage = 0;
+    // buffers of moist_adjoint_run, allocated on its first call
+    struct Adj {
+        DevParams<double> pd;
+        double *dz, *z, *zf;
+        double *Lst[7], *LS0[7], *Lph[5], *seed[7];
+        double* acc;  // 16 per-stage accumulators, contiguous (one memset)
+        double *Lqout[3], *mu[3], *J, *LP[2][4];
+        double *Ta, *Tb, *Tc, *Lx, *Ly, *Ctmp, *Ltp_rho, *Ltp_rt, *Linc_rho, *Linc_rt, *Lsed;
+        double *Lpar, *obj, *prec_w, *stage;
+        Tape tp;
+        std::vector<std::array<T*, 7>> ck;   // States every ckpt_every steps
+        std::vector<std::array<T*, 7>> seg;  // the States of one segment
+        std::array<T*, 8> fin;               // the final State and prec
+    };
+    Adj* adj = nullptr;
     // profiling: events recorded before each kernel group when active
     bool prof_on = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -232,6 +285,7 @@ struct Ctx : CtxBase {
 
     ~Ctx() override {
         if (st) cudaStreamSynchronize(st);
+        delete adj;
         for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
         for (void* a : allocs) cudaFree(a);
     }
@@ -252,6 +306,22 @@ struct Ctx : CtxBase {
         if (r_ != MOIST_OK) return r_;           \
         CK(cudaMemsetAsync((ptr), 0, std::max<size_t>((n), 1) * sizeof(*(ptr)), st)); \
     } while (0)
+
+    // device copies of nf whole fields (up to 8) in one launch
+    int copyf(const T* const* src, T* const* dst, int nf, size_t n = 0) {
+        if (n == 0) n = fsz;
+        for (int f0 = 0; f0 < nf; f0 += 8) {
+            CopyList<T> l{};
+            l.nf = std::min(8, nf - f0);
+            for (int j = 0; j < l.nf; j++) {
+                l.src[j] = src[f0 + j];
+                l.dst[j] = dst[f0 + j];
+            }
+            k_copy_fields<T><<<std::min<size_t>(1184, (n + 255) / 256), 256, 0, st>>>(l, n);
+            CKL();
+        }
+        return MOIST_OK;
+    }
 
     int init(const moist_params* c) {
         nx = c->nx;
@@ -539,6 +609,11 @@ struct Ctx : CtxBase {
 
     int run_stage(StateP<T> s_in, StateP<T> s0, T* const qout[3], StateP<T> s_out, T dt_stage, int ns_s) {
         const dim3 b2(32, 8), g2(cdiv(nx, 32), cdiv(nz, 8));
+        const int js = tape_stage;
+        if (tape) {
+            const T* src[7] = {s_in.rho, s_in.ru, s_in.rw, s_in.rt, s_in.qv, s_in.qc, s_in.qr};
+            if (int r = copyf(src, tape->in[js], 7)) return r;
+        }
         MARK(MOIST_KGROUP_PROLOGUE, 3);
         TendArgs<T> ta_{s_in, s0, ph, pres, theta, uface, wface, R_rho, R_ru, R_rw, R_rt, rho_p, ru_p[0], rw_p,
                         rt_p[0], mfx, mfz, halo_vals, halo_vals + 1};
@@ -556,6 +631,12 @@ struct Ctx : CtxBase {
             k_thomas_strip<T, TT><<<gs, STRIP_THREADS, strip_smem, st>>>(dp, theta, rt2p, dt_s, strip_wc, ta, tb, tc,
                                                                          tcp, tpiv, err);
             CKL();
+        }
+        if (tape) {
+            const T* src[5] = {rho_p, ru_p[0], rw_p, rt_p[0], R_rt};
+            T* dst[5] = {tape->sub[js][0][0], tape->sub[js][0][1], tape->sub[js][0][2], tape->sub[js][0][3],
+                         tape->rrt[js]};
+            if (int r = copyf(src, dst, 5)) return r;
         }
         const double fact_tp64 = (double)T(0.5) * (1.0 + (double)dp.beta);
         for (int n = 1; n <= ns_s; n++) {
@@ -590,6 +671,14 @@ struct Ctx : CtxBase {
             k_substep_strip<T, TT><<<gs, STRIP_THREADS, strip_smem, st>>>(dp, sa, dt_s, T(ns_s), fact_tp64, strip_wc,
                                                                           err);
             CKL();
+            if (tape) {
+                const T* src[4] = {rho_p, ru_p[n % 2], rw_p, rt_p[n % 3]};
+                if (int r = copyf(src, tape->sub[js][n].data(), 4)) return r;
+            }
+        }
+        if (tape) {
+            const T* src[2] = {mfx, mfz};
+            if (int r = copyf(src, tape->mf[js], 2)) return r;
         }
         TracerArgs<T> tr;
         const T* qin[3] = {s_in.qv, s_in.qc, s_in.qr};
@@ -633,6 +722,10 @@ struct Ctx : CtxBase {
             k_tracer_wavefront<T><<<3, nthr, 3 * nz * sizeof(T), st>>>(dp, tr, err);
             CKL();
         }
+        if (tape) {
+            const T* src[3] = {qout[0], qout[1], qout[2]};
+            if (int r = copyf(src, tape->qout[js], 3)) return r;
+        }
         MARK(MOIST_KGROUP_UPDATE, 2);
         UpdArgs<T> ua{s_in, s_out, rho_p, ru_p[ns_s % 2], rw_p, rt_p[ns_s % 3], ph};
         if (rec) {
@@ -661,8 +754,11 @@ struct Ctx : CtxBase {
         const int ns1 = std::max(1, (int)std::ceil(ns / 3.0));
         const int ns2 = std::max(1, (int)std::ceil(ns / 2.0));
         T* const nq[3] = {nxt.qv, nxt.qc, nxt.qr};
+        tape_stage = 0;
         if ((r = run_stage(cur, cur, nq, nxt, dt / T(3), ns1)) != MOIST_OK) return r;
+        tape_stage = 1;
         if ((r = run_stage(nxt, cur, tmpq, with_q(nxt, tmpq), dt / T(2), ns2)) != MOIST_OK) return r;
+        tape_stage = 2;
         if ((r = run_stage(with_q(nxt, tmpq), cur, nq, nxt, dt, ns)) != MOIST_OK) return r;
         MARK(MOIST_KGROUP_OTHER, 1);
         if (rec) {
@@ -815,6 +911,326 @@ struct Ctx : CtxBase {
         CK(cudaMemcpyAsync(out, bud_res, 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         return MOIST_OK;
+    }
+
+    // ------------------------------------------------------------------ adjoint (adjoint.cuh)
+    int stage_substeps(int j) const {
+        return j == 0 ? std::max(1, (int)std::ceil(ns / 3.0)) : (j == 1 ? std::max(1, (int)std::ceil(ns / 2.0)) : ns);
+    }
+
+    int adj_alloc(int nsteps, int ckpt) {
+        if (!adj) {
+            adj = new Adj();
+            Adj& A = *adj;
+            std::vector<T> h(nz);
+            std::vector<double> hd(nz);
+            double** g[3] = {&A.dz, &A.z, &A.zf};
+            const T* src[3] = {g_dz, g_z, g_zf};
+            for (int j = 0; j < 3; j++) {
+                AL(*g[j], (size_t)nz);
+                CK(cudaMemcpyAsync(h.data(), src[j], nz * sizeof(T), cudaMemcpyDeviceToHost, st));
+                CK(cudaStreamSynchronize(st));
+                for (int k = 0; k < nz; k++) hd[k] = (double)h[k];
+                CK(cudaMemcpyAsync(*g[j], hd.data(), nz * sizeof(double), cudaMemcpyHostToDevice, st));
+                CK(cudaStreamSynchronize(st));
+            }
+            A.pd = params_to_double(dp);
+            A.pd.dz = A.dz;
+            A.pd.z = A.z;
+            A.pd.zf = A.zf;
+            for (int f = 0; f < 7; f++) {
+                AL(A.Lst[f], fsz);
+                AL(A.LS0[f], fsz);
+                AL(A.seed[f], fsz);
+            }
+            for (int f = 0; f < 5; f++) AL(A.Lph[f], fsz);
+            AL(A.acc, 16 * fsz);
+            for (int t = 0; t < 3; t++) {
+                AL(A.Lqout[t], fsz);
+                AL(A.mu[t], fsz);
+            }
+            AL(A.J, 3 * TR_SLOTS * fsz);
+            for (int q = 0; q < 2; q++)
+                for (int f = 0; f < 4; f++) AL(A.LP[q][f], fsz);
+            for (double** f : {&A.Ta, &A.Tb, &A.Tc, &A.Lx, &A.Ly, &A.Ctmp, &A.Ltp_rho, &A.Ltp_rt, &A.Linc_rho,
+                               &A.Linc_rt, &A.Lsed})
+                AL(*f, fsz);
+            AL(A.Lpar, 2);
+            AL(A.obj, 1);
+            AL(A.prec_w, (size_t)P);
+            AL(A.stage, (size_t)nz * (nx + 2 * halo));
+            Tape& tp = A.tp;
+            for (int j = 0; j < 3; j++) {
+                for (int f = 0; f < 7; f++) AL(tp.in[j][f], fsz);
+                tp.sub[j].resize(stage_substeps(j) + 1);
+                for (auto& a : tp.sub[j])
+                    for (int f = 0; f < 4; f++) AL(a[f], fsz);
+                AL(tp.rrt[j], fsz);
+                AL(tp.mf[j][0], fsz);
+                AL(tp.mf[j][1], fsz);
+                for (int t = 0; t < 3; t++) AL(tp.qout[j][t], fsz);
+            }
+            for (int f = 0; f < 7; f++) AL(A.fin[f], fsz);
+            AL(A.fin[7], (size_t)P);
+        }
+        Adj& A = *adj;
+        const size_t nck = (size_t)((nsteps + ckpt - 1) / ckpt);
+        while (A.ck.size() < nck) {
+            std::array<T*, 7> a;
+            for (int f = 0; f < 7; f++) AL(a[f], fsz);
+            A.ck.push_back(a);
+        }
+        while (A.seg.size() < (size_t)ckpt) {
+            std::array<T*, 7> a;
+            for (int f = 0; f < 7; f++) AL(a[f], fsz);
+            A.seg.push_back(a);
+        }
+        return MOIST_OK;
+    }
+
+    std::array<T*, 7> cur_fields() const { return {cur.rho, cur.ru, cur.rw, cur.rt, cur.qv, cur.qc, cur.qr}; }
+
+    // the adjoint of one large step: lambda of the step's output State in A.Lst becomes the
+    // lambda of its input State; the tape holds the step's internals
+    int adj_step() {
+        Adj& A = *adj;
+        Tape& tp = A.tp;
+        const dim3 b(ADJ_THREADS), gc(cdiv(nx, ADJ_THREADS), nz), gc3(cdiv(nx, ADJ_THREADS), nz, 3);
+        const unsigned gcol = cdiv(nx, 128);
+        const dim3 b2(32, 8), g2(cdiv(nx, 32), cdiv(nz, 8));
+        const T dtT = dp.dt;
+        const T dst[3] = {dtT / T(3), dtT / T(2), dtT};
+        const T fact_tpT = T(0.5) * (T(1.0) + dp.beta), fact_tmT = T(0.5) * (T(1.0) - dp.beta);
+        int lp = 0;
+        for (int j = 2; j >= 0; j--) {
+            const int m = stage_substeps(j);
+            const StateP<T> s{tp.in[j][0], tp.in[j][1], tp.in[j][2], tp.in[j][3], tp.in[j][4], tp.in[j][5], tp.in[j][6]};
+            k_diag<T><<<g2, b2, 0, st>>>(dp, s, pres, theta, rt2p, uface, wface, err);
+            AdjStage<T> a{};
+            a.s = s;
+            a.theta = theta;
+            a.rt2 = rt2p;
+            a.pres = pres;
+            a.uf = uface;
+            a.wf = wface;
+            a.rrt = tp.rrt[j];
+            a.mfx = tp.mf[j][0];
+            a.mfz = tp.mf[j][1];
+            for (int t = 0; t < 3; t++) {
+                a.qout[t] = tp.qout[j][t];
+                a.q0[t] = tp.in[0][4 + t];
+                a.Lqout[t] = A.Lqout[t];
+            }
+            a.dt_stage = (double)dst[j];
+            a.dt_s = (double)(dst[j] / T(m));
+            a.m = m;
+            a.fact_tp64 = (double)T(0.5) * (1.0 + (double)dp.beta);
+            a.fact = (double)(fact_tmT / fact_tpT);
+            for (int f = 0; f < 7; f++) {
+                a.Lst[f] = A.Lst[f];
+                a.LS0[f] = A.LS0[f];
+            }
+            for (int f = 0; f < 5; f++) a.Lph[f] = A.Lph[f];
+            double* acc[16];
+            for (int q = 0; q < 16; q++) acc[q] = A.acc + (size_t)q * fsz;
+            a.LRrho = acc[0];
+            a.LRu = acc[1];
+            a.LRw = acc[2];
+            a.LRt = acc[3];
+            a.Ltheta = acc[4];
+            a.Lrt2 = acc[5];
+            a.Lpres = acc[6];
+            a.Luf = acc[7];
+            a.Lwf = acc[8];
+            a.La = acc[9];
+            a.Lb = acc[10];
+            a.Lc = acc[11];
+            a.Lmfx = acc[12];
+            a.Lmfz = acc[13];
+            a.Lpend[0] = acc[14];
+            a.Lpend[1] = acc[15];
+            a.Ta = A.Ta;
+            a.Tb = A.Tb;
+            a.Tc = A.Tc;
+            a.Lx = A.Lx;
+            a.Ly = A.Ly;
+            a.Ctmp = A.Ctmp;
+            a.Ltp_rho = A.Ltp_rho;
+            a.Ltp_rt = A.Ltp_rt;
+            a.Linc_rho = A.Linc_rho;
+            a.Linc_rt = A.Linc_rt;
+            CK(cudaMemsetAsync(A.acc, 0, 16 * fsz * sizeof(double), st));
+            k_adj_tri_coef<T><<<gcol, 128, 0, st>>>(A.pd, a);
+            DP<4> LPc{{A.LP[lp][0], A.LP[lp][1], A.LP[lp][2], A.LP[lp][3]}};
+            k_adj_update<T><<<gc, b, 0, st>>>(A.pd, a, LPc);
+            k_adj_tr_jac<T><<<gc3, b, 0, st>>>(A.pd, a, A.J);
+            const DP<3> lq{{A.Lqout[0], A.Lqout[1], A.Lqout[2]}}, mu{{A.mu[0], A.mu[1], A.mu[2]}};
+            k_adj_tr_rev<<<3, (nz + 31) / 32 * 32, 3 * nz * sizeof(double), st>>>(nx, nz, P, A.J, lq, mu);
+            k_adj_tr_scatter<T><<<gc3, b, 0, st>>>(A.pd, a, A.J, mu);
+            k_adj_mf<T><<<gc, b, 0, st>>>(A.pd, a);
+            for (int n = m; n >= 1; n--) {
+                AdjSub<T> sb;
+                sb.prev_rt = tp.sub[j][n - 1][3];
+                sb.prev_rw = tp.sub[j][n - 1][2];
+                sb.old_rt = tp.sub[j][std::max(n - 2, 0)][3];
+                sb.ru = tp.sub[j][n][1];
+                sb.rw = tp.sub[j][n][2];
+                for (int f = 0; f < 4; f++) {
+                    sb.LPn[f] = A.LP[lp][f];
+                    sb.LPo[f] = A.LP[1 - lp][f];
+                }
+                sb.n = n;
+                k_adj_sub_vert<T><<<gc, b, 0, st>>>(A.pd, a, sb);
+                k_adj_sub_thomas<T><<<gcol, 128, 0, st>>>(A.pd, dp, a, sb);
+                k_adj_sub_expl<T><<<gc, b, 0, st>>>(A.pd, a, sb);
+                k_adj_sub_horiz<T><<<gc, b, 0, st>>>(A.pd, a, sb);
+                lp = 1 - lp;
+            }
+            DP<4> LP0{{A.LP[lp][0], A.LP[lp][1], A.LP[lp][2], A.LP[lp][3]}};
+            k_adj_p0<T><<<gc, b, 0, st>>>(A.pd, a, LP0);
+            k_adj_tri_coef_T<T><<<gcol, 128, 0, st>>>(A.pd, a);
+            k_adj_tend_T<T><<<gc, b, 0, st>>>(A.pd, a);
+            k_adj_face_T<T><<<gc, b, 0, st>>>(A.pd, a);
+            k_adj_diag_T<T><<<gc, b, 0, st>>>(A.pd, a);
+            CKL();
+        }
+        AdjPhys<T> ph;
+        ph.s = StateP<T>{tp.in[0][0], tp.in[0][1], tp.in[0][2], tp.in[0][3], tp.in[0][4], tp.in[0][5], tp.in[0][6]};
+        ph.sed = d_qr_sed;
+        for (int f = 0; f < 7; f++) ph.Lst[f] = A.Lst[f];
+        for (int f = 0; f < 5; f++) ph.Lph[f] = A.Lph[f];
+        ph.Lsed = A.Lsed;
+        ph.prec_w = A.prec_w;
+        ph.Lpar = A.Lpar;
+        k_adj_kessler<T><<<gc, b, 0, st>>>(A.pd, ph);
+        k_adj_sed<T><<<gc, b, 0, st>>>(A.pd, ph);
+        DP<7> L7, S7;
+        DP<5> L5;
+        for (int f = 0; f < 7; f++) {
+            L7.f[f] = A.Lst[f];
+            S7.f[f] = A.LS0[f];
+        }
+        for (int f = 0; f < 5; f++) L5.f[f] = A.Lph[f];
+        k_adj_step_end<<<gc, b, 0, st>>>(nx, nz, P, L7, S7, L5);
+        CKL();
+        return MOIST_OK;
+    }
+
+    int adjoint_run(int nsteps, int ckpt, const moist_adjoint_seed* seed, moist_adjoint_grad* out) override {
+        if (int r = check_stage_shape()) return r;
+        if (!out || nsteps < 1 || ckpt < 1)
+            return set_err(owner, MOIST_ERR_ARG, "moist_adjoint_run needs out != NULL, nsteps >= 1 and ckpt_every >= 1");
+        if (dp.do_sf || dp.do_rd)
+            return set_err(owner, MOIST_ERR_UNSUPPORTED,
+                           "moist_adjoint_run covers do_sf = do_rd = 0 (surface fluxes and radiation are not differentiated)");
+        ckpt = std::min(ckpt, nsteps);
+        if (int r = adj_alloc(nsteps, ckpt)) return r;
+        Adj& A = *adj;
+        const int ia = nx + 2 * halo;
+        const dim3 b(ADJ_THREADS), gc(cdiv(nx, ADJ_THREADS), nz), gr(cdiv(ia, ADJ_THREADS), nz);
+        // seeds
+        bool seed_on[7];
+        for (int f = 0; f < 7; f++) {
+            const double* h = seed ? seed->state[f] : nullptr;
+            seed_on[f] = h != nullptr;
+            if (h) {
+                CK(cudaMemcpyAsync(A.stage, h, (size_t)nz * ia * sizeof(double), cudaMemcpyHostToDevice, st));
+                k_adj_from_ref<<<gc, b, 0, st>>>(nx, nz, halo, P, A.stage, A.seed[f]);
+                CKL();
+            }
+        }
+        const bool prec_on = seed && seed->prec_weight;
+        if (prec_on) CK(cudaMemcpyAsync(A.prec_w, seed->prec_weight + halo, nx * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(reset_err());
+        int r;
+        // forward run, keeping the State every ckpt steps
+        const auto t0 = std::chrono::steady_clock::now();
+        for (int n = 0; n < nsteps; n++) {
+            if (n % ckpt == 0) {
+                const auto src = cur_fields();
+                if ((r = copyf(src.data(), A.ck[n / ckpt].data(), 7)) != MOIST_OK) return r;
+            }
+            if ((r = launch_step()) != MOIST_OK) return r;
+        }
+        CK(cudaStreamSynchronize(st));
+        const auto t1 = std::chrono::steady_clock::now();
+        // objective and the final State
+        CK(cudaMemsetAsync(A.obj, 0, sizeof(double), st));
+        DP<7> sd;
+        for (int f = 0; f < 7; f++) sd.f[f] = seed_on[f] ? A.seed[f] : nullptr;
+        k_adj_objective<T><<<gc, b, 0, st>>>(nx, nz, P, cur, prec, prec_on ? A.prec_w : nullptr, sd, A.obj);
+        CKL();
+        {
+            const auto src = cur_fields();
+            if ((r = copyf(src.data(), A.fin.data(), 7)) != MOIST_OK) return r;
+            CK(cudaMemcpyAsync(A.fin[7], prec, P * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        }
+        // lambda of the final State = the seeds
+        for (int f = 0; f < 7; f++) {
+            if (seed_on[f])
+                CK(cudaMemcpyAsync(A.Lst[f], A.seed[f], fsz * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            else
+                CK(cudaMemsetAsync(A.Lst[f], 0, fsz * sizeof(double), st));
+            CK(cudaMemsetAsync(A.LS0[f], 0, fsz * sizeof(double), st));
+        }
+        for (int f = 0; f < 5; f++) CK(cudaMemsetAsync(A.Lph[f], 0, fsz * sizeof(double), st));
+        CK(cudaMemsetAsync(A.Lpar, 0, 2 * sizeof(double), st));
+        if (!prec_on) CK(cudaMemsetAsync(A.prec_w, 0, P * sizeof(double), st));
+        // reverse sweep, one segment of ckpt steps at a time
+        const int nck = (nsteps + ckpt - 1) / ckpt;
+        for (int sg = nck - 1; sg >= 0; sg--) {
+            const int n0 = sg * ckpt, n1 = std::min(n0 + ckpt, nsteps);
+            {
+                const auto dstf = cur_fields();
+                if ((r = copyf(A.ck[sg].data(), dstf.data(), 7)) != MOIST_OK) return r;
+                if ((r = copyf(A.ck[sg].data(), A.seg[0].data(), 7)) != MOIST_OK) return r;
+            }
+            for (int n = n0; n < n1 - 1; n++) {
+                if ((r = launch_step()) != MOIST_OK) return r;
+                const auto src = cur_fields();
+                if ((r = copyf(src.data(), A.seg[n - n0 + 1].data(), 7)) != MOIST_OK) return r;
+            }
+            for (int n = n1 - 1; n >= n0; n--) {
+                const auto dstf = cur_fields();
+                if ((r = copyf(A.seg[n - n0].data(), dstf.data(), 7)) != MOIST_OK) return r;
+                tape = &A.tp;
+                r = launch_step();
+                tape = nullptr;
+                if (r != MOIST_OK) return r;
+                if ((r = adj_step()) != MOIST_OK) return r;
+            }
+        }
+        CK(cudaStreamSynchronize(st));
+        const auto t2 = std::chrono::steady_clock::now();
+        // results
+        for (int f = 0; f < 7; f++) {
+            if (!out->state[f]) continue;
+            k_adj_to_ref<<<gr, b, 0, st>>>(nx, nz, halo, P, A.Lst[f], A.stage);
+            CKL();
+            CK(cudaMemcpyAsync(out->state[f], A.stage, (size_t)nz * ia * sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
+        double hp[3];
+        CK(cudaMemcpyAsync(hp, A.Lpar, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hp + 2, A.obj, sizeof(double), cudaMemcpyDeviceToHost, st));
+        // the context keeps the final State
+        {
+            const auto dstf = cur_fields();
+            if ((r = copyf(A.fin.data(), dstf.data(), 7)) != MOIST_OK) return r;
+            CK(cudaMemcpyAsync(prec, A.fin[7], P * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        }
+        CK(cudaStreamSynchronize(st));
+        if (out->prec) {
+            for (int j = 0; j < ia; j++) {
+                const int i = j - halo;
+                out->prec[j] = (prec_on && i >= 0 && i < nx) ? seed->prec_weight[j] : 0.0;
+            }
+        }
+        out->k_auto = hp[0];
+        out->qc_threshold = hp[1];
+        out->objective = hp[2];
+        out->forward_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        out->reverse_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
+        return finish();
     }
 };
 
@@ -1473,6 +1889,12 @@ int moist_budget(moist_ctx* c, double out[4]) {
     if (!c || !out) return MOIST_ERR_ARG;
     CTX_DEVICE(c);
     return c->impl->budget(out);
+}
+int moist_adjoint_run(moist_ctx* c, int nsteps, int ckpt_every, const moist_adjoint_seed* seed,
+                      moist_adjoint_grad* out) {
+    if (!c) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
+    return c->impl->adjoint_run(nsteps, ckpt_every, seed, out);
 }
 void* moist_stream(moist_ctx* c) { return c ? (void*)c->stream : nullptr; }
 int moist_synchronize(moist_ctx* c) {

@@ -89,6 +89,43 @@ class Model:
     def nan_field(self):
         return lib().moist_nan_field(self.ctx)
 
+    def adjoint(self, nsteps, ckpt_every=50, prec_weight=None, state_seed=None):
+        """Advance the resident State nsteps large steps and return the gradient of
+        J = sum(prec_weight * prec_final) + sum_f sum(state_seed[f] * S_final.f)
+        (moist_adjoint_run). prec_weight: (ia,) array or None; state_seed: dict from the
+        prognostic field names (rho, rho_u, rho_w, rho_theta, rho_qv, rho_qc, rho_qr) to (ka, ia)
+        arrays. Returns a dict: the gradients w.r.t. the initial fields as (ka, ia) float64 arrays
+        (halo columns 0), "prec", "k_auto", "qc_threshold", "objective", "forward_ms",
+        "reverse_ms". The Model is left at the final State."""
+        p = self.p
+        ka, ia = p.ka, p.ia
+        keep = []
+
+        def f64(a, shape):
+            a = np.asfortranarray(np.asarray(a, dtype=np.float64))
+            if a.shape != shape:
+                raise ValueError("seed of shape %s, expected %s" % (a.shape, shape))
+            keep.append(a)
+            return a.ctypes.data
+
+        seed = abi.moist_adjoint_seed()
+        if prec_weight is not None:
+            seed.prec_weight = f64(prec_weight, (ia,))
+        for j, name in enumerate(abi.PROGNOSTIC):
+            if state_seed is not None and name in state_seed:
+                seed.state[j] = f64(state_seed[name], (ka, ia))
+        grads = {name: np.zeros((ka, ia), dtype=np.float64, order="F") for name in abi.PROGNOSTIC}
+        grads["prec"] = np.zeros(ia, dtype=np.float64)
+        out = abi.moist_adjoint_grad()
+        for j, name in enumerate(abi.PROGNOSTIC):
+            out.state[j] = grads[name].ctypes.data
+        out.prec = grads["prec"].ctypes.data
+        _raise(lib().moist_adjoint_run(self.ctx, int(nsteps), int(ckpt_every), C.byref(seed), C.byref(out)),
+               self.ctx, "moist_adjoint_run")
+        grads.update(k_auto=out.k_auto, qc_threshold=out.qc_threshold, objective=out.objective,
+                     forward_ms=out.forward_ms, reverse_ms=out.reverse_ms)
+        return grads
+
 
 def rk3_step(s, p, nsteps=1, flags=0):
     """rk3_step!(s, p) applied nsteps times; s is updated in place."""
