@@ -16,6 +16,8 @@ e2e:    the same metric through the reference-facing call rk3_step!(s, p) on a h
         wall clock around each call.
 roofline: the kernel group with the largest device time; achieved = its algorithmic bytes per
         launch (words per cell below x cells) / its mean launch time from the same events.
+adjoint: (1 GPU, Float32) moist_adjoint_run on the 512 x 96 single-bubble domain, 600 steps,
+        rain objective, checkpoints every 50 steps: forward and reverse wall times and their ratio.
 ensemble: (1 GPU, Float32) the batched forward: 256 uneven members advanced together (one packed
         launch per kernel of the step, one CUDA graph per step), device time per step, its
         cell-steps/s, HBM fraction of the whole step's algorithmic bytes and ratio to `value`.
@@ -186,6 +188,32 @@ def measure_ensemble(nmem, steps, warmup, peak, plain_value):
                         "state with fp64 w-p elimination" % nmem}
 
 
+def measure_adjoint(nsteps, ckpt):
+    """Adjoint workload: 512 x 96 single bubble, Float32 forward, objective = total surface rain
+    after nsteps large steps, gradient w.r.t. the initial State and K_auto, Qc_threshold through
+    moist_adjoint_run with checkpoints every ckpt steps. Wall time of the forward run and of the
+    reverse sweep (recomputation included), both measured by the library around synchronised
+    device work."""
+    from moist2d_b200 import model
+    from moist2d_b200.init import single_bubble
+    p, s = single_bubble(np.float32)
+    w = np.zeros(p.ia)
+    w[p.is_ - 1:p.ie] = float(p.dx)
+    with model.Model(p) as m:
+        m.upload(s)
+        m.adjoint(2, 1, prec_weight=w)  # warm-up: allocation of the adjoint buffers
+        m.upload(s)
+        g = m.adjoint(nsteps, ckpt, prec_weight=w)
+    cells = p.Nx * p.Nz
+    return {"workload": "single bubble 512x96 (dx=250 m, dz=125 m), dt=2 s, ns=8, Float32 state, "
+                        "rain objective, gradient w.r.t. the initial State, K_auto, Qc_threshold",
+            "steps": nsteps, "ckpt_every": ckpt, "forward_ms": g["forward_ms"], "reverse_ms": g["reverse_ms"],
+            "adjoint_over_forward": g["reverse_ms"] / g["forward_ms"],
+            "forward_cell_steps_per_s": cells * nsteps / (g["forward_ms"] / 1e3),
+            "adjoint_cell_steps_per_s": cells * nsteps / (g["reverse_ms"] / 1e3),
+            "objective": g["objective"], "dJ_dK_auto": g["k_auto"], "dJ_dQc_threshold": g["qc_threshold"]}
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's CPU path (no Julia here: the threaded oracle port)."""
     if rank != 0:
@@ -235,6 +263,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end measurement")
     ap.add_argument("--ensemble", type=int, default=256,
                     help="members of the batched-ensemble measurement (0 skips it)")
+    ap.add_argument("--adjoint-steps", type=int, default=600,
+                    help="large steps of the adjoint measurement (0 skips it)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -364,6 +394,12 @@ def main():
             ens = measure_ensemble(args.ensemble, max(3, min(args.steps, 10)), args.warmup, peak, value)
         except Exception as e:  # the ensemble must not hide the single-domain number
             ens = {"value": None, "error": str(e)}
+    adj = None
+    if rank == 0 and world == 1 and args.adjoint_steps > 0 and args.precision == "f32":
+        try:
+            adj = measure_adjoint(args.adjoint_steps, 50)
+        except Exception as e:
+            adj = {"error": str(e)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -390,6 +426,7 @@ def main():
             "kernel_ms_per_step": {g: float(group_ms[j] / args.steps) for j, g in enumerate(gnames)},
             "clocks": clk,
             "ensemble": ens,
+            "adjoint": adj,
         }
         print(json.dumps(line), flush=True)
 

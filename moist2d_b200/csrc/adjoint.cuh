@@ -347,7 +347,8 @@ struct AdjStage {
     double* Lpend[2];            // pending lambda of rho_theta_p_old
     double* Lqout[3];
     double *Ta, *Tb, *Tc;        // w-p coefficients (double)
-    double *Lx, *Ly, *Ctmp;      // Thomas scratch
+    double *Tcp, *Trd;           // elimination of the transposed system: modified super-diagonal, 1 / pivot
+    double *Lx, *Ly;             // right-hand side and solution of the transposed solve
     double *Ltp_rho, *Ltp_rt, *Linc_rho, *Linc_rt;
 };
 
@@ -373,31 +374,40 @@ __device__ __forceinline__ void aadd(double* a, double v) { atomicAdd(a, v); }
 
 // ----------------------------------------------------------------------------- stage prologue
 
-// w-p coefficients a, b, c of implicit_correction! (moist.jl:982-1008) in double, per column
+// w-p coefficients a, b, c of implicit_correction! (moist.jl:982-1008) in double, per cell
 template <class T>
 __global__ void k_adj_tri_coef(DevParams<double> p, AdjStage<T> a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nx = p.nx, nz = p.nz, P = p.P;
-    if (i >= nx) return;
+    ADJ_CELL(k, i);
+    const int ke = nz - 1, n = nz - 1;
+    if (k >= n) return;
     const double* dz = p.dz;
     const double* z = p.z;
-    const int ke = nz - 1, n = nz - 1;
     const double fact_tp = 0.5 * (1.0 + p.beta);
-    const double dt_tp2 = (a.dt_s * fact_tp) * (a.dt_s * fact_tp);
-    auto thh = [&](int k) {
-        return f2h((double)a.theta[MOIST_IDX(k, i)], (double)a.theta[MOIST_IDX(k + 1, i)], dz[k], dz[k + 1]);
-    };
-    double th_prev = 0.0, th_cur = thh(0);
-    for (int k = 0; k < n; k++) {
-        const double th_next = (k + 1 <= ke - 1) ? thh(k + 1) : 0.0;
-        const double r_k = a.rt2[MOIST_IDX(k, i)], r_kp = a.rt2[MOIST_IDX(k + 1, i)];
-        const double dzc = z[k + 1] - z[k];
-        a.Tb[MOIST_IDX(k, i)] = dt_tp2 * (r_k / dz[k] + r_kp / dz[k + 1]) * th_cur / dzc;
-        a.Ta[MOIST_IDX(k, i)] = k > 0 ? -dt_tp2 * (r_k * th_prev / (dzc * dz[k]) - p.GRAV / (dz[k] + dz[k + 1])) : 0.0;
-        a.Tc[MOIST_IDX(k, i)] =
-            k < ke - 1 ? -dt_tp2 * (r_kp * th_next / (dzc * dz[k + 1]) + p.GRAV / (dz[k] + dz[k + 1])) : 0.0;
-        th_prev = th_cur;
-        th_cur = th_next;
+    const double C = (a.dt_s * fact_tp) * (a.dt_s * fact_tp);
+    auto TH = [&](int kk) { return (double)a.theta[MOIST_IDX(kk, i)]; };
+    auto thh = [&](int kk) { return f2h(TH(kk), TH(kk + 1), dz[kk], dz[kk + 1]); };
+    const double r_k = a.rt2[c], r_kp = a.rt2[c + P];
+    const double dzc = z[k + 1] - z[k];
+    a.Tb[c] = C * (r_k / dz[k] + r_kp / dz[k + 1]) * thh(k) / dzc;
+    a.Ta[c] = k > 0 ? -C * (r_k * thh(k - 1) / (dzc * dz[k]) - p.GRAV / (dz[k] + dz[k + 1])) : 0.0;
+    a.Tc[c] = k < ke - 1 ? -C * (r_kp * thh(k + 1) / (dzc * dz[k + 1]) + p.GRAV / (dz[k] + dz[k + 1])) : 0.0;
+}
+
+// elimination of the transposed system A^T (sub-diagonal c_{j-1}, diagonal b_j + 1,
+// super-diagonal a_{j+1}), once per stage and column: modified super-diagonal and 1 / pivot
+__global__ void k_adj_tri_fact(int nx, int nz, int P, const double* __restrict__ Ta, const double* __restrict__ Tb,
+                               const double* __restrict__ Tc, double* __restrict__ Tcp, double* __restrict__ Trd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nx) return;
+    const int n = nz - 1;
+    double cp = 0.0;
+    for (int j = 0; j < n; j++) {
+        const size_t cj = MOIST_IDX(j, i);
+        const double sub = j > 0 ? Tc[cj - P] : 0.0;
+        const double rd = 1.0 / (Tb[cj] + 1.0 - sub * cp);
+        cp = (j < n - 1 ? Ta[cj + P] : 0.0) * rd;
+        Tcp[cj] = cp;
+        Trd[cj] = rd;
     }
 }
 
@@ -478,7 +488,7 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_tr_jac(DevParams<double> p,
 // of (k, i): (k, i+1) [slot L1], (k, i+2) [L2], (k+1, i) [B1], (k+2, i) [B2]. One block per
 // tracer, thread k owns row k; row k handles column nx-1-(d-(nz-1-k)) at step d, after the rows
 // above it, whose results come through a 3-step ring in shared memory.
-__global__ void k_adj_tr_rev(int nx, int nz, int P, const double* J, DP<3> lam_new, DP<3> mu) {
+__global__ void k_adj_tr_rev(int nx, int nz, int P, const double* __restrict__ J, DP<3> lam_new, DP<3> mu) {
     extern __shared__ double ring[];  // [3][nz]
     const int t = blockIdx.x;
     const int k = threadIdx.x;
@@ -492,17 +502,39 @@ __global__ void k_adj_tr_rev(int nx, int nz, int P, const double* J, DP<3> lam_n
     double* m = mu.f[t];
     const bool active = k < nz;
     double mp1 = 0.0, mp2 = 0.0;  // mu(k, i+1), mu(k, i+2)
+    // the next step's inputs, loaded one step ahead (they do not depend on mu)
+    double f_ln = 0.0, f_a1 = 0.0, f_a2 = 0.0, f_b1 = 0.0, f_b2 = 0.0;
+    auto fetch = [&](int i) {
+        const size_t cc = MOIST_IDX(k, i);
+        f_ln = ln[cc];
+        f_a1 = i + 1 < nx ? JL1[cc + 1] : 0.0;
+        f_a2 = i + 2 < nx ? JL2[cc + 2] : 0.0;
+        f_b1 = k + 1 < nz ? JB1[cc + P] : 0.0;
+        f_b2 = k + 2 < nz ? JB2[cc + 2 * P] : 0.0;
+        // a row walks its arrays backwards, one 128-byte line per 16 steps: ask for the line
+        // 16 steps ahead into L1 so that the loads above hit
+        if (i >= 16) {
+            const size_t cf = cc - 16;
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(ln + cf));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(JL1 + cf + 1));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(JL2 + cf + 2));
+            if (k + 1 < nz) asm volatile("prefetch.global.L1 [%0];" ::"l"(JB1 + cf + P));
+            if (k + 2 < nz) asm volatile("prefetch.global.L1 [%0];" ::"l"(JB2 + cf + 2 * P));
+        }
+    };
+    if (active) fetch(nx - 1);
     const int nsteps = nx + nz - 1;
     for (int d = 0; d < nsteps; d++) {
         const int i = nx - 1 - (d - (nz - 1 - k));
         if (active && i >= 0 && i < nx) {
-            const size_t cc = MOIST_IDX(k, i);
-            double v = ln[cc];
-            if (i + 1 < nx) v += mp1 * JL1[cc + 1];
-            if (i + 2 < nx) v += mp2 * JL2[cc + 2];
-            if (k + 1 < nz) v += ring[((d + 2) % 3) * nz + k + 1] * JB1[cc + P];
-            if (k + 2 < nz) v += ring[((d + 1) % 3) * nz + k + 2] * JB2[cc + 2 * P];
-            m[cc] = v;
+            const double l = f_ln, a1 = f_a1, a2 = f_a2, b1 = f_b1, b2 = f_b2;
+            if (i >= 1) fetch(i - 1);
+            double v = l;
+            if (i + 1 < nx) v += mp1 * a1;
+            if (i + 2 < nx) v += mp2 * a2;
+            if (k + 1 < nz) v += ring[((d + 2) % 3) * nz + k + 1] * b1;
+            if (k + 2 < nz) v += ring[((d + 1) % 3) * nz + k + 2] * b2;
+            m[MOIST_IDX(k, i)] = v;
             ring[(d % 3) * nz + k] = v;
             mp2 = mp1;
             mp1 = v;
@@ -619,86 +651,120 @@ __global__ void k_adj_sub_vert(DevParams<double> p, AdjStage<T> a, AdjSub<T> b) 
     a.Lx[c] = lx;
 }
 
-// (2) per column: the transposed Thomas solve y = A^-T lambda_x (A = tri(a, b + 1, c)), the
-// coefficients' lambda -y x^T, the right-hand side d = rho_w_p + drho_w - fact (a, b, c) rho_w_p
-// (moist.jl:1009-1018) and drho_w = dt_s (R_rho_w - rt2pres_h buoyancy + grav) (1397-1408)
+// (2a) y = A^-T lambda_x with the stage's elimination (A = tri(a, b + 1, c), the w-p system of
+// moist.jl:1009-1018). A block of ADJ_SOLVE_THREADS threads owns `wc` adjacent columns: all of
+// them stage the columns' right-hand sides and elimination factors in shared memory with
+// coalesced row loads, one thread per column runs the two recurrences from shared memory, and
+// all write the solution back by rows.
+constexpr int ADJ_SOLVE_THREADS = 256;
+__host__ __device__ inline int adj_solve_cols(int nz) {  // widest of 32, 16, 8, 4 within 200 KB
+    int w = 32;
+    while (w > 4 && (size_t)32 * nz * w > 200 * 1024) w /= 2;
+    return w;
+}
+__host__ __device__ inline size_t adj_solve_smem(int nz) { return (size_t)4 * nz * adj_solve_cols(nz) * sizeof(double); }
+
+__global__ void __launch_bounds__(ADJ_SOLVE_THREADS) k_adj_sub_solve(int nx, int nz, int P, const double* __restrict__ Tc,
+                                                                     const double* __restrict__ Tcp,
+                                                                     const double* __restrict__ Trd,
+                                                                     const double* __restrict__ Lx,
+                                                                     double* __restrict__ Ly) {
+    extern __shared__ double sm[];
+    const int wc = adj_solve_cols(nz);
+    const int i0 = blockIdx.x * wc;
+    const int n = nz - 1;
+    double* sg = sm;                 // [n][wc] right-hand side, then g', then y
+    double* ssub = sm + nz * wc;     // c_{j-1}
+    double* srd = sm + 2 * nz * wc;  // 1 / pivot
+    double* scp = sm + 3 * nz * wc;  // modified super-diagonal
+    for (int e = threadIdx.x; e < n * wc; e += blockDim.x) {
+        const int j = e / wc, cc = e - j * wc, i = i0 + cc;
+        if (i >= nx) continue;
+        const size_t cj = MOIST_IDX(j, i);
+        sg[e] = Lx[cj];
+        ssub[e] = j > 0 ? Tc[cj - P] : 0.0;
+        srd[e] = Trd[cj];
+        scp[e] = Tcp[cj];
+    }
+    __syncthreads();
+    const int cc = threadIdx.x;
+    if (cc < wc && i0 + cc < nx) {
+        double g = 0.0;
+        for (int j = 0; j < n; j++) {
+            const int e = j * wc + cc;
+            g = (sg[e] - ssub[e] * g) * srd[e];
+            sg[e] = g;
+        }
+        double y = g;
+        for (int j = n - 2; j >= 0; j--) {
+            const int e = j * wc + cc;
+            y = sg[e] - scp[e] * y;
+            sg[e] = y;
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * wc; e += blockDim.x) {
+        const int j = e / wc, c2 = e - j * wc, i = i0 + c2;
+        if (i < nx) Ly[MOIST_IDX(j, i)] = sg[e];
+    }
+}
+
+// (2b) per cell k, from y of faces k and k-1: the coefficients' lambda -y x^T, the right-hand
+// side d = rho_w_p + drho_w - fact (a, b, c) rho_w_p (moist.jl:1009-1018) and
+// drho_w = dt_s (R_rho_w - rt2pres_h buoyancy + grav) (1397-1408)
 template <class T>
-__global__ void k_adj_sub_thomas(DevParams<double> p, DevParams<T> pt, AdjStage<T> a, AdjSub<T> b) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nx = p.nx, nz = p.nz, P = p.P;
-    if (i >= nx) return;
+__global__ void k_adj_sub_rhs(DevParams<double> p, DevParams<T> pt, AdjStage<T> a, AdjSub<T> b) {
+    ADJ_CELL(k, i);
     const int n = nz - 1;
     const double* z = p.z;
-    const double dts = a.dt_s, fact = a.fact;
-    // forward elimination on A^T: sub-diagonal c_{j-1}, diagonal b_j + 1, super-diagonal a_{j+1}
-    double cp_prev = 0.0, gp_prev = 0.0;
-    for (int j = 0; j < n; j++) {
-        const size_t cj = MOIST_IDX(j, i);
-        const double B = a.Tb[cj] + 1.0;
-        const double sub = j > 0 ? a.Tc[cj - P] : 0.0;
-        const double den = B - sub * cp_prev;
-        const double sup = j < n - 1 ? a.Ta[cj + P] : 0.0;
-        const double cpj = sup / den;
-        const double gpj = (a.Lx[cj] - sub * gp_prev) / den;
-        a.Ctmp[cj] = cpj;
-        a.Ly[cj] = gpj;
-        cp_prev = cpj;
-        gp_prev = gpj;
-    }
-    double y_next = gp_prev;
-    for (int j = n - 2; j >= 0; j--) {
-        const size_t cj = MOIST_IDX(j, i);
-        const double y = a.Ly[cj] - a.Ctmp[cj] * y_next;
-        a.Ly[cj] = y;
-        y_next = y;
-    }
-    // rho_theta_p at the off-centred time level, recomputed as the forward substep forms it
+    const double dts = a.dt_s, fact = a.fact, g2 = -p.GRAV * 0.5;
     const int im = wrapx(i - 1, nx), ip = wrapx(i + 1, nx);
-    auto rt_tp = [&](int k) -> double {
-        const size_t cc = MOIST_IDX(k, i);
-        const T th_i = a.theta[cc], th_ip = a.theta[MOIST_IDX(k, ip)], th_im = a.theta[MOIST_IDX(k, im)];
-        const T u_p = b.ru[cc], u_m = b.ru[MOIST_IDX(k, im)];
+    // rho_theta_p at the off-centred time level, recomputed as the forward substep forms it
+    auto rt_tp = [&](int kk) -> double {
+        const size_t cc = MOIST_IDX(kk, i);
+        const T th_i = a.theta[cc], th_ip = a.theta[MOIST_IDX(kk, ip)], th_im = a.theta[MOIST_IDX(kk, im)];
+        const T u_p = b.ru[cc], u_m = b.ru[MOIST_IDX(kk, im)];
         const T flux_ip = (th_ip + th_i) * T(0.5) * u_p;
         const T flux_im = (th_i + th_im) * T(0.5) * u_m;
         const T advection = -(flux_ip - flux_im) / pt.dx;
         const T inc = (T)a.dt_s * (a.rrt[cc] + advection);
         return (double)(T)((double)b.prev_rt[cc] + a.fact_tp64 * (double)inc);
     };
-    for (int k = 0; k < nz; k++) {
-        a.Ltp_rho[MOIST_IDX(k, i)] = 0.0;
-        a.Ltp_rt[MOIST_IDX(k, i)] = 0.0;
+    double lrt2 = 0.0, ltp_rt = 0.0, ltp_rho = 0.0, lpw = 0.0;
+    const double tp_k = rt_tp(k);
+    if (k < n) {  // face k
+        const double y = a.Ly[c];
+        const double xk = b.rw[c];
+        const double xkm = k > 0 ? (double)b.rw[c - P] : 0.0;
+        const double xkp = k < n - 1 ? (double)b.rw[c + P] : 0.0;
+        const double wk = b.prev_rw[c];
+        const double wkp = k < n - 1 ? (double)b.prev_rw[c + P] : 0.0;
+        if (k > 0) a.La[c] += -y * xkm - fact * wk * y;
+        a.Lb[c] += -y * xk - fact * wk * y;
+        if (k < n - 1) a.Lc[c] += -y * xkp - fact * wkp * y;
+        lpw = y * (1.0 - fact * ((k > 0 ? a.Ta[c] : 0.0) + a.Tb[c]));
+        a.LRw[c] += dts * y;
+        const double dzc = z[k + 1] - z[k];
+        const double buoy = (rt_tp(k + 1) - tp_k) / dzc;
+        const double rt2h = ((double)a.rt2[c] + (double)a.rt2[c + P]) * 0.5;
+        lrt2 += -dts * buoy * 0.5 * y;
+        ltp_rt += dts * rt2h * y / dzc;
+        ltp_rho += dts * g2 * y;
     }
-    double y_prev = 0.0;
-    double tp_j = rt_tp(0);
-    for (int j = 0; j < n; j++) {
-        const size_t cj = MOIST_IDX(j, i);
-        const double y = a.Ly[cj];
-        const double xj = b.rw[cj];
-        const double xjm = j > 0 ? (double)b.rw[cj - P] : 0.0;
-        const double xjp = j < n - 1 ? (double)b.rw[cj + P] : 0.0;
-        const double wj = b.prev_rw[cj];
-        const double wjp = j < n - 1 ? (double)b.prev_rw[cj + P] : 0.0;
-        if (j > 0) a.La[cj] += -y * xjm - fact * wj * y;
-        a.Lb[cj] += -y * xj - fact * wj * y;
-        if (j < n - 1) a.Lc[cj] += -y * xjp - fact * wjp * y;
-        double lw = y * (1.0 - fact * ((j > 0 ? a.Ta[cj] : 0.0) + a.Tb[cj]));
-        if (j > 0) lw += -fact * a.Tc[cj - P] * y_prev;
-        b.LPo[2][cj] = lw;
-        a.LRw[cj] += dts * y;
-        const double tp_jp = rt_tp(j + 1);
-        const double dzc = z[j + 1] - z[j];
-        const double buoy = (tp_jp - tp_j) / dzc;
-        const double rt2h = ((double)a.rt2[cj] + (double)a.rt2[cj + P]) * 0.5;
-        a.Lrt2[cj] += -dts * buoy * 0.5 * y;
-        a.Lrt2[cj + P] += -dts * buoy * 0.5 * y;
-        a.Ltp_rt[cj + P] += -dts * rt2h * y / dzc;
-        a.Ltp_rt[cj] += dts * rt2h * y / dzc;
-        a.Ltp_rho[cj] += dts * (-p.GRAV * 0.5) * y;
-        a.Ltp_rho[cj + P] += dts * (-p.GRAV * 0.5) * y;
-        y_prev = y;
-        tp_j = tp_jp;
+    if (k >= 1) {  // face k-1
+        const double y = a.Ly[c - P];
+        const double dzc = z[k] - z[k - 1];
+        const double buoy = (tp_k - rt_tp(k - 1)) / dzc;
+        const double rt2h = ((double)a.rt2[c - P] + (double)a.rt2[c]) * 0.5;
+        lrt2 += -dts * buoy * 0.5 * y;
+        ltp_rt += -dts * rt2h * y / dzc;
+        ltp_rho += dts * g2 * y;
+        if (k < n) lpw += -fact * a.Tc[c - P] * y;
     }
-    b.LPo[2][MOIST_IDX(n, i)] = 0.0;
+    a.Lrt2[c] += lrt2;
+    a.Ltp_rt[c] = ltp_rt;
+    a.Ltp_rho[c] = ltp_rho;
+    b.LPo[2][c] = lpw;
 }
 
 // (3) explicit rho_p / rho_theta_p updates and their off-centred values (moist.jl:1367-1396)
@@ -763,46 +829,42 @@ __global__ void k_adj_p0(DevParams<double> p, AdjStage<T> a, DP<4> LP) {
 
 // ----------------------------------------------------------------------------- stage tendencies
 
-// lambda of the w-p coefficients -> theta, rt2pres (per column)
+// lambda of the w-p coefficients -> theta, rt2pres, per cell: theta_h(j) enters b_j, a_{j+1},
+// c_{j-1}; rt2pres(k) enters b_k, a_k, b_{k-1}, c_{k-1}
 template <class T>
 __global__ void k_adj_tri_coef_T(DevParams<double> p, AdjStage<T> a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nx = p.nx, nz = p.nz, P = p.P;
-    if (i >= nx) return;
+    ADJ_CELL(k, i);
+    const int n = nz - 1;
     const double* dz = p.dz;
     const double* z = p.z;
-    const int n = nz - 1;
     const double fact_tp = 0.5 * (1.0 + p.beta);
     const double C = (a.dt_s * fact_tp) * (a.dt_s * fact_tp);
-    auto thh = [&](int k) {
-        return f2h((double)a.theta[MOIST_IDX(k, i)], (double)a.theta[MOIST_IDX(k + 1, i)], dz[k], dz[k + 1]);
+    auto TH = [&](int kk) { return (double)a.theta[MOIST_IDX(kk, i)]; };
+    auto R = [&](int kk) { return (double)a.rt2[MOIST_IDX(kk, i)]; };
+    auto thh = [&](int kk) { return f2h(TH(kk), TH(kk + 1), dz[kk], dz[kk + 1]); };
+    auto dzc = [&](int kk) { return z[kk + 1] - z[kk]; };
+    auto LA = [&](int j) { return a.La[MOIST_IDX(j, i)]; };
+    auto LB = [&](int j) { return a.Lb[MOIST_IDX(j, i)]; };
+    auto LC = [&](int j) { return a.Lc[MOIST_IDX(j, i)]; };
+    auto lthh = [&](int j) {
+        double l = LB(j) * C * (R(j) / dz[j] + R(j + 1) / dz[j + 1]) / dzc(j);
+        if (j + 1 < n) l += LA(j + 1) * (-C * R(j + 1) / (dzc(j + 1) * dz[j + 1]));
+        if (j >= 1) l += LC(j - 1) * (-C * R(j) / (dzc(j - 1) * dz[j]));
+        return l;
     };
-    double* lth_h = a.Ly;  // lambda of theta_h, [n] per column
-    for (int k = 0; k < n; k++) lth_h[MOIST_IDX(k, i)] = 0.0;
-    for (int k = 0; k < n; k++) {
-        const size_t ck = MOIST_IDX(k, i);
-        const double la = a.La[ck], lb = a.Lb[ck], lc = a.Lc[ck];
-        const double dzc = z[k + 1] - z[k];
-        const double r_k = a.rt2[ck], r_kp = a.rt2[ck + P];
-        const double th_k = thh(k);
-        a.Lrt2[ck] += lb * C * th_k / (dzc * dz[k]);
-        a.Lrt2[ck + P] += lb * C * th_k / (dzc * dz[k + 1]);
-        lth_h[ck] += lb * C * (r_k / dz[k] + r_kp / dz[k + 1]) / dzc;
-        if (k > 0) {
-            a.Lrt2[ck] += la * (-C * thh(k - 1) / (dzc * dz[k]));
-            lth_h[ck - P] += la * (-C * r_k / (dzc * dz[k]));
-        }
-        if (k < n - 1) {
-            a.Lrt2[ck + P] += lc * (-C * thh(k + 1) / (dzc * dz[k + 1]));
-            lth_h[ck + P] += lc * (-C * r_kp / (dzc * dz[k + 1]));
-        }
+    double lth = 0.0, lr = 0.0;
+    if (k < n) {
+        lth += lthh(k) * dz[k + 1] / (dz[k] + dz[k + 1]);
+        lr += LB(k) * C * thh(k) / (dzc(k) * dz[k]);
+        if (k > 0) lr += LA(k) * (-C * thh(k - 1) / (dzc(k) * dz[k]));
     }
-    for (int k = 0; k < n; k++) {
-        const size_t ck = MOIST_IDX(k, i);
-        const double l = lth_h[ck], s = dz[k] + dz[k + 1];
-        a.Ltheta[ck] += l * dz[k + 1] / s;
-        a.Ltheta[ck + P] += l * dz[k] / s;
+    if (k >= 1) {
+        lth += lthh(k - 1) * dz[k - 1] / (dz[k - 1] + dz[k]);
+        lr += LB(k - 1) * C * thh(k - 1) / (dzc(k - 1) * dz[k]);
+        if (k < n) lr += LC(k - 1) * (-C * thh(k) / (dzc(k - 1) * dz[k]));
     }
+    a.Ltheta[c] += lth;
+    a.Lrt2[c] += lr;
 }
 
 // lambda of R_rho, R_rho_u, R_rho_w, R_rho_theta -> their inputs

@@ -72,9 +72,10 @@ template <int N>
 MM_HD Dual<N> operator/(const Dual<N>& a, const Dual<N>& b) {
     Dual<N> r;
     const double q = a.v / b.v;
+    const double rb = 1.0 / b.v;
     r.v = q;
 #pragma unroll
-    for (int j = 0; j < N; j++) r.d[j] = (a.d[j] - q * b.d[j]) / b.v;
+    for (int j = 0; j < N; j++) r.d[j] = (a.d[j] - q * b.d[j]) * rb;
     return r;
 }
 template <int N>

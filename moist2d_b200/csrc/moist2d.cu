@@ -238,6 +238,7 @@ struct Ctx : CtxBase {
         T* rrt[3];                             // R_rho_theta
         T* mf[3][2];                           // momentum fluxes after the substeps
         T* qout[3][3];                         // tracer sweep results
+        T* sed;                                // d_rho_qr_sed of the step's physics
     };
     Tape* tape = nullptr;
     int tape_stage = 0;
@@ -248,11 +249,11 @@ struct Ctx : CtxBase {
         double *Lst[7], *LS0[7], *Lph[5], *seed[7];
         double* acc;  // 16 per-stage accumulators, contiguous (one memset)
         double *Lqout[3], *mu[3], *J, *LP[2][4];
-        double *Ta, *Tb, *Tc, *Lx, *Ly, *Ctmp, *Ltp_rho, *Ltp_rt, *Linc_rho, *Linc_rt, *Lsed;
+        double *Ta, *Tb, *Tc, *Tcp, *Trd, *Lx, *Ly, *Ltp_rho, *Ltp_rt, *Linc_rho, *Linc_rt, *Lsed;
         double *Lpar, *obj, *prec_w, *stage;
-        Tape tp;
+        std::vector<Tape> tapes;             // one per step of a segment, or one
         std::vector<std::array<T*, 7>> ck;   // States every ckpt_every steps
-        std::vector<std::array<T*, 7>> seg;  // the States of one segment
+        std::vector<std::array<T*, 7>> seg;  // the States of one segment (when one tape is kept)
         std::array<T*, 8> fin;               // the final State and prec
     };
     Adj* adj = nullptr;
@@ -750,6 +751,10 @@ struct Ctx : CtxBase {
     int launch_step() {
         int r;
         if ((r = launch_physics(4)) != MOIST_OK) return r;
+        if (tape) {
+            const T* src[1] = {d_qr_sed};
+            if ((r = copyf(src, &tape->sed, 1)) != MOIST_OK) return r;
+        }
         const T dt = dp.dt;
         const int ns1 = std::max(1, (int)std::ceil(ns / 3.0));
         const int ns2 = std::max(1, (int)std::ceil(ns / 2.0));
@@ -934,6 +939,8 @@ struct Ctx : CtxBase {
                 CK(cudaMemcpyAsync(*g[j], hd.data(), nz * sizeof(double), cudaMemcpyHostToDevice, st));
                 CK(cudaStreamSynchronize(st));
             }
+            CK(cudaFuncSetAttribute(k_adj_sub_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)adj_solve_smem(nz)));
             A.pd = params_to_double(dp);
             A.pd.dz = A.dz;
             A.pd.z = A.z;
@@ -952,35 +959,35 @@ struct Ctx : CtxBase {
             AL(A.J, 3 * TR_SLOTS * fsz);
             for (int q = 0; q < 2; q++)
                 for (int f = 0; f < 4; f++) AL(A.LP[q][f], fsz);
-            for (double** f : {&A.Ta, &A.Tb, &A.Tc, &A.Lx, &A.Ly, &A.Ctmp, &A.Ltp_rho, &A.Ltp_rt, &A.Linc_rho,
-                               &A.Linc_rt, &A.Lsed})
+            for (double** f : {&A.Ta, &A.Tb, &A.Tc, &A.Tcp, &A.Trd, &A.Lx, &A.Ly, &A.Ltp_rho, &A.Ltp_rt,
+                               &A.Linc_rho, &A.Linc_rt, &A.Lsed})
                 AL(*f, fsz);
             AL(A.Lpar, 2);
             AL(A.obj, 1);
             AL(A.prec_w, (size_t)P);
             AL(A.stage, (size_t)nz * (nx + 2 * halo));
-            Tape& tp = A.tp;
-            for (int j = 0; j < 3; j++) {
-                for (int f = 0; f < 7; f++) AL(tp.in[j][f], fsz);
-                tp.sub[j].resize(stage_substeps(j) + 1);
-                for (auto& a : tp.sub[j])
-                    for (int f = 0; f < 4; f++) AL(a[f], fsz);
-                AL(tp.rrt[j], fsz);
-                AL(tp.mf[j][0], fsz);
-                AL(tp.mf[j][1], fsz);
-                for (int t = 0; t < 3; t++) AL(tp.qout[j][t], fsz);
-            }
             for (int f = 0; f < 7; f++) AL(A.fin[f], fsz);
             AL(A.fin[7], (size_t)P);
         }
         Adj& A = *adj;
+        // a tape per step of a segment when that fits in half the free device memory (the
+        // segment is then recomputed once), else one tape and the segment's States
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        const size_t need = (size_t)std::max<long>(0, (long)ckpt - (long)A.tapes.size()) * tape_fields() * fsz * sizeof(T);
+        seg_tapes = A.tapes.size() >= (size_t)ckpt || need <= free_b / 2;
+        const size_t ntapes = seg_tapes ? (size_t)ckpt : 1;
+        while (A.tapes.size() < ntapes) {
+            A.tapes.emplace_back();
+            if (int r = alloc_tape(A.tapes.back())) return r;
+        }
         const size_t nck = (size_t)((nsteps + ckpt - 1) / ckpt);
         while (A.ck.size() < nck) {
             std::array<T*, 7> a;
             for (int f = 0; f < 7; f++) AL(a[f], fsz);
             A.ck.push_back(a);
         }
-        while (A.seg.size() < (size_t)ckpt) {
+        while (!seg_tapes && A.seg.size() < (size_t)ckpt) {
             std::array<T*, 7> a;
             for (int f = 0; f < 7; f++) AL(a[f], fsz);
             A.seg.push_back(a);
@@ -988,15 +995,37 @@ struct Ctx : CtxBase {
         return MOIST_OK;
     }
 
+    bool seg_tapes = false;
+
+    size_t tape_fields() const {
+        size_t n = 21 + 3 + 6 + 9 + 1;
+        for (int j = 0; j < 3; j++) n += 4 * (size_t)(stage_substeps(j) + 1);
+        return n;
+    }
+
+    int alloc_tape(Tape& tp) {
+        for (int j = 0; j < 3; j++) {
+            for (int f = 0; f < 7; f++) AL(tp.in[j][f], fsz);
+            tp.sub[j].resize(stage_substeps(j) + 1);
+            for (auto& a : tp.sub[j])
+                for (int f = 0; f < 4; f++) AL(a[f], fsz);
+            AL(tp.rrt[j], fsz);
+            AL(tp.mf[j][0], fsz);
+            AL(tp.mf[j][1], fsz);
+            for (int t = 0; t < 3; t++) AL(tp.qout[j][t], fsz);
+        }
+        AL(tp.sed, fsz);
+        return MOIST_OK;
+    }
+
     std::array<T*, 7> cur_fields() const { return {cur.rho, cur.ru, cur.rw, cur.rt, cur.qv, cur.qc, cur.qr}; }
 
     // the adjoint of one large step: lambda of the step's output State in A.Lst becomes the
     // lambda of its input State; the tape holds the step's internals
-    int adj_step() {
+    int adj_step(const Tape& tp) {
         Adj& A = *adj;
-        Tape& tp = A.tp;
         const dim3 b(ADJ_THREADS), gc(cdiv(nx, ADJ_THREADS), nz), gc3(cdiv(nx, ADJ_THREADS), nz, 3);
-        const unsigned gcol = cdiv(nx, 128);
+        const unsigned gcol = cdiv(nx, 32);
         const dim3 b2(32, 8), g2(cdiv(nx, 32), cdiv(nz, 8));
         const T dtT = dp.dt;
         const T dst[3] = {dtT / T(3), dtT / T(2), dtT};
@@ -1052,15 +1081,17 @@ struct Ctx : CtxBase {
             a.Ta = A.Ta;
             a.Tb = A.Tb;
             a.Tc = A.Tc;
+            a.Tcp = A.Tcp;
+            a.Trd = A.Trd;
             a.Lx = A.Lx;
             a.Ly = A.Ly;
-            a.Ctmp = A.Ctmp;
             a.Ltp_rho = A.Ltp_rho;
             a.Ltp_rt = A.Ltp_rt;
             a.Linc_rho = A.Linc_rho;
             a.Linc_rt = A.Linc_rt;
             CK(cudaMemsetAsync(A.acc, 0, 16 * fsz * sizeof(double), st));
-            k_adj_tri_coef<T><<<gcol, 128, 0, st>>>(A.pd, a);
+            k_adj_tri_coef<T><<<gc, b, 0, st>>>(A.pd, a);
+            k_adj_tri_fact<<<gcol, 32, 0, st>>>(nx, nz, P, A.Ta, A.Tb, A.Tc, A.Tcp, A.Trd);
             DP<4> LPc{{A.LP[lp][0], A.LP[lp][1], A.LP[lp][2], A.LP[lp][3]}};
             k_adj_update<T><<<gc, b, 0, st>>>(A.pd, a, LPc);
             k_adj_tr_jac<T><<<gc3, b, 0, st>>>(A.pd, a, A.J);
@@ -1081,14 +1112,16 @@ struct Ctx : CtxBase {
                 }
                 sb.n = n;
                 k_adj_sub_vert<T><<<gc, b, 0, st>>>(A.pd, a, sb);
-                k_adj_sub_thomas<T><<<gcol, 128, 0, st>>>(A.pd, dp, a, sb);
+                k_adj_sub_solve<<<cdiv(nx, adj_solve_cols(nz)), ADJ_SOLVE_THREADS, adj_solve_smem(nz), st>>>(
+                    nx, nz, P, A.Tc, A.Tcp, A.Trd, A.Lx, A.Ly);
+                k_adj_sub_rhs<T><<<gc, b, 0, st>>>(A.pd, dp, a, sb);
                 k_adj_sub_expl<T><<<gc, b, 0, st>>>(A.pd, a, sb);
                 k_adj_sub_horiz<T><<<gc, b, 0, st>>>(A.pd, a, sb);
                 lp = 1 - lp;
             }
             DP<4> LP0{{A.LP[lp][0], A.LP[lp][1], A.LP[lp][2], A.LP[lp][3]}};
             k_adj_p0<T><<<gc, b, 0, st>>>(A.pd, a, LP0);
-            k_adj_tri_coef_T<T><<<gcol, 128, 0, st>>>(A.pd, a);
+            k_adj_tri_coef_T<T><<<gc, b, 0, st>>>(A.pd, a);
             k_adj_tend_T<T><<<gc, b, 0, st>>>(A.pd, a);
             k_adj_face_T<T><<<gc, b, 0, st>>>(A.pd, a);
             k_adj_diag_T<T><<<gc, b, 0, st>>>(A.pd, a);
@@ -1096,7 +1129,7 @@ struct Ctx : CtxBase {
         }
         AdjPhys<T> ph;
         ph.s = StateP<T>{tp.in[0][0], tp.in[0][1], tp.in[0][2], tp.in[0][3], tp.in[0][4], tp.in[0][5], tp.in[0][6]};
-        ph.sed = d_qr_sed;
+        ph.sed = tp.sed;
         for (int f = 0; f < 7; f++) ph.Lst[f] = A.Lst[f];
         for (int f = 0; f < 5; f++) ph.Lph[f] = A.Lph[f];
         ph.Lsed = A.Lsed;
@@ -1180,6 +1213,19 @@ struct Ctx : CtxBase {
         const int nck = (nsteps + ckpt - 1) / ckpt;
         for (int sg = nck - 1; sg >= 0; sg--) {
             const int n0 = sg * ckpt, n1 = std::min(n0 + ckpt, nsteps);
+            if (seg_tapes) {  // recompute the segment once, taping every step
+                const auto dstf = cur_fields();
+                if ((r = copyf(A.ck[sg].data(), dstf.data(), 7)) != MOIST_OK) return r;
+                for (int n = n0; n < n1; n++) {
+                    tape = &A.tapes[n - n0];
+                    r = launch_step();
+                    tape = nullptr;
+                    if (r != MOIST_OK) return r;
+                }
+                for (int n = n1 - 1; n >= n0; n--)
+                    if ((r = adj_step(A.tapes[n - n0])) != MOIST_OK) return r;
+                continue;
+            }
             {
                 const auto dstf = cur_fields();
                 if ((r = copyf(A.ck[sg].data(), dstf.data(), 7)) != MOIST_OK) return r;
@@ -1193,11 +1239,11 @@ struct Ctx : CtxBase {
             for (int n = n1 - 1; n >= n0; n--) {
                 const auto dstf = cur_fields();
                 if ((r = copyf(A.seg[n - n0].data(), dstf.data(), 7)) != MOIST_OK) return r;
-                tape = &A.tp;
+                tape = &A.tapes[0];
                 r = launch_step();
                 tape = nullptr;
                 if (r != MOIST_OK) return r;
-                if ((r = adj_step()) != MOIST_OK) return r;
+                if ((r = adj_step(A.tapes[0])) != MOIST_OK) return r;
             }
         }
         CK(cudaStreamSynchronize(st));
