@@ -166,18 +166,22 @@ template <class T>
 struct FTend {
     __device__ void operator()(const BTend<T>& a, int bx, int by) const { b_tend(a.p, a.a, a.err, bx, by); }
 };
+// The factorisation and the acoustic substep run one thread per column in the batch: the
+// ensemble's columns give every SM enough warps to overlap their recurrences, which the column
+// strips of a single domain have to stage through shared memory instead (same values).
 template <class T, class TT>
 struct FThomas {
-    __device__ void operator()(const BThomas<T, TT>& a, int bx, int by) const {
-        b_thomas_strip<T, TT>(a.p, a.theta, a.rt2pres, a.dt_s, a.wc, a.ta, a.tb, a.tc, a.tcp, a.tpiv, a.err, bx, by);
+    __device__ void operator()(const BThomas<T, TT>& a, int bx, int) const {
+        b_thomas_col<T, TT>(a.p, a.theta, a.rt2pres, a.dt_s, a.ta, a.tb, a.tc, a.tcp, a.tpiv, a.err, bx);
     }
 };
 template <class T, class TT>
 struct FSub {
-    __device__ void operator()(const BSub<T, TT>& a, int bx, int by) const {
-        b_substep_strip<T, TT>(a.p, a.a, a.dt_s, a.ns_T, a.fact_tp64, a.wc, a.err, bx, by);
+    __device__ void operator()(const BSub<T, TT>& a, int bx, int) const {
+        b_substep_col<T, TT>(a.p, a.a, a.dt_s, a.ns_T, a.fact_tp64, a.err, bx);
     }
 };
+constexpr int BATCH_COL_THREADS = 64;
 template <class T>
 struct FPrep {
     __device__ void operator()(const BPrep<T>& a, int bx, int by) const {

@@ -438,9 +438,9 @@ __global__ void k_tend(DevParams<T> p, TendArgs<T> a, const int* err) {
 // dt_s, which are fixed during a stage, so the pivots and modified super-diagonal are formed
 // once per stage; each substep then repeats only the right-hand-side recurrence.
 template <class T, class TT>
-__global__ void k_thomas_factors(DevParams<T> p, const T* theta, const T* rt2pres, T dt_s, T* ta, T* tb,
-                                 T* tc, TT* tcp, TT* tpiv, const int* err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_thomas_col(DevParams<T> p, const T* theta, const T* rt2pres, T dt_s, T* ta, T* tb,
+                                             T* tc, TT* tcp, TT* tpiv, const int* err, int bx) {
+    const int i = bx * blockDim.x + threadIdx.x;
     const int nx = p.nx, nz = p.nz, P = p.P;
     if (i >= nx || halted(err)) return;
     const T* dz = p.dz;
@@ -476,6 +476,11 @@ __global__ void k_thomas_factors(DevParams<T> p, const T* theta, const T* rt2pre
         th_cur = th_next;
     }
 }
+template <class T, class TT>
+__global__ void k_thomas_factors(DevParams<T> p, const T* theta, const T* rt2pres, T dt_s, T* ta, T* tb,
+                                 T* tc, TT* tcp, TT* tpiv, const int* err) {
+    b_thomas_col(p, theta, rt2pres, dt_s, ta, tb, tc, tcp, tpiv, err, blockIdx.x);
+}
 
 template <class T, class TT>
 struct SubArgs {
@@ -493,9 +498,9 @@ struct SubArgs {
 // explicit rho_p / rho_theta_p, off-centred right-hand side, Thomas sweep for rho_w_p,
 // vertical rho_p / rho_theta_p updates, time-averaged momentum fluxes.
 template <class T, class TT>
-__global__ void k_substep(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T, double fact_tp64,
-                          const int* err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_substep_col(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T, double fact_tp64,
+                                              const int* err, int bx) {
+    const int i = bx * blockDim.x + threadIdx.x;
     const int nx = p.nx, nz = p.nz, P = p.P;
     if (i >= nx || halted(err)) return;
     const T dx = p.dx, EPS = p.EPS;
@@ -605,6 +610,11 @@ __global__ void k_substep(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T, doub
         a.rt_out[c] = a.rt_out[c] + dt_s * advection;
         if (k < ke) a.mfz[c] = a.mfz[c] + a.rw_p[c] / ns_T;
     }
+}
+template <class T, class TT>
+__global__ void k_substep(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T, double fact_tp64,
+                          const int* err) {
+    b_substep_col(p, a, dt_s, ns_T, fact_tp64, err, blockIdx.x);
 }
 
 // ----------------------------------------------------------------------------- column strips

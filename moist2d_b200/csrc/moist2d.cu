@@ -1503,10 +1503,9 @@ struct BatchImpl : BatchBase {
                 break;
             case BK_THOMAS:
             case BK_SUB:
-                block = dim3(STRIP_THREADS);
-                smem = max_strip_smem;
+                block = dim3(BATCH_COL_THREADS);
                 for (int i = 0; i < n; i++)
-                    for (unsigned bx = 0; bx < cdiv(m[i]->nx, m[i]->strip_wc); bx++) it.push_back({i, (int)bx, 0});
+                    for (unsigned bx = 0; bx < cdiv(m[i]->nx, BATCH_COL_THREADS); bx++) it.push_back({i, (int)bx, 0});
                 break;
             case BK_STREAM: {
                 // the longest sweeps (nx + nz steps) first, so that the short ones fill the tail
@@ -1535,14 +1534,14 @@ struct BatchImpl : BatchBase {
             BATCH_LAUNCH(BK_MEMSET, BMemset, FMemset, 1)
             BATCH_LAUNCH(BK_SF, BSf<T>, FSf<T>, 1)
             BATCH_LAUNCH(BK_RD, BRd<T>, FRd<T>, 1)
-            BATCH_LAUNCH(BK_PHYS, BPhys<T>, FPhys<T>, 1)
-            BATCH_LAUNCH(BK_DIAG, BDiag<T>, FDiag<T>, 1)
-            BATCH_LAUNCH(BK_TEND, BTend<T>, FTend<T>, 1)
+            BATCH_LAUNCH(BK_PHYS, BPhys<T>, FPhys<T>, 3)
+            BATCH_LAUNCH(BK_DIAG, BDiag<T>, FDiag<T>, 4)
+            BATCH_LAUNCH(BK_TEND, BTend<T>, FTend<T>, 4)
             BATCH_LAUNCH(BK_THOMAS, SINGLE_ARG(BThomas<T, TT>), SINGLE_ARG(FThomas<T, TT>), 4)
             BATCH_LAUNCH(BK_SUB, SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSub<T, TT>), 4)
-            BATCH_LAUNCH(BK_PREP, BPrep<T>, FPrep<T>, 1)
+            BATCH_LAUNCH(BK_PREP, BPrep<T>, FPrep<T>, 4)
             BATCH_LAUNCH(BK_STREAM, BStream<T>, FStream<T>, 1)
-            BATCH_LAUNCH(BK_UPD, BUpd<T>, FUpd<T>, 1)
+            BATCH_LAUNCH(BK_UPD, BUpd<T>, FUpd<T>, 4)
             BATCH_LAUNCH(BK_STAGE_END, BStageEnd, FStageEnd, 1)
             BATCH_LAUNCH(BK_PREC, BPrec<T>, FPrec<T>, 1)
             default:
