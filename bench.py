@@ -18,6 +18,8 @@ roofline: the kernel group with the largest device time; achieved = its algorith
         launch (words per cell below x cells) / its mean launch time from the same events.
 adjoint: (1 GPU, Float32) moist_adjoint_run on the 512 x 96 single-bubble domain, 600 steps,
         rain objective, checkpoints every 50 steps: forward and reverse wall times and their ratio.
+adjoint_ensemble: (1 GPU, Float32) moist_batch_adjoint_run on 64 uneven members (nx 512..1536,
+        nz 96/128), 20 steps, concurrent against one member at a time.
 ensemble: (1 GPU, Float32) the batched forward: 256 uneven members advanced together (one packed
         launch per kernel of the step, one CUDA graph per step), device time per step, its
         cell-steps/s, HBM fraction of the whole step's algorithmic bytes and ratio to `value`.
@@ -214,6 +216,45 @@ def measure_adjoint(nsteps, ckpt):
             "objective": g["objective"], "dJ_dK_auto": g["k_auto"], "dJ_dQc_threshold": g["qc_threshold"]}
 
 
+def measure_adjoint_ensemble(nmem, nsteps, ckpt):
+    """Batched adjoint: nmem Float32 members (nx in {512, 1024, 1536}, nz in {96, 128}, seeded
+    bubbles on the analytic sounding), rain objective per member, moist_batch_adjoint_run over
+    nsteps large steps with checkpoints every ckpt steps: wall time with the members running
+    concurrently and with one member at a time (nthreads = 1), and the batched forward's device
+    time for the same steps."""
+    from moist2d_b200 import model
+    from moist2d_b200.init import ensemble_member
+    mem = [ensemble_member(np.float32, seed=5, member=m, nx_choices=(512, 1024, 1536), nz_choices=(96, 128))
+           for m in range(nmem)]
+    cells = sum(p.Nx * p.Nz for p, _ in mem)
+    weights = []
+    for p, _ in mem:
+        w = np.zeros(p.ia)
+        w[p.is_ - 1:p.ie] = float(p.dx)
+        weights.append(w)
+    out = {"members": nmem, "cells": cells, "steps": nsteps, "ckpt_every": ckpt}
+    with model.Ensemble([p for p, _ in mem]) as e:
+        def upload():
+            for i, (_, s) in enumerate(mem):
+                e.upload(i, s)
+        upload()
+        e.adjoint(ckpt, ckpt, prec_weights=weights)  # warm-up: the members' adjoint buffers
+        for name, nt in (("concurrent", 0), ("one_at_a_time", 1)):
+            upload()
+            t0 = time.perf_counter()
+            e.adjoint(nsteps, ckpt, prec_weights=weights, nthreads=nt)
+            out[name + "_ms"] = (time.perf_counter() - t0) * 1e3
+        upload()
+        e.step(2)
+        out["forward_batched_ms"] = e.time_steps(nsteps)
+    out["speedup_vs_one_at_a_time"] = out["one_at_a_time_ms"] / out["concurrent_ms"]
+    out["adjoint_cell_steps_per_s"] = cells * nsteps / (out["concurrent_ms"] / 1e3)
+    out["adjoint_over_batched_forward"] = out["concurrent_ms"] / out["forward_batched_ms"]
+    out["workload"] = ("%d members, nx in {512,1024,1536}, nz in {96,128}, dx=250 m, dz=125 m, dt=2 s, ns=8, "
+                       "Float32, rain objective per member, %d of the 900 steps" % (nmem, nsteps))
+    return out
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's CPU path (no Julia here: the threaded oracle port)."""
     if rank != 0:
@@ -265,6 +306,8 @@ def main():
                     help="members of the batched-ensemble measurement (0 skips it)")
     ap.add_argument("--adjoint-steps", type=int, default=600,
                     help="large steps of the adjoint measurement (0 skips it)")
+    ap.add_argument("--adjoint-ensemble", type=int, default=64,
+                    help="members of the batched-adjoint measurement (0 skips it)")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
@@ -400,6 +443,12 @@ def main():
             adj = measure_adjoint(args.adjoint_steps, 50)
         except Exception as e:
             adj = {"error": str(e)}
+    adj_ens = None
+    if rank == 0 and world == 1 and args.adjoint_ensemble > 0 and args.precision == "f32":
+        try:
+            adj_ens = measure_adjoint_ensemble(args.adjoint_ensemble, 20, 10)
+        except Exception as e:
+            adj_ens = {"error": str(e)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -427,6 +476,7 @@ def main():
             "clocks": clk,
             "ensemble": ens,
             "adjoint": adj,
+            "adjoint_ensemble": adj_ens,
         }
         print(json.dumps(line), flush=True)
 

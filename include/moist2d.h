@@ -299,6 +299,16 @@ typedef struct moist_adjoint_grad {
 int moist_adjoint_run(moist_ctx* ctx, int nsteps, int ckpt_every, const moist_adjoint_seed* seed,
                       moist_adjoint_grad* out);
 
+/* moist_adjoint_run for every member of a batch (no counterpart in the reference): seeds[m] and
+ * out[m] belong to member m (seeds may be NULL: J = 0). The members' adjoint buffers are
+ * allocated one member at a time, then the members run concurrently from up to nthreads host
+ * threads (nthreads <= 0: one per member), each on its member context's stream, so that their
+ * kernels share the GPU. Each member is left at its final State; the next moist_batch_step
+ * continues from there. The first failing member's status is returned, its index in
+ * moist_batch_last_error. */
+int moist_batch_adjoint_run(moist_batch* b, int nsteps, int ckpt_every, const moist_adjoint_seed* seeds,
+                            moist_adjoint_grad* out, int nthreads);
+
 /* Kernel groups of one large step, for moist_step_profile. */
 enum {
     MOIST_KGROUP_PHYSICS = 0,   /* surface fluxes, radiation, Kessler + sedimentation + phys assembly */

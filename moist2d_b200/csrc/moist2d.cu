@@ -7,12 +7,14 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/moist2d.h"
@@ -56,6 +58,8 @@ struct CtxBase {
 struct BatchBase {
     virtual ~BatchBase() {}
     virtual int step(int nsteps) = 0;
+    virtual int adjoint(int nsteps, int ckpt, const moist_adjoint_seed* seeds, moist_adjoint_grad* out,
+                        int nthreads) = 0;
     virtual int time_steps(int nsteps, float* ms) = 0;
     virtual int profile(int nsteps, float* total_ms, float* group_ms) = 0;
 };
@@ -395,8 +399,13 @@ struct Ctx : CtxBase {
             }
         }
         strip_smem = strip_smem_bytes<T, TT>(nz, strip_wc);
-        CK(cudaFuncSetAttribute(k_thomas_strip<T, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem));
-        CK(cudaFuncSetAttribute(k_substep_strip<T, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)strip_smem));
+        // the limit is a property of the kernel, shared by every context of the process (whose
+        // strips differ, and a batch widens its members' strips): allow the device maximum, the
+        // launch's own size sets the occupancy
+        int optin = 0;
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        CK(cudaFuncSetAttribute(k_thomas_strip<T, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        CK(cudaFuncSetAttribute(k_substep_strip<T, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
         return MOIST_OK;
     }
 
@@ -939,8 +948,10 @@ struct Ctx : CtxBase {
                 CK(cudaMemcpyAsync(*g[j], hd.data(), nz * sizeof(double), cudaMemcpyHostToDevice, st));
                 CK(cudaStreamSynchronize(st));
             }
-            CK(cudaFuncSetAttribute(k_adj_sub_solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)adj_solve_smem(nz)));
+            int dev = 0, optin = 0;  // shared by all contexts (other nz): the device maximum
+            CK(cudaGetDevice(&dev));
+            CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+            CK(cudaFuncSetAttribute(k_adj_sub_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
             A.pd = params_to_double(dp);
             A.pd.dz = A.dz;
             A.pd.z = A.z;
@@ -972,10 +983,14 @@ struct Ctx : CtxBase {
         Adj& A = *adj;
         // a tape per step of a segment when that fits in half the free device memory (the
         // segment is then recomputed once), else one tape and the segment's States
-        size_t free_b = 0, total_b = 0;
-        CK(cudaMemGetInfo(&free_b, &total_b));
-        const size_t need = (size_t)std::max<long>(0, (long)ckpt - (long)A.tapes.size()) * tape_fields() * fsz * sizeof(T);
-        seg_tapes = A.tapes.size() >= (size_t)ckpt || need <= free_b / 2;
+        if (ckpt != adj_ckpt) {  // decided once per checkpoint interval
+            size_t free_b = 0, total_b = 0;
+            CK(cudaMemGetInfo(&free_b, &total_b));
+            const size_t need =
+                (size_t)std::max<long>(0, (long)ckpt - (long)A.tapes.size()) * tape_fields() * fsz * sizeof(T);
+            seg_tapes = A.tapes.size() >= (size_t)ckpt || need <= free_b / 2;
+            adj_ckpt = ckpt;
+        }
         const size_t ntapes = seg_tapes ? (size_t)ckpt : 1;
         while (A.tapes.size() < ntapes) {
             A.tapes.emplace_back();
@@ -996,6 +1011,7 @@ struct Ctx : CtxBase {
     }
 
     bool seg_tapes = false;
+    int adj_ckpt = -1;  // checkpoint interval the tape mode was chosen for
 
     size_t tape_fields() const {
         size_t n = 21 + 3 + 6 + 9 + 1;
@@ -1553,9 +1569,69 @@ struct BatchImpl : BatchBase {
     }
 #undef BATCH_LAUNCH
 
+    // the members' State buffers the two step graphs read at parity 0 (cur0) and 1 (nxt0)
+    std::vector<StateP<T>> cur0, nxt0;
+
+    // A member stepped on its own (its moist_rk3_step, moist_adjoint_run, ...) swaps its current
+    // and next State; the graphs read the buffers of their parity, so move such a member's State
+    // back into the buffer the next graph reads.
+    int sync_members() {
+        for (size_t i = 0; i < m.size(); i++) {
+            const StateP<T>& want = parity == 0 ? cur0[i] : nxt0[i];
+            const StateP<T>& other = parity == 0 ? nxt0[i] : cur0[i];
+            if (m[i]->cur.rho == want.rho) continue;
+            const T* src[7] = {m[i]->cur.rho, m[i]->cur.ru, m[i]->cur.rw, m[i]->cur.rt,
+                               m[i]->cur.qv, m[i]->cur.qc, m[i]->cur.qr};
+            T* dst[7] = {want.rho, want.ru, want.rw, want.rt, want.qv, want.qc, want.qr};
+            for (int f = 0; f < 7; f++)
+                BCK(cudaMemcpyAsync(dst[f], src[f], m[i]->fsz * sizeof(T), cudaMemcpyDeviceToDevice, st));
+            m[i]->cur = want;
+            m[i]->nxt = other;
+        }
+        return MOIST_OK;
+    }
+
+    // every member's moist_adjoint_run, the members' device buffers allocated one member at a
+    // time first, then the runs from up to nthreads host threads (each member works on its own
+    // stream, so their kernels overlap on the GPU)
+    int adjoint(int nsteps, int ckpt, const moist_adjoint_seed* seeds, moist_adjoint_grad* out,
+                int nthreads) override {
+        const int n = (int)m.size();
+        if (!out || nsteps < 1 || ckpt < 1)
+            return set_berr(owner, MOIST_ERR_ARG, "moist_batch_adjoint_run needs out != NULL, nsteps >= 1, ckpt_every >= 1");
+        BCK(cudaStreamSynchronize(st));
+        const int ck = std::min(ckpt, nsteps);
+        for (int i = 0; i < n; i++) {
+            if (m[i]->dp.do_sf || m[i]->dp.do_rd) break;  // reported by the member's own call
+            if (int r = m[i]->adj_alloc(nsteps, ck))
+                return set_berr(owner, r, "member %d: %s", i, m[i]->owner->err.c_str());
+        }
+        std::atomic<int> next{0};
+        std::vector<int> rc(n, MOIST_OK);
+        const int dev = owner->device;
+        auto work = [&]() {
+            cudaSetDevice(dev);
+            for (int i; (i = next.fetch_add(1)) < n;)
+                rc[i] = m[i]->adjoint_run(nsteps, ckpt, seeds ? seeds + i : nullptr, out + i);
+        };
+        const int nt = std::max(1, std::min(nthreads > 0 ? nthreads : n, n));
+        std::vector<std::thread> th;
+        for (int t = 1; t < nt; t++) th.emplace_back(work);
+        work();
+        for (auto& t : th) t.join();
+        for (int i = 0; i < n; i++)
+            if (rc[i] != MOIST_OK) {
+                if (rc[i] == MOIST_ERR_NAN) owner->nan_member = i;
+                return set_berr(owner, rc[i], "member %d: %s", i, m[i]->owner->err.c_str());
+            }
+        return MOIST_OK;
+    }
+
     int build() {
         const int n = (int)m.size();
         for (auto* c : m) {
+            cur0.push_back(c->cur);
+            nxt0.push_back(c->nxt);
             // a batch has blocks enough for every SM without narrow strips: take the widest
             // strip whose shared memory leaves room for several blocks per SM
             for (int w : {8, 4, 2, 1}) {
@@ -1637,6 +1713,7 @@ struct BatchImpl : BatchBase {
 
     int step(int nsteps) override {
         const int n = (int)m.size();
+        if (int r = sync_members()) return r;
         k_reset_err<<<cdiv(n, 128), 128, 0, st>>>(errs, n);
         if (int r = launch_steps(nsteps)) return r;
         k_gather_err<<<cdiv(n, 128), 128, 0, st>>>(errs, n, err_all);
@@ -1664,6 +1741,7 @@ struct BatchImpl : BatchBase {
 
     // nsteps without the graphs: events around every packed launch, summed per kernel group
     int profile(int nsteps, float* total_ms, float* group_ms) override {
+        if (int r = sync_members()) return r;
         static const int group_of[BK_NKINDS] = {MOIST_KGROUP_PHYSICS,  MOIST_KGROUP_PHYSICS, MOIST_KGROUP_PHYSICS,
                                                 MOIST_KGROUP_PHYSICS,  MOIST_KGROUP_PROLOGUE, MOIST_KGROUP_PROLOGUE,
                                                 MOIST_KGROUP_PROLOGUE, MOIST_KGROUP_SUBSTEP, MOIST_KGROUP_TRACER,
@@ -1697,6 +1775,7 @@ struct BatchImpl : BatchBase {
     }
 
     int time_steps(int nsteps, float* ms) override {
+        if (int r = sync_members()) return r;
         cudaEvent_t e0, e1;
         BCK(cudaEventCreate(&e0));
         BCK(cudaEventCreate(&e1));
@@ -1865,6 +1944,13 @@ int moist_batch_upload(moist_batch* b, int member, const moist_state_host* s) {
 int moist_batch_download(moist_batch* b, int member, moist_state_host* s) {
     moist_ctx* c = moist_batch_member(b, member);
     return c ? moist_download_state(c, s) : MOIST_ERR_ARG;
+}
+
+int moist_batch_adjoint_run(moist_batch* b, int nsteps, int ckpt_every, const moist_adjoint_seed* seeds,
+                            moist_adjoint_grad* out, int nthreads) {
+    if (!b) return MOIST_ERR_ARG;
+    cudaSetDevice(b->device);
+    return b->impl->adjoint(nsteps, ckpt_every, seeds, out, nthreads);
 }
 
 int moist_batch_step(moist_batch* b, int nsteps) {

@@ -271,6 +271,44 @@ class Ensemble:
     def nan_member(self):
         return lib().moist_batch_nan_member(self.b)
 
+    def adjoint(self, nsteps, ckpt_every=50, prec_weights=None, state_seeds=None, nthreads=0):
+        """moist_batch_adjoint_run: Model.adjoint for every member, run concurrently.
+        prec_weights / state_seeds: per-member lists (entries as for Model.adjoint) or None.
+        Returns one gradient dict per member; every member is left at its final State."""
+        n = len(self.params)
+        keep = []
+
+        def f64(a, shape):
+            a = np.asfortranarray(np.asarray(a, dtype=np.float64))
+            if a.shape != shape:
+                raise ValueError("seed of shape %s, expected %s" % (a.shape, shape))
+            keep.append(a)
+            return a.ctypes.data
+
+        seeds = (abi.moist_adjoint_seed * n)()
+        outs = (abi.moist_adjoint_grad * n)()
+        grads = []
+        for m, p in enumerate(self.params):
+            ka, ia = p.ka, p.ia
+            if prec_weights is not None and prec_weights[m] is not None:
+                seeds[m].prec_weight = f64(prec_weights[m], (ia,))
+            sd = state_seeds[m] if state_seeds is not None else None
+            g = {name: np.zeros((ka, ia), dtype=np.float64, order="F") for name in abi.PROGNOSTIC}
+            g["prec"] = np.zeros(ia, dtype=np.float64)
+            for j, name in enumerate(abi.PROGNOSTIC):
+                if sd is not None and name in sd:
+                    seeds[m].state[j] = f64(sd[name], (ka, ia))
+                outs[m].state[j] = g[name].ctypes.data
+            outs[m].prec = g["prec"].ctypes.data
+            grads.append(g)
+        self._check(lib().moist_batch_adjoint_run(self.b, int(nsteps), int(ckpt_every), seeds, outs, int(nthreads)),
+                    "moist_batch_adjoint_run")
+        for m, g in enumerate(grads):
+            o = outs[m]
+            g.update(k_auto=o.k_auto, qc_threshold=o.qc_threshold, objective=o.objective,
+                     forward_ms=o.forward_ms, reverse_ms=o.reverse_ms)
+        return grads
+
     def budget(self, i):
         out = (C.c_double * 4)()
         ctx = self.member(i)

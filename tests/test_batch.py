@@ -80,3 +80,55 @@ def test_ensemble_rejects_mixed_substeps():
     p2 = p1.replace(ns=5)
     with pytest.raises(ValueError):
         model.Ensemble([p1, p2])
+
+
+def test_member_stepped_alone_then_batch():
+    """A member advanced through its own context (moist_batch_member + moist_rk3_step) swaps its
+    State buffers; the next batch step continues from that State."""
+    mem = members(np.float32)
+    with model.Ensemble([p for p, _ in mem]) as e:
+        for i, (_, s) in enumerate(mem):
+            e.upload(i, s)
+        e.step(1)
+        ctx = e.member(2)
+        model._raise(lib_step(ctx, 1), ctx, "moist_rk3_step on a member")
+        e.step(2)
+        got = [e.download(i, s.copy()) for i, (_, s) in enumerate(mem)]
+    for j, ((p, s), g) in enumerate(zip(mem, got)):
+        compare(g, model.rk3_step(s.copy(), p, 4 if j == 2 else 3), p)
+
+
+def lib_step(ctx, n):
+    from moist2d_b200._lib import lib
+    return lib().moist_rk3_step(ctx, n)
+
+
+@pytest.mark.parametrize("T", [np.float32, np.float64], ids=["f32", "f64"])
+def test_batch_adjoint_matches_single_adjoints(T):
+    """moist_batch_adjoint_run gives every member the gradient of its own moist_adjoint_run
+    (a context with the same streaming tracer sweep; the adjoint's atomic sums may round in a
+    different order) and leaves the members where the batch continues from."""
+    mem = members(T)
+    rng = np.random.default_rng(4)
+    weights = []
+    for p, _ in mem:
+        w = np.zeros(p.ia)
+        w[p.is_ - 1:p.ie] = float(p.dx)
+        weights.append(w)
+    seeds = [{"rho_theta": rng.standard_normal((p.ka, p.ia)) * 1e-3} for p, _ in mem]
+    with model.Ensemble([p for p, _ in mem]) as e:
+        for i, (_, s) in enumerate(mem):
+            e.upload(i, s)
+        got = e.adjoint(3, 2, prec_weights=weights, state_seeds=seeds, nthreads=3)
+        e.step(1)
+        fin = [e.download(i, s.copy()) for i, (_, s) in enumerate(mem)]
+    for i, (p, s) in enumerate(mem):
+        with model.Model(p, abi.MOIST_FLAG_TRACER_STREAM) as m:
+            m.upload(s)
+            ref = m.adjoint(3, 2, prec_weight=weights[i], state_seed=seeds[i])
+        for f in abi.PROGNOSTIC:
+            scale = max(np.max(np.abs(ref[f])), 1e-300)
+            assert np.max(np.abs(got[i][f] - ref[f])) <= 1e-10 * scale, (i, f)
+        for k in ("k_auto", "qc_threshold", "objective"):
+            assert np.isclose(got[i][k], ref[k], rtol=1e-10, atol=0.0), (i, k)
+        compare(fin[i], model.rk3_step(s.copy(), p, 4), p)
