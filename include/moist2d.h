@@ -309,6 +309,17 @@ int moist_adjoint_run(moist_ctx* ctx, int nsteps, int ckpt_every, const moist_ad
 int moist_batch_adjoint_run(moist_batch* b, int nsteps, int ckpt_every, const moist_adjoint_seed* seeds,
                             moist_adjoint_grad* out, int nthreads);
 
+/* ---- Autotuner (no counterpart in the reference). moist_autotune times nsteps large steps of
+ * the context for every strip width of the factorisation and acoustic-substep kernels (1, 2, 4
+ * or 8 columns per block) and every exact tracer sweep the context can run (tiled; streaming
+ * when nz <= 256), each from the same saved State, keeps the fastest for the context's later
+ * steps and restores the State: results are the same bit for bit whatever it picks.
+ * moist_batch_autotune does the same for a batch over the threads per block (32, 64, 128,
+ * 256) of its per-column kernels and rebuilds the batch's step graphs. report (if not NULL)
+ * receives the timings and the choice. */
+int moist_autotune(moist_ctx* ctx, int nsteps, char* report, size_t report_len);
+int moist_batch_autotune(moist_batch* b, int nsteps, char* report, size_t report_len);
+
 /* Kernel groups of one large step, for moist_step_profile. */
 enum {
     MOIST_KGROUP_PHYSICS = 0,   /* surface fluxes, radiation, Kessler + sedimentation + phys assembly */

@@ -53,6 +53,7 @@ struct CtxBase {
     virtual int rk3_host(moist_state_host* s, int nsteps) = 0;
     virtual int pass_counts(int* counts, int n) = 0;
     virtual int adjoint_run(int nsteps, int ckpt, const moist_adjoint_seed* seed, moist_adjoint_grad* out) = 0;
+    virtual int autotune(int nsteps, std::string& report) = 0;
 };
 
 struct BatchBase {
@@ -60,6 +61,7 @@ struct BatchBase {
     virtual int step(int nsteps) = 0;
     virtual int adjoint(int nsteps, int ckpt, const moist_adjoint_seed* seeds, moist_adjoint_grad* out,
                         int nthreads) = 0;
+    virtual int autotune(int nsteps, std::string& report) = 0;
     virtual int time_steps(int nsteps, float* ms) = 0;
     virtual int profile(int nsteps, float* total_ms, float* group_ms) = 0;
 };
@@ -927,6 +929,97 @@ struct Ctx : CtxBase {
         return MOIST_OK;
     }
 
+    // ------------------------------------------------------------------ autotuner
+    // Times nsteps large steps for every strip width of the factorisation and substep kernels
+    // (1, 2, 4, 8 columns) and every tracer sweep this context can run (tiled, row-streaming),
+    // each from the same saved State, keeps the fastest and restores the State. All candidates
+    // give the same results bit for bit, so the choice changes only the speed.
+    int autotune(int nsteps, std::string& report) override {
+        if (int r = check_stage_shape()) return r;
+        if (nsteps < 1) return set_err(owner, MOIST_ERR_ARG, "moist_autotune needs nsteps >= 1");
+        int dev = 0, optin = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        if (nz <= STREAM_MAX_ROWS && !s_old[0]) {  // buffers of the streaming sweep
+            for (int t = 0; t < 3; t++) AL(s_old[t], fsz);
+            AL(rrho, fsz);
+        }
+        std::array<T*, 8>& save = tune_save;
+        if (!save[0]) {  // kept for later calls
+            for (int f = 0; f < 7; f++) AL(save[f], fsz);
+            AL(save[7], (size_t)P);
+        }
+        {
+            const auto src = cur_fields();
+            if (int r = copyf(src.data(), save.data(), 7)) return r;
+            CK(cudaMemcpyAsync(save[7], prec, P * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        }
+        struct Cand {
+            int wc;
+            int tracer;  // 0 tiles, 1 stream
+        };
+        std::vector<Cand> cands;
+        for (int tr = 0; tr < 2; tr++) {
+            if (tr == 0 && !strips) continue;  // the tiles need all of them resident (init_tiles)
+            if (tr == 1 && !s_old[0]) continue;
+            for (int w : {1, 2, 4, 8})
+                if (w <= nx && strip_smem_bytes<T, TT>(nz, w) <= (size_t)optin) cands.push_back({w, tr});
+        }
+        const int wc0 = strip_wc, str0 = use_stream, til0 = use_tiles;
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        float best = 1e30f;
+        Cand bc{wc0, str0 ? 1 : 0};
+        char buf[128];
+        for (const Cand& c : cands) {
+            strip_wc = c.wc;
+            strip_smem = strip_smem_bytes<T, TT>(nz, c.wc);
+            use_tiles = c.tracer == 0;
+            use_stream = c.tracer == 1;
+            const auto dst = cur_fields();
+            if (int r = copyf(save.data(), dst.data(), 7)) return r;
+            CK(reset_err());
+            int r = launch_step();  // warm-up
+            CK(cudaEventRecord(e0, st));
+            for (int n = 0; n < nsteps && r == MOIST_OK; n++) r = launch_step();
+            CK(cudaEventRecord(e1, st));
+            if (r != MOIST_OK) return r;
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            ms /= nsteps;
+            snprintf(buf, sizeof buf, "%sstrip %d, %s: %.3f ms", report.empty() ? "" : "; ", c.wc,
+                     c.tracer ? "stream" : "tiles", ms);
+            report += buf;
+            if (ms < best) {
+                best = ms;
+                bc = c;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (cands.empty()) {
+            strip_wc = wc0;
+            use_stream = str0;
+            use_tiles = til0;
+        } else {
+            strip_wc = bc.wc;
+            use_tiles = bc.tracer == 0;
+            use_stream = bc.tracer == 1;
+        }
+        strip_smem = strip_smem_bytes<T, TT>(nz, strip_wc);
+        snprintf(buf, sizeof buf, " -> strip %d, %s (%.3f ms per step)", strip_wc, use_stream ? "stream" : "tiles", best);
+        report += buf;
+        {
+            const auto dst = cur_fields();
+            if (int r = copyf(save.data(), dst.data(), 7)) return r;
+            CK(cudaMemcpyAsync(prec, save[7], P * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        }
+        CK(reset_err());
+        return finish();
+    }
+
     // ------------------------------------------------------------------ adjoint (adjoint.cuh)
     int stage_substeps(int j) const {
         return j == 0 ? std::max(1, (int)std::ceil(ns / 3.0)) : (j == 1 ? std::max(1, (int)std::ceil(ns / 2.0)) : ns);
@@ -1011,6 +1104,7 @@ struct Ctx : CtxBase {
     }
 
     bool seg_tapes = false;
+    std::array<T*, 8> tune_save{};  // the State saved by autotune
     int adj_ckpt = -1;  // checkpoint interval the tape mode was chosen for
 
     size_t tape_fields() const {
@@ -1464,6 +1558,8 @@ struct BatchImpl : BatchBase {
     };
     std::vector<Slot> slots[2];
     std::vector<void*> allocs;
+    int col_threads = BATCH_COL_THREADS;  // threads per block of the per-column kernels
+    std::vector<std::array<T*, 8>> tune_save;  // the members' States saved by autotune
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     int parity = 0;
     int** errs = nullptr;  // device: the members' error words
@@ -1519,9 +1615,9 @@ struct BatchImpl : BatchBase {
                 break;
             case BK_THOMAS:
             case BK_SUB:
-                block = dim3(BATCH_COL_THREADS);
+                block = dim3(col_threads);
                 for (int i = 0; i < n; i++)
-                    for (unsigned bx = 0; bx < cdiv(m[i]->nx, BATCH_COL_THREADS); bx++) it.push_back({i, (int)bx, 0});
+                    for (unsigned bx = 0; bx < cdiv(m[i]->nx, col_threads); bx++) it.push_back({i, (int)bx, 0});
                 break;
             case BK_STREAM: {
                 // the longest sweeps (nx + nz steps) first, so that the short ones fill the tail
@@ -1686,7 +1782,16 @@ struct BatchImpl : BatchBase {
         if (int r = dalloc(&errs, n)) return r;
         if (int r = dalloc(&err_all, 4 * n)) return r;
         BCK(cudaMemcpy(errs, ev.data(), n * sizeof(int*), cudaMemcpyHostToDevice));
+        return capture();
+    }
+
+    // the two step graphs (even and odd step) from the packed slots
+    int capture() {
         for (int q = 0; q < 2; q++) {
+            if (exec[q]) {
+                cudaGraphExecDestroy(exec[q]);
+                exec[q] = nullptr;
+            }
             cudaGraph_t g;
             BCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             int r = MOIST_OK;
@@ -1699,6 +1804,79 @@ struct BatchImpl : BatchBase {
             cudaGraphDestroy(g);
             if (e != cudaSuccess) return set_berr(owner, MOIST_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
         }
+        return MOIST_OK;
+    }
+
+    // new work lists for the per-column kernels and new graphs
+    int set_col_threads(int ct) {
+        col_threads = ct;
+        for (int q = 0; q < 2; q++)
+            for (Slot& sl : slots[q]) {
+                if (sl.kind != BK_SUB && sl.kind != BK_THOMAS) continue;
+                std::vector<BItem> it;
+                items_of(sl.kind, it, sl.block, sl.smem);
+                BItem* ditems;
+                if (int r = dalloc(&ditems, it.size())) return r;
+                BCK(cudaMemcpy(ditems, it.data(), it.size() * sizeof(BItem), cudaMemcpyHostToDevice));
+                sl.items = ditems;
+                sl.nitems = (unsigned)it.size();
+            }
+        return capture();
+    }
+
+    // Times nsteps batch steps for 32, 64, 128 and 256 threads per block of the per-column
+    // kernels (factorisation and acoustic substep), each from the same saved States, keeps the
+    // fastest and restores the States (same results for every choice).
+    int autotune(int nsteps, std::string& report) override {
+        if (nsteps < 1) return set_berr(owner, MOIST_ERR_ARG, "moist_batch_autotune needs nsteps >= 1");
+        if (int r = sync_members()) return r;
+        const int n = (int)m.size();
+        std::vector<std::array<T*, 8>>& save = tune_save;
+        if (save.empty()) {  // kept for later calls
+            save.resize(n);
+            for (int i = 0; i < n; i++) {
+                for (int f = 0; f < 7; f++)
+                    if (int r = dalloc(&save[i][f], m[i]->fsz)) return r;
+                if (int r = dalloc(&save[i][7], (size_t)m[i]->P)) return r;
+            }
+        }
+        auto copy_all = [&](bool to_save) -> int {
+            for (int i = 0; i < n; i++) {
+                const auto cf = m[i]->cur_fields();
+                for (int f = 0; f < 7; f++) {
+                    T* a = to_save ? save[i][f] : cf[f];
+                    const T* b = to_save ? cf[f] : save[i][f];
+                    BCK(cudaMemcpyAsync(a, b, m[i]->fsz * sizeof(T), cudaMemcpyDeviceToDevice, st));
+                }
+                T* a = to_save ? save[i][7] : m[i]->prec;
+                const T* b = to_save ? m[i]->prec : save[i][7];
+                BCK(cudaMemcpyAsync(a, b, m[i]->P * sizeof(T), cudaMemcpyDeviceToDevice, st));
+            }
+            return MOIST_OK;
+        };
+        if (int r = copy_all(true)) return r;
+        float best = 1e30f;
+        int bct = col_threads;
+        char buf[96];
+        for (int ct : {32, 64, 128, 256}) {
+            if (int r = set_col_threads(ct)) return r;
+            if (int r = copy_all(false)) return r;
+            float ms = 0.f;
+            if (int r = launch_steps(1)) return r;  // warm-up
+            if (int r = time_steps(nsteps, &ms)) return r;
+            ms /= nsteps;
+            snprintf(buf, sizeof buf, "%scolumn block %d: %.2f ms", report.empty() ? "" : "; ", ct, ms);
+            report += buf;
+            if (ms < best) {
+                best = ms;
+                bct = ct;
+            }
+        }
+        if (int r = set_col_threads(bct)) return r;
+        if (int r = copy_all(false)) return r;
+        BCK(cudaStreamSynchronize(st));
+        snprintf(buf, sizeof buf, " -> column block %d (%.2f ms per step)", bct, best);
+        report += buf;
         return MOIST_OK;
     }
 
@@ -1951,6 +2129,24 @@ int moist_batch_adjoint_run(moist_batch* b, int nsteps, int ckpt_every, const mo
     if (!b) return MOIST_ERR_ARG;
     cudaSetDevice(b->device);
     return b->impl->adjoint(nsteps, ckpt_every, seeds, out, nthreads);
+}
+
+int moist_autotune(moist_ctx* c, int nsteps, char* report, size_t report_len) {
+    if (!c) return MOIST_ERR_ARG;
+    if (cudaSetDevice(c->device) != cudaSuccess) return MOIST_ERR_CUDA;
+    std::string rep;
+    const int r = c->impl->autotune(nsteps, rep);
+    if (report && report_len) snprintf(report, report_len, "%s", rep.c_str());
+    return r;
+}
+
+int moist_batch_autotune(moist_batch* b, int nsteps, char* report, size_t report_len) {
+    if (!b) return MOIST_ERR_ARG;
+    cudaSetDevice(b->device);
+    std::string rep;
+    const int r = b->impl->autotune(nsteps, rep);
+    if (report && report_len) snprintf(report, report_len, "%s", rep.c_str());
+    return r;
 }
 
 int moist_batch_step(moist_batch* b, int nsteps) {

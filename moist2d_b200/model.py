@@ -89,6 +89,13 @@ class Model:
     def nan_field(self):
         return lib().moist_nan_field(self.ctx)
 
+    def autotune(self, nsteps=3):
+        """moist_autotune: time every strip width and exact tracer sweep from the current State,
+        keep the fastest, restore the State; returns the report (timings and choice)."""
+        buf = C.create_string_buffer(2048)
+        _raise(lib().moist_autotune(self.ctx, int(nsteps), buf, len(buf)), self.ctx, "moist_autotune")
+        return buf.value.decode()
+
     def adjoint(self, nsteps, ckpt_every=50, prec_weight=None, state_seed=None):
         """Advance the resident State nsteps large steps and return the gradient of
         J = sum(prec_weight * prec_final) + sum_f sum(state_seed[f] * S_final.f)
@@ -270,6 +277,13 @@ class Ensemble:
     @property
     def nan_member(self):
         return lib().moist_batch_nan_member(self.b)
+
+    def autotune(self, nsteps=2):
+        """moist_batch_autotune: time the per-column kernels' block sizes from the current
+        States, keep the fastest, restore the States; returns the report."""
+        buf = C.create_string_buffer(1024)
+        self._check(lib().moist_batch_autotune(self.b, int(nsteps), buf, len(buf)), "moist_batch_autotune")
+        return buf.value.decode()
 
     def adjoint(self, nsteps, ckpt_every=50, prec_weights=None, state_seeds=None, nthreads=0):
         """moist_batch_adjoint_run: Model.adjoint for every member, run concurrently.
