@@ -176,6 +176,7 @@ def measure_ensemble(nmem, steps, warmup, peak, plain_value):
         for i, (_, s) in enumerate(mem):
             e.upload(i, s)
         setup_s = time.perf_counter() - t0
+        tune = e.autotune(2)
         e.step(warmup)
         ms = e.time_steps(steps) / steps
         tot, g = e.profile(2)
@@ -184,7 +185,7 @@ def measure_ensemble(nmem, steps, warmup, peak, plain_value):
             "value": value, "unit": "cell-steps/s", "vs_plain": value / plain_value,
             "hbm_frac": cells * words * 4 / (ms / 1e3) / 1e9 / peak,
             "group_ms_per_step": {k: float(x) / 2 for k, x in zip(GROUPS, g)},
-            "setup_s": setup_s,
+            "setup_s": setup_s, "autotune": tune,
             "workload": "%d members, nx in {256,...,2048}, nz in {64,96,128}, dx=250 m, dz=125 m, "
                         "dt=2 s, ns=8, one seeded bubble each on the analytic sounding, Float32 "
                         "state with fp64 w-p elimination" % nmem}
@@ -339,6 +340,7 @@ def main():
     bpw = np.dtype(T).itemsize
     m = Model(p)
     m.upload(s)
+    tune = m.autotune(3)  # strip width and tracer sweep; leaves the State as it was
     ext = torch.cuda.ExternalStream(L.moist_stream(m.ctx), device=torch.device("cuda", local_rank))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -467,7 +469,7 @@ def main():
                        (" state, fp64 w-p elimination" if args.precision == "f32" else ""),
                        "l2": "flushed before every timed step (256 MiB write)",
                        "parallelism": "replicas" if world > 1 else "single domain",
-                       "words_per_cell_step": words_per_cell_step(p.ns)},
+                       "words_per_cell_step": words_per_cell_step(p.ns), "autotune": tune},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
