@@ -309,6 +309,27 @@ int moist_adjoint_run(moist_ctx* ctx, int nsteps, int ckpt_every, const moist_ad
 int moist_batch_adjoint_run(moist_batch* b, int nsteps, int ckpt_every, const moist_adjoint_seed* seeds,
                             moist_adjoint_grad* out, int nthreads);
 
+/* output_history's primitive variables (moist.jl:1795-1835) computed on the device from the
+ * context State, so that a run_sim-style driver reads only what it writes to its history file:
+ * out[f] (f = MOIST_DIAG_*, NULL to skip) receives field f as a host (Nz, Nx) array of the
+ * context precision, z fastest, interior only (the file's layout); summary (if not NULL)
+ * receives the run log's min w, max w (m/s), max qc, max qr (g/kg), min RH, max RH (%)
+ * (moist.jl:1838-1843). The energy sums of the log come from moist_budget. */
+enum {
+    MOIST_DIAG_U = 0,       /* u at cell centres, (rho_u[i] + rho_u[i-1]) / 2 / rho */
+    MOIST_DIAG_W = 1,       /* w at cell centres */
+    MOIST_DIAG_THETA = 2,
+    MOIST_DIAG_QV = 3,
+    MOIST_DIAG_QC = 4,
+    MOIST_DIAG_QR = 5,
+    MOIST_DIAG_PRES = 6,
+    MOIST_DIAG_TEMP = 7,
+    MOIST_DIAG_THETAE = 8,  /* equivalent potential temperature */
+    MOIST_DIAG_RH = 9,      /* relative humidity (%) */
+    MOIST_NDIAG = 10
+};
+int moist_history_diagnostics(moist_ctx* ctx, void* const out[MOIST_NDIAG], double summary[6]);
+
 /* ---- Autotuner (no counterpart in the reference). moist_autotune times nsteps large steps of
  * the context for every strip width of the factorisation and acoustic-substep kernels (1, 2, 4
  * or 8 columns per block) and every exact tracer sweep the context can run (tiled; streaming

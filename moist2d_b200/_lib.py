@@ -19,7 +19,7 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_batch_destroy", "moist_batch_member", "moist_batch_upload", "moist_batch_download",
            "moist_batch_step", "moist_batch_time_steps", "moist_batch_last_error", "moist_batch_nan_member",
            "moist_batch_profile", "moist_adjoint_run", "moist_batch_adjoint_run",
-           "moist_autotune", "moist_batch_autotune")
+           "moist_autotune", "moist_batch_autotune", "moist_history_diagnostics")
 
 
 def lib():
@@ -74,6 +74,7 @@ def lib():
         L.moist_batch_profile.argtypes = [B, I, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.moist_adjoint_run.argtypes = [Ctx, I, I, C.POINTER(moist_adjoint_seed), C.POINTER(moist_adjoint_grad)]
         L.moist_autotune.argtypes = [Ctx, I, C.c_char_p, C.c_size_t]
+        L.moist_history_diagnostics.argtypes = [Ctx, C.POINTER(V), C.POINTER(D)]
         L.moist_batch_autotune.argtypes = [B, I, C.c_char_p, C.c_size_t]
         L.moist_batch_adjoint_run.argtypes = [B, I, I, C.POINTER(moist_adjoint_seed), C.POINTER(moist_adjoint_grad), I]
         _lib = L

@@ -18,6 +18,7 @@ MOIST_ERR_NOMEM = 6
 MOIST_FLAG_TRI_NATIVE = 1
 MOIST_FLAG_TRACER_WAVEFRONT = 2
 MOIST_FLAG_TRACER_STREAM = 4
+MOIST_NDIAG = 10
 
 MOIST_KGROUP_PHYSICS = 0
 MOIST_KGROUP_PROLOGUE = 1

@@ -966,6 +966,76 @@ __global__ void k_tracer_wavefront(DevParams<T> p, TracerArgs<T> a, const int* e
     }
 }
 
+// ----------------------------------------------------------------------------- history output
+
+constexpr int HIST_THREADS = 256;
+
+// output_history's primitive variables (moist.jl:1795-1835), one thread per cell: out[f] holds
+// field f (u, w, theta, qv, qc, qr, pres, temp, theta_e, RH) as an (nz, nx) array with z fastest
+// (the history file's layout); part[block][6] = min w, max w, max qc, max qr, min RH, max RH of
+// the block's cells.
+template <class T>
+__global__ void __launch_bounds__(HIST_THREADS) k_history_diag(DevParams<T> p, StateP<T> s, T* out, double* part) {
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    const size_t ncell = (size_t)nx * nz;
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double v6[6] = {1e300, -1e300, -1e300, -1e300, 1e300, -1e300};
+    if (idx < ncell) {
+        const int k = (int)(idx / nx), i = (int)(idx - (size_t)k * nx);
+        const size_t c = MOIST_IDX(k, i);
+        const T rho = s.rho[c], rt = s.rt[c];
+        const T rho_inv = T(1.0) / rho;
+        const T theta = rt * rho_inv;
+        const T qv = s.qv[c] * rho_inv, qc = s.qc[c] * rho_inv, qr = s.qr[c] * rho_inv;
+        const T u = (s.ru[c] + s.ru[MOIST_IDX(k, wrapx(i - 1, nx))]) * T(0.5) * rho_inv;
+        const T w = k > 0 ? (s.rw[c] + s.rw[c - P]) * T(0.5) * rho_inv : s.rw[c] * T(0.5) * rho_inv;
+        const T qt = qv + qc + qr;
+        const T qd = T(1.0) - qt;
+        const T r = p.Rd * qd + p.Rv * qv;
+        T cp = p.Cpd * qd + p.Cpv * qv + p.Cpl * (qc + qr);
+        const T cv = cp - r;
+        const T pi = mm::mpow(r * rt / p.P0, r / cv);
+        const T pres = p.P0 * mm::mpow(pi, cp / r);
+        const T temp = theta * pi;
+        T es, d1, qsat, d2;
+        sat_vp(temp, p, es, d1);
+        sat_q(pres, es, p, qsat, d2);
+        const T RH = qsat > T(1e-10) ? qv / qsat * T(100.0) : T(0.0);
+        const T presv = rho * qv * p.Rv * temp;  // partial pressure of vapour
+        const T presd = pres - presv;
+        cp = p.Cpd * qd + p.Cpl * qt;
+        const T thetae = temp * mm::mpow(presd / p.P0, -p.Rd / cp) * mm::mexp(p.Lv * qv / (cp * temp));
+        const T v[10] = {u, w, theta, qv, qc, qr, pres, temp, thetae, RH};
+        const size_t o = (size_t)k + (size_t)nz * i;
+        for (int f = 0; f < 10; f++) out[(size_t)f * ncell + o] = v[f];
+        v6[0] = w;
+        v6[1] = w;
+        v6[2] = qc;
+        v6[3] = qr;
+        v6[4] = RH;
+        v6[5] = RH;
+    }
+    __shared__ double red[6][HIST_THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int j = 0; j < 6; j++) {
+        double x = v6[j];
+        const bool mn = j == 0 || j == 4;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = mn ? fmin(x, y) : fmax(x, y);
+        }
+        if (lane == 0) red[j][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int j = threadIdx.x;
+        const bool mn = j == 0 || j == 4;
+        double x = red[j][0];
+        for (int q = 1; q < HIST_THREADS / 32; q++) x = mn ? fmin(x, red[j][q]) : fmax(x, red[j][q]);
+        part[(size_t)blockIdx.x * 6 + j] = x;
+    }
+}
+
 // ----------------------------------------------------------------------------- stage epilogue
 
 template <class T>

@@ -54,6 +54,7 @@ struct CtxBase {
     virtual int pass_counts(int* counts, int n) = 0;
     virtual int adjoint_run(int nsteps, int ckpt, const moist_adjoint_seed* seed, moist_adjoint_grad* out) = 0;
     virtual int autotune(int nsteps, std::string& report) = 0;
+    virtual int history(void* const out[MOIST_NDIAG], double summary[6]) = 0;
 };
 
 struct BatchBase {
@@ -929,6 +930,44 @@ struct Ctx : CtxBase {
         return MOIST_OK;
     }
 
+    // ------------------------------------------------------------------ history diagnostics
+    // output_history's primitive variables on the device (k_history_diag); only the requested
+    // fields travel to the host
+    int history(void* const out[MOIST_NDIAG], double summary[6]) override {
+        const size_t ncell = (size_t)nx * nz;
+        const unsigned nb = (unsigned)((ncell + HIST_THREADS - 1) / HIST_THREADS);
+        if (!hist) {
+            AL(hist, (size_t)MOIST_NDIAG * ncell);
+            AL(hist_part, (size_t)nb * 6);
+        }
+        k_history_diag<T><<<nb, HIST_THREADS, 0, st>>>(dp, cur, hist, hist_part);
+        CKL();
+        for (int f = 0; f < MOIST_NDIAG; f++)
+            if (out && out[f])
+                CK(cudaMemcpyAsync(out[f], hist + (size_t)f * ncell, ncell * sizeof(T), cudaMemcpyDeviceToHost, st));
+        std::vector<double> part;
+        if (summary) {
+            part.resize((size_t)nb * 6);
+            CK(cudaMemcpyAsync(part.data(), hist_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
+        CK(cudaStreamSynchronize(st));
+        if (summary) {
+            double r[6] = {1e300, -1e300, -1e300, -1e300, 1e300, -1e300};
+            for (unsigned b = 0; b < nb; b++)
+                for (int j = 0; j < 6; j++) {
+                    const double x = part[(size_t)b * 6 + j];
+                    r[j] = (j == 0 || j == 4) ? std::min(r[j], x) : std::max(r[j], x);
+                }
+            summary[0] = r[0];           // w min (m/s)
+            summary[1] = r[1];           // w max
+            summary[2] = r[2] * 1000.0;  // qc max (g/kg)
+            summary[3] = r[3] * 1000.0;  // qr max (g/kg)
+            summary[4] = r[4];           // RH min (%)
+            summary[5] = r[5];           // RH max
+        }
+        return MOIST_OK;
+    }
+
     // ------------------------------------------------------------------ autotuner
     // Times nsteps large steps for every strip width of the factorisation and substep kernels
     // (1, 2, 4, 8 columns) and every tracer sweep this context can run (tiled, row-streaming),
@@ -1104,6 +1143,8 @@ struct Ctx : CtxBase {
     }
 
     bool seg_tapes = false;
+    T* hist = nullptr;         // history diagnostics, [MOIST_NDIAG][nz * nx]
+    double* hist_part = nullptr;
     std::array<T*, 8> tune_save{};  // the State saved by autotune
     int adj_ckpt = -1;  // checkpoint interval the tape mode was chosen for
 
@@ -2129,6 +2170,12 @@ int moist_batch_adjoint_run(moist_batch* b, int nsteps, int ckpt_every, const mo
     if (!b) return MOIST_ERR_ARG;
     cudaSetDevice(b->device);
     return b->impl->adjoint(nsteps, ckpt_every, seeds, out, nthreads);
+}
+
+int moist_history_diagnostics(moist_ctx* c, void* const out[MOIST_NDIAG], double summary[6]) {
+    if (!c) return MOIST_ERR_ARG;
+    if (cudaSetDevice(c->device) != cudaSuccess) return MOIST_ERR_CUDA;
+    return c->impl->history(out, summary);
 }
 
 int moist_autotune(moist_ctx* c, int nsteps, char* report, size_t report_len) {

@@ -89,6 +89,21 @@ class Model:
     def nan_field(self):
         return lib().moist_nan_field(self.ctx)
 
+    HISTORY_FIELDS = ("u", "w", "theta", "qv", "qc", "qr", "pres", "temp", "thetae", "RH")
+
+    def history(self, fields=HISTORY_FIELDS):
+        """output_history's primitive variables from the device State (moist_history_diagnostics):
+        dict of the requested fields as (Nz, Nx) arrays (z fastest) plus "summary": min w,
+        max w, max qc (g/kg), max qr (g/kg), min RH, max RH."""
+        p = self.p
+        out = {f: np.zeros((p.Nz, p.Nx), dtype=p.T, order="F") for f in fields}
+        arr = (C.c_void_p * abi.MOIST_NDIAG)(*[out[f].ctypes.data if f in out else None
+                                               for f in self.HISTORY_FIELDS])
+        summ = (C.c_double * 6)()
+        _raise(lib().moist_history_diagnostics(self.ctx, arr, summ), self.ctx, "moist_history_diagnostics")
+        out["summary"] = dict(zip(("w_min", "w_max", "qc_max_gkg", "qr_max_gkg", "rh_min", "rh_max"), summ[:]))
+        return out
+
     def autotune(self, nsteps=3):
         """moist_autotune: time every strip width and exact tracer sweep from the current State,
         keep the fastest, restore the State; returns the report (timings and choice)."""

@@ -32,6 +32,7 @@ def lib():
         L = C.CDLL(_SO)
         P, S, V, D, I = C.POINTER(moist_params), C.POINTER(moist_state_host), C.c_void_p, C.c_double, C.c_int
         L.oracle_rk3_step.argtypes = [P, I, I, S, I]
+        L.oracle_history_diag.argtypes = [P, I, S, C.POINTER(V)]
         L.oracle_compute_step.argtypes = [P, I, I, C.POINTER(V), S, S, D, I]
         L.oracle_cloud_microphysics.argtypes = [P, I, S]
         L.oracle_rain_sedimentation.argtypes = [P, I, S, V]
@@ -66,6 +67,20 @@ def budget_terms(s, p):
     out = [np.zeros((p.Nz, p.Nx)) for _ in range(3)] + [np.zeros(p.Nx)]
     _check(lib().oracle_budget_terms(C.byref(cp), p.precision, C.byref(h),
                                      *[o.ctypes.data_as(C.c_void_p) for o in out]))
+    return out
+
+
+HISTORY_FIELDS = ("u", "w", "theta", "qv", "qc", "qr", "pres", "temp", "thetae", "RH")
+
+
+def history_diag(s, p):
+    """output_history's primitive variables (moist.jl:1795-1835): dict of (Nz, Nx) arrays of
+    type T (Fortran order, z fastest)."""
+    cp = p.to_c()
+    h = s.to_c()
+    out = {f: np.zeros((p.Nz, p.Nx), dtype=p.T, order="F") for f in HISTORY_FIELDS}
+    arr = (C.c_void_p * 10)(*[out[f].ctypes.data for f in HISTORY_FIELDS])
+    _check(lib().oracle_history_diag(C.byref(cp), p.precision, C.byref(h), arr))
     return out
 
 

@@ -234,9 +234,57 @@ int budget_terms_t(const moist_params* cp, const moist_state_host* hs, double* m
     return -1;
 }
 
+// output_history's primitive variables (moist.jl:1795-1835): out[f] is a (Nz, Nx) array,
+// z fastest, of u, w, theta, qv, qc, qr, pres, temp, theta_e, RH (the MOIST_DIAG_* order)
+template <class T>
+int history_diag_t(const moist_params* cp, const moist_state_host* hs, void* const* out) {
+    const Par<T> p = Par<T>::from_c(*cp);
+    State<T> s(p);
+    load(s, hs);
+    exchange_halo(s.rho_u.a(), p);  // moist.jl:1798
+    auto rho = s.rho.a(), ru = s.rho_u.a(), rw = s.rho_w.a(), rt = s.rho_theta.a();
+    auto rqv = s.rho_qv.a(), rqc = s.rho_qc.a(), rqr = s.rho_qr.a();
+    T* o[10];
+    for (int f = 0; f < 10; f++) o[f] = (T*)out[f];
+    for (int j = 0; j < p.Nx; j++)
+        for (int k = 0; k < p.Nz; k++) {
+            const int i = p.is + j;
+            const size_t c = (size_t)k + (size_t)p.Nz * j;
+            const T rho_inv = T(1.0) / rho(k, i);
+            const T theta = rt(k, i) * rho_inv;
+            const T qv = rqv(k, i) * rho_inv, qc = rqc(k, i) * rho_inv, qr = rqr(k, i) * rho_inv;
+            const T u = (ru(k, i) + ru(k, i - 1)) * T(0.5) * rho_inv;
+            const T w = k > 0 ? (rw(k, i) + rw(k - 1, i)) * T(0.5) * rho_inv : rw(k, i) * T(0.5) * rho_inv;
+            const T qt = qv + qc + qr;
+            const T qd = T(1.0) - qt;
+            const T r = p.Rd * qd + p.Rv * qv;
+            T cp = p.Cpd * qd + p.Cpv * qv + p.Cpl * (qc + qr);
+            const T cv = cp - r;
+            const T pi = mm::mpow(r * rt(k, i) / p.P0, r / cv);
+            const T pres = p.P0 * mm::mpow(pi, cp / r);
+            const T temp = theta * pi;
+            T es, d1, qsat, d2;
+            saturation_vapor_pressure(temp, p, &es, &d1);
+            saturation_specific_humidity(pres, es, p, &qsat, &d2);
+            const T RH = qsat > T(1e-10) ? qv / qsat * T(100.0) : T(0.0);
+            const T presv = rho(k, i) * qv * p.Rv * temp;
+            const T presd = pres - presv;
+            cp = p.Cpd * qd + p.Cpl * qt;
+            const T thetae = temp * mm::mpow(presd / p.P0, -p.Rd / cp) * mm::mexp(p.Lv * qv / (cp * temp));
+            const T v[10] = {u, w, theta, qv, qc, qr, pres, temp, thetae, RH};
+            for (int f = 0; f < 10; f++) o[f][c] = v[f];
+        }
+    return -1;
+}
+
 }  // namespace
 
 extern "C" {
+
+int oracle_history_diag(const moist_params* cp, int prec, const moist_state_host* s, void* const* out) {
+    if (!params_ok(cp) || !s || !out) return -2;
+    return prec == MOIST_F32 ? history_diag_t<float>(cp, s, out) : history_diag_t<double>(cp, s, out);
+}
 
 int oracle_budget_terms(const moist_params* cp, int prec, const moist_state_host* s, double* mass, double* water,
                         double* energy, double* rain) {
