@@ -181,6 +181,19 @@ struct FSub {
         b_substep_col<T, TT>(a.p, a.a, a.dt_s, a.ns_T, a.fact_tp64, a.err, bx);
     }
 };
+// the same two kernels over column strips (for ensembles too small to fill the GPU with columns)
+template <class T, class TT>
+struct FThomasStrip {
+    __device__ void operator()(const BThomas<T, TT>& a, int bx, int by) const {
+        b_thomas_strip<T, TT>(a.p, a.theta, a.rt2pres, a.dt_s, a.wc, a.ta, a.tb, a.tc, a.tcp, a.tpiv, a.err, bx, by);
+    }
+};
+template <class T, class TT>
+struct FSubStrip {
+    __device__ void operator()(const BSub<T, TT>& a, int bx, int by) const {
+        b_substep_strip<T, TT>(a.p, a.a, a.dt_s, a.ns_T, a.fact_tp64, a.wc, a.err, bx, by);
+    }
+};
 constexpr int BATCH_COL_THREADS = 64;
 template <class T>
 struct FPrep {

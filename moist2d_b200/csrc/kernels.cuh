@@ -966,6 +966,22 @@ __global__ void k_tracer_wavefront(DevParams<T> p, TracerArgs<T> a, const int* e
     }
 }
 
+// ----------------------------------------------------------------------------- state hash
+
+// order-independent hash of the bit patterns of a field: out += sum_j bits(f[j]) * (2 j + 1)
+// (mod 2^64), for checking that two runs produced the same State
+template <class T>
+__global__ void k_hash(const T* __restrict__ f, size_t n, unsigned long long* out) {
+    unsigned long long h = 0;
+    for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (size_t)gridDim.x * blockDim.x) {
+        const unsigned long long b = sizeof(T) == 4 ? (unsigned long long)__float_as_uint((float)f[j])
+                                                    : (unsigned long long)__double_as_longlong((double)f[j]);
+        h += b * (2ull * j + 1ull);
+    }
+    for (int o = 16; o > 0; o >>= 1) h += __shfl_xor_sync(0xffffffffu, h, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, h);
+}
+
 // ----------------------------------------------------------------------------- history output
 
 constexpr int HIST_THREADS = 256;

@@ -930,6 +930,18 @@ struct Ctx : CtxBase {
         return MOIST_OK;
     }
 
+    // hash of the current State's bit patterns (7 fields and prec), queued on the stream
+    unsigned long long* hash_buf = nullptr;
+    int queue_state_hash(unsigned long long* dst_slot) {
+        if (!hash_buf) AL(hash_buf, 64);
+        CK(cudaMemsetAsync(dst_slot, 0, sizeof(unsigned long long), st));
+        const auto cf = cur_fields();
+        for (int f = 0; f < 7; f++) k_hash<T><<<64, 256, 0, st>>>(cf[f], fsz, dst_slot);
+        k_hash<T><<<1, 256, 0, st>>>(prec, (size_t)P, dst_slot);
+        CKL();
+        return MOIST_OK;
+    }
+
     // ------------------------------------------------------------------ history diagnostics
     // output_history's primitive variables on the device (k_history_diag); only the requested
     // fields travel to the host
@@ -987,11 +999,22 @@ struct Ctx : CtxBase {
         if (!save[0]) {  // kept for later calls
             for (int f = 0; f < 7; f++) AL(save[f], fsz);
             AL(save[7], (size_t)P);
+            AL(tune_halo, 2);
         }
+        // the State: prognostic fields, accumulated rain and the two halo values the surface
+        // fluxes carry across steps
+        auto restore = [&]() -> int {
+            const auto dst = cur_fields();
+            if (int r = copyf(save.data(), dst.data(), 7)) return r;
+            CK(cudaMemcpyAsync(prec, save[7], P * sizeof(T), cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(halo_vals, tune_halo, 2 * sizeof(T), cudaMemcpyDeviceToDevice, st));
+            return MOIST_OK;
+        };
         {
             const auto src = cur_fields();
             if (int r = copyf(src.data(), save.data(), 7)) return r;
             CK(cudaMemcpyAsync(save[7], prec, P * sizeof(T), cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(tune_halo, halo_vals, 2 * sizeof(T), cudaMemcpyDeviceToDevice, st));
         }
         struct Cand {
             int wc;
@@ -1011,20 +1034,29 @@ struct Ctx : CtxBase {
         float best = 1e30f;
         Cand bc{wc0, str0 ? 1 : 0};
         char buf[128];
-        for (const Cand& c : cands) {
+        if (!hash_buf) AL(hash_buf, 64);
+        std::vector<unsigned long long> hashes(cands.size());
+        for (size_t ci = 0; ci < cands.size(); ci++) {
+            const Cand& c = cands[ci];
             strip_wc = c.wc;
             strip_smem = strip_smem_bytes<T, TT>(nz, c.wc);
             use_tiles = c.tracer == 0;
             use_stream = c.tracer == 1;
-            const auto dst = cur_fields();
-            if (int r = copyf(save.data(), dst.data(), 7)) return r;
+            if (int rr = restore()) return rr;
             CK(reset_err());
             int r = launch_step();  // warm-up
             CK(cudaEventRecord(e0, st));
             for (int n = 0; n < nsteps && r == MOIST_OK; n++) r = launch_step();
             CK(cudaEventRecord(e1, st));
             if (r != MOIST_OK) return r;
+            if (int rh = queue_state_hash(hash_buf)) return rh;
+            CK(cudaMemcpyAsync(&hashes[ci], hash_buf, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
             CK(cudaEventSynchronize(e1));
+            CK(cudaStreamSynchronize(st));
+            if (hashes[ci] != hashes[0])
+                return set_err(owner, MOIST_ERR_CUDA,
+                               "autotune: strip %d / %s gives another State than the first candidate", c.wc,
+                               c.tracer ? "stream" : "tiles");
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, e0, e1));
             ms /= nsteps;
@@ -1050,11 +1082,7 @@ struct Ctx : CtxBase {
         strip_smem = strip_smem_bytes<T, TT>(nz, strip_wc);
         snprintf(buf, sizeof buf, " -> strip %d, %s (%.3f ms per step)", strip_wc, use_stream ? "stream" : "tiles", best);
         report += buf;
-        {
-            const auto dst = cur_fields();
-            if (int r = copyf(save.data(), dst.data(), 7)) return r;
-            CK(cudaMemcpyAsync(prec, save[7], P * sizeof(T), cudaMemcpyDeviceToDevice, st));
-        }
+        if (int rr = restore()) return rr;
         CK(reset_err());
         return finish();
     }
@@ -1146,6 +1174,7 @@ struct Ctx : CtxBase {
     T* hist = nullptr;         // history diagnostics, [MOIST_NDIAG][nz * nx]
     double* hist_part = nullptr;
     std::array<T*, 8> tune_save{};  // the State saved by autotune
+    T* tune_halo = nullptr;
     int adj_ckpt = -1;  // checkpoint interval the tape mode was chosen for
 
     size_t tape_fields() const {
@@ -1600,7 +1629,9 @@ struct BatchImpl : BatchBase {
     std::vector<Slot> slots[2];
     std::vector<void*> allocs;
     int col_threads = BATCH_COL_THREADS;  // threads per block of the per-column kernels
+    bool sub_strips = false;               // factorisation and substep over column strips instead
     std::vector<std::array<T*, 8>> tune_save;  // the members' States saved by autotune
+    std::vector<T*> tune_halo;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     int parity = 0;
     int** errs = nullptr;  // device: the members' error words
@@ -1656,9 +1687,16 @@ struct BatchImpl : BatchBase {
                 break;
             case BK_THOMAS:
             case BK_SUB:
-                block = dim3(col_threads);
-                for (int i = 0; i < n; i++)
-                    for (unsigned bx = 0; bx < cdiv(m[i]->nx, col_threads); bx++) it.push_back({i, (int)bx, 0});
+                if (sub_strips) {  // column strips of each member's recorded width
+                    block = dim3(STRIP_THREADS);
+                    smem = max_strip_smem;
+                    for (int i = 0; i < n; i++)
+                        for (unsigned bx = 0; bx < cdiv(m[i]->nx, m[i]->strip_wc); bx++) it.push_back({i, (int)bx, 0});
+                } else {
+                    block = dim3(col_threads);
+                    for (int i = 0; i < n; i++)
+                        for (unsigned bx = 0; bx < cdiv(m[i]->nx, col_threads); bx++) it.push_back({i, (int)bx, 0});
+                }
                 break;
             case BK_STREAM: {
                 // the longest sweeps (nx + nz steps) first, so that the short ones fill the tail
@@ -1690,8 +1728,22 @@ struct BatchImpl : BatchBase {
             BATCH_LAUNCH(BK_PHYS, BPhys<T>, FPhys<T>, 3)
             BATCH_LAUNCH(BK_DIAG, BDiag<T>, FDiag<T>, 4)
             BATCH_LAUNCH(BK_TEND, BTend<T>, FTend<T>, 4)
-            BATCH_LAUNCH(BK_THOMAS, SINGLE_ARG(BThomas<T, TT>), SINGLE_ARG(FThomas<T, TT>), 4)
-            BATCH_LAUNCH(BK_SUB, SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSub<T, TT>), 4)
+            case BK_THOMAS:
+                if (sub_strips)
+                    k_batched<BThomas<T, TT>, FThomasStrip<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
+                        s.items, (const BThomas<T, TT>*)s.args, FThomasStrip<T, TT>{});
+                else
+                    k_batched<BThomas<T, TT>, FThomas<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
+                        s.items, (const BThomas<T, TT>*)s.args, FThomas<T, TT>{});
+                break;
+            case BK_SUB:
+                if (sub_strips)
+                    k_batched<BSub<T, TT>, FSubStrip<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
+                        s.items, (const BSub<T, TT>*)s.args, FSubStrip<T, TT>{});
+                else
+                    k_batched<BSub<T, TT>, FSub<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
+                        s.items, (const BSub<T, TT>*)s.args, FSub<T, TT>{});
+                break;
             BATCH_LAUNCH(BK_PREP, BPrep<T>, FPrep<T>, 4)
             BATCH_LAUNCH(BK_STREAM, BStream<T>, FStream<T>, 1)
             BATCH_LAUNCH(BK_UPD, BUpd<T>, FUpd<T>, 4)
@@ -1781,10 +1833,14 @@ struct BatchImpl : BatchBase {
             max_strip_smem = std::max(max_strip_smem, c->strip_smem);
             max_rows = std::max(max_rows, (c->nz + 31) / 32 * 32);
         }
-        BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BThomas<T, TT>), SINGLE_ARG(FThomas<T, TT>), 4>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_strip_smem));
-        BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSub<T, TT>), 4>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_strip_smem));
+        {  // the limit is shared by every batch of the process: allow the device maximum
+            int optin = 0;
+            BCK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, owner->device));
+            BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BThomas<T, TT>), SINGLE_ARG(FThomasStrip<T, TT>), 4>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSubStrip<T, TT>), 4>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+        }
         for (int q = 0; q < 2; q++) {
             std::vector<StepRecord> rec(n);
             for (int i = 0; i < n; i++) {
@@ -1848,9 +1904,11 @@ struct BatchImpl : BatchBase {
         return MOIST_OK;
     }
 
-    // new work lists for the per-column kernels and new graphs
+    // new work lists for the per-column kernels (ct threads per block, or column strips when
+    // ct == 0) and new graphs
     int set_col_threads(int ct) {
-        col_threads = ct;
+        sub_strips = ct == 0;
+        if (ct > 0) col_threads = ct;
         for (int q = 0; q < 2; q++)
             for (Slot& sl : slots[q]) {
                 if (sl.kind != BK_SUB && sl.kind != BK_THOMAS) continue;
@@ -1865,9 +1923,9 @@ struct BatchImpl : BatchBase {
         return capture();
     }
 
-    // Times nsteps batch steps for 32, 64, 128 and 256 threads per block of the per-column
-    // kernels (factorisation and acoustic substep), each from the same saved States, keeps the
-    // fastest and restores the States (same results for every choice).
+    // Times nsteps batch steps for the factorisation and acoustic substep over column strips and
+    // one thread per column with 32, 64, 128 and 256 threads per block, each from the same saved
+    // States, keeps the fastest and restores the States (same results for every choice).
     int autotune(int nsteps, std::string& report) override {
         if (nsteps < 1) return set_berr(owner, MOIST_ERR_ARG, "moist_batch_autotune needs nsteps >= 1");
         if (int r = sync_members()) return r;
@@ -1875,6 +1933,9 @@ struct BatchImpl : BatchBase {
         std::vector<std::array<T*, 8>>& save = tune_save;
         if (save.empty()) {  // kept for later calls
             save.resize(n);
+            tune_halo.resize(n);
+            for (int i = 0; i < n; i++)
+                if (int r = dalloc(&tune_halo[i], 2)) return r;
             for (int i = 0; i < n; i++) {
                 for (int f = 0; f < 7; f++)
                     if (int r = dalloc(&save[i][f], m[i]->fsz)) return r;
@@ -1892,21 +1953,48 @@ struct BatchImpl : BatchBase {
                 T* a = to_save ? save[i][7] : m[i]->prec;
                 const T* b = to_save ? m[i]->prec : save[i][7];
                 BCK(cudaMemcpyAsync(a, b, m[i]->P * sizeof(T), cudaMemcpyDeviceToDevice, st));
+                T* ha = to_save ? tune_halo[i] : m[i]->halo_vals;  // carried by the surface fluxes
+                const T* hb = to_save ? m[i]->halo_vals : tune_halo[i];
+                BCK(cudaMemcpyAsync(ha, hb, 2 * sizeof(T), cudaMemcpyDeviceToDevice, st));
             }
             return MOIST_OK;
         };
         if (int r = copy_all(true)) return r;
         float best = 1e30f;
-        int bct = col_threads;
+        int bct = sub_strips ? 0 : col_threads;
         char buf[96];
-        for (int ct : {32, 64, 128, 256}) {
+        unsigned long long* hb;
+        if (int r = dalloc(&hb, 1)) return r;
+        unsigned long long h0 = 0;
+        bool first = true;
+        for (int ct : {0, 32, 64, 128, 256}) {
             if (int r = set_col_threads(ct)) return r;
             if (int r = copy_all(false)) return r;
             float ms = 0.f;
             if (int r = launch_steps(1)) return r;  // warm-up
             if (int r = time_steps(nsteps, &ms)) return r;
+            // every candidate starts from the same States: their results must agree bit for bit
+            BCK(cudaMemsetAsync(hb, 0, sizeof(unsigned long long), st));
+            for (int i = 0; i < n; i++) {
+                const auto cf = m[i]->cur_fields();
+                for (int f = 0; f < 7; f++) k_hash<T><<<64, 256, 0, st>>>(cf[f], m[i]->fsz, hb);
+                k_hash<T><<<1, 256, 0, st>>>(m[i]->prec, (size_t)m[i]->P, hb);
+            }
+            unsigned long long h = 0;
+            BCK(cudaMemcpyAsync(&h, hb, sizeof h, cudaMemcpyDeviceToHost, st));
+            BCK(cudaStreamSynchronize(st));
+            if (first) {
+                h0 = h;
+                first = false;
+            } else if (h != h0) {
+                return set_berr(owner, MOIST_ERR_CUDA, "autotune: column block %d gives other States than column strips",
+                                ct);
+            }
             ms /= nsteps;
-            snprintf(buf, sizeof buf, "%scolumn block %d: %.2f ms", report.empty() ? "" : "; ", ct, ms);
+            if (ct == 0)
+                snprintf(buf, sizeof buf, "%scolumn strips: %.2f ms", report.empty() ? "" : "; ", ms);
+            else
+                snprintf(buf, sizeof buf, "%scolumn block %d: %.2f ms", report.empty() ? "" : "; ", ct, ms);
             report += buf;
             if (ms < best) {
                 best = ms;
@@ -1916,7 +2004,10 @@ struct BatchImpl : BatchBase {
         if (int r = set_col_threads(bct)) return r;
         if (int r = copy_all(false)) return r;
         BCK(cudaStreamSynchronize(st));
-        snprintf(buf, sizeof buf, " -> column block %d (%.2f ms per step)", bct, best);
+        if (bct == 0)
+            snprintf(buf, sizeof buf, " -> column strips (%.2f ms per step)", best);
+        else
+            snprintf(buf, sizeof buf, " -> column block %d (%.2f ms per step)", bct, best);
         report += buf;
         return MOIST_OK;
     }
