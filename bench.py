@@ -71,6 +71,22 @@ def make_workload(name, T):
     return p, s, desc
 
 
+def max_over_ranks(x, world, device="cuda"):
+    """The largest x over the ranks: a replicated job takes as long as its slowest rank."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(cells, world, seconds):
+    """Whole-job cell-steps/s of `world` replicas of `cells` cells, one step per `seconds`."""
+    return cells * world / seconds
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -371,14 +387,8 @@ def main():
         dist.barrier()
     clk = clocks.stop()
 
-    t_local = step_ms / args.steps
-    if world > 1:
-        t = torch.tensor([t_local], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    else:
-        t_max = t_local
-    value = cells * world / (t_max / 1e3)
+    t_max = max_over_ranks(step_ms / args.steps, world)
+    value = job_throughput(cells, world, t_max / 1e3)
 
     # end to end: rk3_step!(s, p) on a page-locked host State, every step
     e2e = None
@@ -405,12 +415,8 @@ def main():
         t0 = time.perf_counter()
         for _ in range(ne2e):
             _raise(L.moist_rk3_step_host(m.ctx, C.byref(h), 1), m.ctx, "e2e step")
-        te = (time.perf_counter() - t0) / ne2e
-        if world > 1:
-            tt = torch.tensor([te], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
-        e2e = {"value": cells * world / te, "unit": "cell-steps/s", "h2d_bytes_per_step": nbytes,
+        te = max_over_ranks((time.perf_counter() - t0) / ne2e, world)
+        e2e = {"value": job_throughput(cells, world, te), "unit": "cell-steps/s", "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "ms_per_step": te * 1e3,
                "how": "moist_rk3_step_host: H2D of the 7 prognostic fields + prec from page-locked "
                       "memory, one rk3 step, D2H of the same, wall clock per call"}
