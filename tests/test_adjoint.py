@@ -204,3 +204,16 @@ def test_adjoint_single_bubble_short():
     seeds = state_seeds(p, s, 9)
     g, _ = run_adjoint(p, s, 3, 2, prec_w, seeds)
     fd_check(p, s, 3, prec_w, seeds, g, ndir=2, seed=21)
+
+
+@pytest.mark.parametrize("nx,nz", [(2, 2), (3, 5), (5, 3)])
+def test_adjoint_tiny_shapes(nx, nz):
+    """Shapes where the periodic wraps alias (i-2 = i+1 for nx = 3, all reads one column for
+    nx = 2), the linear-index clamp reads column 0, and the w-p system has one unknown."""
+    from states import small_case
+    p, s = small_case(np.float64, nx, nz, do_sf=False, do_rd=False)
+    prec_w = rain_weight(p)
+    seeds = state_seeds(p, s, 13)
+    g, _ = run_adjoint(p, s, 2, 1, prec_w, seeds)
+    assert np.isclose(g["objective"], oracle_J(p, s, 2, prec_w, seeds), rtol=1e-13, atol=0.0)
+    fd_check(p, s, 2, prec_w, seeds, g, ndir=3, seed=nx * 10 + nz, h=1e-7)
