@@ -1630,6 +1630,7 @@ struct BatchImpl : BatchBase {
     std::vector<void*> allocs;
     int col_threads = BATCH_COL_THREADS;  // threads per block of the per-column kernels
     bool sub_strips = false;               // factorisation and substep over column strips instead
+    int stream_minb = 1;                   // register bound of the streaming tracer sweep (1 or 2)
     std::vector<std::array<T*, 8>> tune_save;  // the members' States saved by autotune
     std::vector<T*> tune_halo;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
@@ -1745,7 +1746,14 @@ struct BatchImpl : BatchBase {
                         s.items, (const BSub<T, TT>*)s.args, FSub<T, TT>{});
                 break;
             BATCH_LAUNCH(BK_PREP, BPrep<T>, FPrep<T>, 4)
-            BATCH_LAUNCH(BK_STREAM, BStream<T>, FStream<T>, 1)
+            case BK_STREAM:
+                if (stream_minb == 2)  // registers bounded so that twice the blocks fit on an SM
+                    k_batched<BStream<T>, FStream<T>, 2><<<s.nitems, s.block, s.smem, st>>>(
+                        s.items, (const BStream<T>*)s.args, FStream<T>{});
+                else
+                    k_batched<BStream<T>, FStream<T>, 1><<<s.nitems, s.block, s.smem, st>>>(
+                        s.items, (const BStream<T>*)s.args, FStream<T>{});
+                break;
             BATCH_LAUNCH(BK_UPD, BUpd<T>, FUpd<T>, 4)
             BATCH_LAUNCH(BK_STAGE_END, BStageEnd, FStageEnd, 1)
             BATCH_LAUNCH(BK_PREC, BPrec<T>, FPrec<T>, 1)
@@ -2001,13 +2009,44 @@ struct BatchImpl : BatchBase {
                 bct = ct;
             }
         }
+        // then, with that form, the register bound of the streaming tracer sweep
+        int bmb = stream_minb;
+        float best_mb = 1e30f;
+        for (int mb : {1, 2}) {
+            stream_minb = mb;
+            if (int r = set_col_threads(bct)) return r;  // recaptures the graphs
+            if (int r = copy_all(false)) return r;
+            float ms = 0.f;
+            if (int r = launch_steps(1)) return r;
+            if (int r = time_steps(nsteps, &ms)) return r;
+            BCK(cudaMemsetAsync(hb, 0, sizeof(unsigned long long), st));
+            for (int i = 0; i < n; i++) {
+                const auto cf = m[i]->cur_fields();
+                for (int f = 0; f < 7; f++) k_hash<T><<<64, 256, 0, st>>>(cf[f], m[i]->fsz, hb);
+                k_hash<T><<<1, 256, 0, st>>>(m[i]->prec, (size_t)m[i]->P, hb);
+            }
+            unsigned long long h = 0;
+            BCK(cudaMemcpyAsync(&h, hb, sizeof h, cudaMemcpyDeviceToHost, st));
+            BCK(cudaStreamSynchronize(st));
+            if (h != h0)
+                return set_berr(owner, MOIST_ERR_CUDA, "autotune: tracer register bound %d gives other States", mb);
+            ms /= nsteps;
+            snprintf(buf, sizeof buf, "; tracer bound %d: %.2f ms", mb, ms);
+            report += buf;
+            if (ms < best_mb) {
+                best_mb = ms;
+                bmb = mb;
+            }
+        }
+        best = best_mb;
+        stream_minb = bmb;
         if (int r = set_col_threads(bct)) return r;
         if (int r = copy_all(false)) return r;
         BCK(cudaStreamSynchronize(st));
         if (bct == 0)
-            snprintf(buf, sizeof buf, " -> column strips (%.2f ms per step)", best);
+            snprintf(buf, sizeof buf, " -> column strips, tracer bound %d (%.2f ms per step)", bmb, best);
         else
-            snprintf(buf, sizeof buf, " -> column block %d (%.2f ms per step)", bct, best);
+            snprintf(buf, sizeof buf, " -> column block %d, tracer bound %d (%.2f ms per step)", bct, bmb, best);
         report += buf;
         return MOIST_OK;
     }
