@@ -10,6 +10,7 @@
  *   implicit_correction!(rho_w, drho_w, theta, rt2pres, dt, p)
  *                                                    moist.jl:974-1030   -> moist_implicit_correction
  *   device(x)  (the CuArray hook)                    moist.jl:227-228    -> moist_ctx_create + moist_upload_state
+ *   output_history(...) field computation            moist.jl:1795-1843  -> moist_history_diagnostics
  * A Julia caller binds them with ccall; Python binds them with ctypes
  * (moist2d_b200/_lib.py).
  *
