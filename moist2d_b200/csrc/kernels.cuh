@@ -476,11 +476,7 @@ __device__ __forceinline__ void b_thomas_col(DevParams<T> p, const T* theta, con
         th_cur = th_next;
     }
 }
-template <class T, class TT>
-__global__ void k_thomas_factors(DevParams<T> p, const T* theta, const T* rt2pres, T dt_s, T* ta, T* tb,
-                                 T* tc, TT* tcp, TT* tpiv, const int* err) {
-    b_thomas_col(p, theta, rt2pres, dt_s, ta, tb, tc, tcp, tpiv, err, blockIdx.x);
-}
+
 
 template <class T, class TT>
 struct SubArgs {
@@ -493,7 +489,8 @@ struct SubArgs {
     TT* dprime;                       // scratch [nz][P]
 };
 
-// One acoustic substep (moist.jl:1355-1459), one thread per column i: horizontal forward
+// One acoustic substep (moist.jl:1355-1459), one thread per column i (the ensembles' form):
+// horizontal forward
 // step of rho_u_p at faces i-1/2 (recomputed, bitwise equal to column i-1's) and i+1/2,
 // explicit rho_p / rho_theta_p, off-centred right-hand side, Thomas sweep for rho_w_p,
 // vertical rho_p / rho_theta_p updates, time-averaged momentum fluxes.
@@ -611,11 +608,7 @@ __device__ __forceinline__ void b_substep_col(DevParams<T> p, SubArgs<T, TT> a, 
         if (k < ke) a.mfz[c] = a.mfz[c] + a.rw_p[c] / ns_T;
     }
 }
-template <class T, class TT>
-__global__ void k_substep(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T, double fact_tp64,
-                          const int* err) {
-    b_substep_col(p, a, dt_s, ns_T, fact_tp64, err, blockIdx.x);
-}
+
 
 // ----------------------------------------------------------------------------- column strips
 //
@@ -623,9 +616,11 @@ __global__ void k_substep(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T, doub
 // STRIP_THREADS threads owns wc adjacent columns (wc = 1, 2, 4 or 8) over all levels: the work
 // that is independent per cell runs over all cells of the strip in parallel with coalesced
 // loads, and only the Thomas recurrences run one thread per column, out of shared memory. The
-// per-column kernels above put every load of a column on the recurrence's critical path; here
-// a substep costs about one recurrence of FP64 latencies. Each value goes through the same
-// operations as in k_thomas_factors / k_substep, so the results agree bit for bit.
+// per-column bodies above put every load of a column on the recurrence's critical path, which
+// a single domain's few columns cannot hide; here a substep costs about one recurrence of FP64
+// latencies. Ensembles, whose many columns do hide it, use the per-column bodies (or these,
+// as their autotuner finds). Each value goes through the same operations in both forms, so
+// the results agree bit for bit.
 
 constexpr int STRIP_THREADS = 256;
 
@@ -655,7 +650,7 @@ struct StripSmem {
     }
 };
 
-// k_thomas_factors over a strip: the coefficients of all rows in parallel, then the pivot
+// b_thomas_col over a strip: the coefficients of all rows in parallel, then the pivot
 // recurrence per column
 template <class T, class TT>
 __device__ __forceinline__ void b_thomas_strip(DevParams<T> p, const T* theta, const T* rt2pres, T dt_s, int wc,
@@ -721,7 +716,7 @@ __global__ void __launch_bounds__(STRIP_THREADS) k_thomas_strip(DevParams<T> p, 
     b_thomas_strip(p, theta, rt2pres, dt_s, wc, ta, tb, tc, tcp, tpiv, err, blockIdx.x, blockIdx.y);
 }
 
-// k_substep over a strip (moist.jl:1355-1459)
+// b_substep_col over a strip (moist.jl:1355-1459)
 template <class T, class TT>
 __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T, double fact_tp64,
                                                 int wc, const int* err, int bx, int by) {
