@@ -156,6 +156,17 @@ MM_HD Dual<N> mpow(const Dual<N>& x, double y) {
     return mpow(x, Dual<N>(y));
 }
 
+// x^4 (gray radiation): d(x^4) = 4 x^3 dx
+template <int N>
+MM_HD Dual<N> mpow4(const Dual<N>& x) {
+    Dual<N> r;
+    r.v = mpow4(x.v);
+    const double g = 4.0 * x.v * x.v * x.v;
+#pragma unroll
+    for (int j = 0; j < N; j++) r.d[j] = g * x.d[j];
+    return r;
+}
+
 template <int N>
 MM_HD Dual<N> msqrt(const Dual<N>& x) {
     Dual<N> r;
@@ -167,9 +178,12 @@ MM_HD Dual<N> msqrt(const Dual<N>& x) {
     return r;
 }
 
+// |x| with the value of fabs (+0 for -0, which the sign-bit selects of jmin/jmax can see)
 template <int N>
 MM_HD Dual<N> mabs(const Dual<N>& x) {
-    return x.v < 0.0 ? -x : x;
+    Dual<N> r = x.v < 0.0 ? -x : x;
+    r.v = fabs(x.v);
+    return r;
 }
 
 }  // namespace mm

@@ -43,6 +43,8 @@ def lib():
         L.oracle_solve_tridiagonal.argtypes = [I, I, V, V, V, V]
         L.oracle_invert_T_for_thetae.argtypes = [P, I, D, D, D, C.POINTER(D)]
         L.oracle_budget_terms.argtypes = [P, I, S, V, V, V, V]
+        L.oracle_tangent_run.argtypes = [P, S, C.POINTER(V), V, D, D, I, V, C.POINTER(V), C.POINTER(D),
+                                         C.POINTER(D)]
         for f in ("oracle_exp_d", "oracle_log_d"):
             getattr(L, f).argtypes = [D]
             getattr(L, f).restype = D
@@ -82,6 +84,40 @@ def history_diag(s, p):
     arr = (C.c_void_p * 10)(*[out[f].ctypes.data for f in HISTORY_FIELDS])
     _check(lib().oracle_history_diag(C.byref(cp), p.precision, C.byref(h), arr))
     return out
+
+
+PROGNOSTIC = ("rho", "rho_u", "rho_w", "rho_theta", "rho_qv", "rho_qc", "rho_qr")
+
+
+def tangent(p, s, nsteps, direction=None, dir_prec=None, d_k_auto=0.0, d_qc_threshold=0.0,
+            prec_weight=None, state_weight=None):
+    """Forward-mode derivative of nsteps Float64 large steps (oracle_tangent.cpp): returns
+    (J, dJ) for J = sum(prec_weight * prec_final) + sum_f sum(state_weight[f] * S_final.f) and its
+    derivative in the direction (direction[f] for the prognostic fields, dir_prec,
+    d_k_auto, d_qc_threshold). s is not modified."""
+    if p.T is not np.float64:
+        raise ValueError("oracle.tangent: Float64 Params and State only")
+    keep = []
+
+    def arr(x, shape):
+        if x is None:
+            return None
+        a = np.asfortranarray(np.broadcast_to(np.asarray(x, dtype=np.float64), shape))
+        keep.append(a)
+        return a.ctypes.data
+
+    f2 = (p.ka, p.ia)
+    direction = direction or {}
+    state_weight = state_weight or {}
+    dirs = (C.c_void_p * 7)(*[arr(direction.get(f), f2) for f in PROGNOSTIC])
+    wts = (C.c_void_p * 7)(*[arr(state_weight.get(f), f2) for f in PROGNOSTIC])
+    cp = p.to_c()
+    h = s.to_c()
+    J, dJ = C.c_double(), C.c_double()
+    _check(lib().oracle_tangent_run(C.byref(cp), C.byref(h), dirs, arr(dir_prec, (p.ia,)), float(d_k_auto),
+                                    float(d_qc_threshold), int(nsteps), arr(prec_weight, (p.ia,)), wts,
+                                    C.byref(J), C.byref(dJ)))
+    return J.value, dJ.value
 
 
 def rk3_step(s, p, nsteps=1, tri64=False):

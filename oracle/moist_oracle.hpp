@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "../include/moist2d.h"
@@ -46,6 +47,23 @@ namespace oracle {
 
 using mm::jmax;
 using mm::jmin;
+
+// Wide<T>: the Float64 in which the reference evaluates the off-centring factor even in Float32
+// runs (moist.jl:1375). A derivative type (oracle_tangent.cpp instantiates the step with
+// mm::Dual) is its own wide type, so that its derivative part is carried through.
+template <class T>
+using Wide = typename std::conditional<std::is_floating_point<T>::value, double, T>::type;
+
+// Grid vectors arrive in the context precision; a derivative type reads them as Float64 values.
+template <class T>
+void grid_assign(std::vector<T>& v, const void* src, int n) {
+    if (std::is_floating_point<T>::value) {
+        v.assign((const T*)src, (const T*)src + n);
+    } else {
+        const double* d = (const double*)src;
+        v.assign(d, d + n);
+    }
+}
 
 template <class T>
 struct Par {
@@ -120,9 +138,9 @@ struct Par {
         p.A_SAT = (T)c.a_sat;
         p.B_SAT = (T)c.b_sat;
         p.EPS = (T)c.eps;
-        p.zf.assign((const T*)c.zf, (const T*)c.zf + c.nz);
-        p.dz.assign((const T*)c.dz, (const T*)c.dz + c.nz);
-        p.z.assign((const T*)c.z, (const T*)c.z + c.nz);
+        grid_assign(p.zf, c.zf, c.nz);
+        grid_assign(p.dz, c.dz, c.nz);
+        grid_assign(p.z, c.z, c.nz);
         return p;
     }
 };
@@ -917,20 +935,21 @@ int compute_step(A2<T> d_rho_phys, A2<T> d_rho_u_phys, A2<T> d_rho_theta_phys, A
         exchange_halo(rho_u_p, p);
         rho_theta_p_old_f.v = rho_theta_p_f.v;
         // Float64 factor even in Float32 runs: T(0.5) * (1.0 + beta) (moist.jl:1375)
-        const double fact_tp = (double)T(0.5) * (1.0 + (double)p.beta_offcenter);
+        using W = Wide<T>;
+        const W fact_tp = W(T(0.5)) * (W(1.0) + W(p.beta_offcenter));
         OMP_FOR
         for (int i = is; i <= ie; i++) {
             std::vector<T> rho_p_tp(ka), rho_theta_p_tp(ka), drho_w_p(ka, T(0));
             for (int k = ks; k <= ke; k++) {
                 T advection = -(rho_u_p(k, i) - rho_u_p(k, i - 1)) / dx;
                 T inc = dt_s * (R_rho(k, i) + advection);
-                rho_p_tp[k] = (T)((double)rho_p(k, i) + fact_tp * (double)inc);
+                rho_p_tp[k] = (T)(W(rho_p(k, i)) + fact_tp * W(inc));
                 rho_p(k, i) += inc;
                 const T flux_ip = (theta(k, i + 1) + theta(k, i)) * T(0.5) * rho_u_p(k, i);
                 const T flux_im = (theta(k, i) + theta(k, i - 1)) * T(0.5) * rho_u_p(k, i - 1);
                 advection = -(flux_ip - flux_im) / dx;
                 inc = dt_s * (R_rho_theta(k, i) + advection);
-                rho_theta_p_tp[k] = (T)((double)rho_theta_p(k, i) + fact_tp * (double)inc);
+                rho_theta_p_tp[k] = (T)(W(rho_theta_p(k, i)) + fact_tp * W(inc));
                 rho_theta_p(k, i) += inc;
             }
             for (int k = ks; k <= ke - 1; k++) {

@@ -9,7 +9,12 @@ seeded random directions v in the seven prognostic fields and in K_auto and Qc_t
 The step is piecewise smooth (upwind and limiter switches, Kessler clamps), so the directions
 are scaled to stay well inside the pieces: h = 1e-6 relative to each field's magnitude (1e-4
 for the two parameters, whose effect on J is small enough that a smaller step loses digits to
-rounding)."""
+rounding).
+
+The same gradients are also compared with the exact directional derivative of the oracle's
+Float64 step computed in forward mode with dual numbers (bind.tangent, oracle_tangent.cpp: the
+ForwardDiff-style derivative of the restated step), where no truncation error hides a
+discrepancy."""
 import numpy as np
 import pytest
 
@@ -217,3 +222,56 @@ def test_adjoint_tiny_shapes(nx, nz):
     g, _ = run_adjoint(p, s, 2, 1, prec_w, seeds)
     assert np.isclose(g["objective"], oracle_J(p, s, 2, prec_w, seeds), rtol=1e-13, atol=0.0)
     fd_check(p, s, 2, prec_w, seeds, g, ndir=3, seed=nx * 10 + nz, h=1e-7)
+
+
+def tangent_check(p, s, nsteps, prec_w, seeds, g, ndir, seed, rtol=1e-12):
+    """<grad, v> against the exact directional derivative of the oracle's Float64 step (forward
+    mode, dual numbers: oracle_tangent.cpp), in seeded state directions and in the two
+    parameters. No truncation error on either side, so the tolerance is rounding only; the
+    state error is taken relative to sum |grad * v| (the size of the terms that cancel)."""
+    rng = np.random.default_rng(seed)
+    worst = 0.0
+    for _ in range(ndir):
+        v = direction(p, s, rng)
+        ad = sum(float(np.sum(g[f] * v[f])) for f in FIELDS)
+        scale = sum(float(np.sum(np.abs(g[f] * v[f]))) for f in FIELDS)
+        J, dJ = bind.tangent(p, s, nsteps, direction=v, prec_weight=prec_w, state_weight=seeds)
+        assert np.isclose(J, g["objective"], rtol=1e-13, atol=0.0)
+        assert scale > 0.0
+        err = abs(ad - dJ) / scale
+        worst = max(worst, err)
+        assert err <= rtol, "adjoint %.15e vs forward mode %.15e (rel %.2e)" % (ad, dJ, err)
+    for key, kw in (("k_auto", "d_k_auto"), ("qc_threshold", "d_qc_threshold")):
+        _, dJ = bind.tangent(p, s, nsteps, prec_weight=prec_w, state_weight=seeds, **{kw: 1.0})
+        err = abs(g[key] - dJ) / max(abs(dJ), 1e-300)
+        worst = max(worst, err)
+        assert err <= rtol, "%s: adjoint %.15e vs forward mode %.15e (rel %.2e)" % (key, g[key], dJ, err)
+    return worst
+
+
+@pytest.mark.parametrize("nsteps", [1, 4, 20])
+def test_adjoint_matches_forward_mode_oracle(nsteps):
+    p, s = bubble_case(np.float64, nx=24, nz=16)
+    prec_w = rain_weight(p)
+    seeds = state_seeds(p, s, 11)
+    g, _ = run_adjoint(p, s, nsteps, 3, prec_w, seeds)
+    tangent_check(p, s, nsteps, prec_w, seeds, g, ndir=4, seed=100 + nsteps)
+
+
+def test_adjoint_matches_forward_mode_oracle_single_bubble():
+    """The adjoint workload's domain (512 x 96), rain objective plus a state seed, 10 steps."""
+    p, s = single_bubble(np.float64)
+    prec_w = rain_weight(p)
+    seeds = state_seeds(p, s, 9)
+    g, _ = run_adjoint(p, s, 10, 5, prec_w, seeds)
+    tangent_check(p, s, 10, prec_w, seeds, g, ndir=2, seed=7)
+
+
+@pytest.mark.parametrize("nx,nz", [(2, 2), (3, 5), (5, 3)])
+def test_adjoint_tiny_shapes_forward_mode(nx, nz):
+    from states import small_case
+    p, s = small_case(np.float64, nx, nz, do_sf=False, do_rd=False)
+    prec_w = rain_weight(p)
+    seeds = state_seeds(p, s, 13)
+    g, _ = run_adjoint(p, s, 3, 2, prec_w, seeds)
+    tangent_check(p, s, 3, prec_w, seeds, g, ndir=3, seed=nx * 10 + nz)
