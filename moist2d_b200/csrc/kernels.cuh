@@ -26,6 +26,14 @@ __device__ __forceinline__ bool halted(const int* err) { return *(volatile const
 
 #define MOIST_IDX(k, i) ((size_t)(k) * P + (i))
 
+// Load of an input that no thread writes during the launch (it was produced by an earlier
+// launch): the read-only data path, which also lets the compiler issue the load ahead of the
+// launch's stores to other arrays, so a column walk keeps several levels' loads in flight.
+template <class X>
+__device__ __forceinline__ X ro(const X* q) {
+    return __ldg(q);
+}
+
 // ----------------------------------------------------------------------------- physics
 
 // surface_fluxes! (moist.jl:714-751), one thread per column. ru_left / rho_right are the
@@ -448,12 +456,12 @@ __device__ __forceinline__ void b_thomas_col(DevParams<T> p, const T* theta, con
     const int ke = nz - 1, n = nz - 1;
     const T fact_tp = T(0.5) * (T(1.0) + p.beta);
     const T dt_tp2 = (dt_s * fact_tp) * (dt_s * fact_tp);
-    T th_prev = T(0), th_cur = f2h(theta[MOIST_IDX(0, i)], theta[MOIST_IDX(1, i)], dz[0], dz[1]);
+    T th_prev = T(0), th_cur = f2h(ro(theta + MOIST_IDX(0, i)), ro(theta + MOIST_IDX(1, i)), dz[0], dz[1]);
     TT cp_prev = TT(0);
     for (int j = 0; j < n; j++) {
         const int k = j;
-        const T th_next = (k + 1 <= ke - 1) ? f2h(theta[MOIST_IDX(k + 1, i)], theta[MOIST_IDX(k + 2, i)], dz[k + 1], dz[k + 2]) : T(0);
-        const T r_k = rt2pres[MOIST_IDX(k, i)], r_kp = rt2pres[MOIST_IDX(k + 1, i)];
+        const T th_next = (k + 1 <= ke - 1) ? f2h(ro(theta + MOIST_IDX(k + 1, i)), ro(theta + MOIST_IDX(k + 2, i)), dz[k + 1], dz[k + 2]) : T(0);
+        const T r_k = ro(rt2pres + MOIST_IDX(k, i)), r_kp = ro(rt2pres + MOIST_IDX(k + 1, i));
         const T b = dt_tp2 * (r_k / dz[k] + r_kp / dz[k + 1]) * th_cur / (z[k + 1] - z[k]);
         const T a = (k > 0) ? -dt_tp2 * (r_k * th_prev / ((z[k + 1] - z[k]) * dz[k]) - p.GRAV / (dz[k] + dz[k + 1])) : T(0);
         const T c = (k < ke - 1) ? -dt_tp2 * (r_kp * th_next / ((z[k + 1] - z[k]) * dz[k + 1]) + p.GRAV / (dz[k] + dz[k + 1])) : T(0);
@@ -492,8 +500,11 @@ struct SubArgs {
 // One acoustic substep (moist.jl:1355-1459), one thread per column i (the ensembles' form):
 // horizontal forward
 // step of rho_u_p at faces i-1/2 (recomputed, bitwise equal to column i-1's) and i+1/2,
-// explicit rho_p / rho_theta_p, off-centred right-hand side, Thomas sweep for rho_w_p,
-// vertical rho_p / rho_theta_p updates, time-averaged momentum fluxes.
+// explicit rho_p / rho_theta_p, off-centred right-hand side and elimination going up the
+// column; back substitution for rho_w_p fused with the vertical rho_p / rho_theta_p updates
+// and the time-averaged momentum fluxes going down. The inputs no thread of the launch writes
+// (tendencies, theta, rt2pres, s.rho_w, the substep-start rho_u_p / rho_theta_p buffers, the
+// stage factors) are read through ro().
 template <class T, class TT>
 __device__ __forceinline__ void b_substep_col(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T, double fact_tp64,
                                               const int* err, int bx) {
@@ -511,11 +522,11 @@ __device__ __forceinline__ void b_substep_col(DevParams<T> p, SubArgs<T, TT> a, 
     auto u_update = [&](int k, int cc) {
         const int cn = wrapx(cc + 1, nx);
         const size_t a0 = MOIST_IDX(k, cc), a1 = MOIST_IDX(k, cn);
-        T grad_x = (a.rt_in[a1] - a.rt_in[a0]) / dx;
-        const T grad_x_old = (a.rt_old[a1] - a.rt_old[a0]) / dx;
+        T grad_x = (ro(a.rt_in + a1) - ro(a.rt_in + a0)) / dx;
+        const T grad_x_old = (ro(a.rt_old + a1) - ro(a.rt_old + a0)) / dx;
         grad_x = grad_x + p.gamma_d * (grad_x - grad_x_old);
-        const T rt2pres_h = (a.rt2pres[a0] + a.rt2pres[a1]) * T(0.5);
-        return a.ru_in[a0] + dt_s * (a.R_ru[a0] - rt2pres_h * grad_x);
+        const T rt2pres_h = (ro(a.rt2pres + a0) + ro(a.rt2pres + a1)) * T(0.5);
+        return ro(a.ru_in + a0) + dt_s * (ro(a.R_ru + a0) - rt2pres_h * grad_x);
     };
     T rho_tp_prev = T(0), rt_tp_prev = T(0);
     TT dprev = TT(0);
@@ -526,15 +537,15 @@ __device__ __forceinline__ void b_substep_col(DevParams<T> p, SubArgs<T, TT> a, 
         a.ru_out[c] = u_p;
         a.mfx[c] = a.mfx[c] + u_p / ns_T;
         T advection = -(u_p - u_m) / dx;
-        T inc = dt_s * (a.R_rho[c] + advection);
+        T inc = dt_s * (ro(a.R_rho + c) + advection);
         const T rho_tp = (T)((double)a.rho_p[c] + fact_tp64 * (double)inc);
         a.rho_p[c] = a.rho_p[c] + inc;
-        const T th_i = a.theta[c], th_ip = a.theta[MOIST_IDX(k, ip)], th_im = a.theta[MOIST_IDX(k, im)];
+        const T th_i = ro(a.theta + c), th_ip = ro(a.theta + MOIST_IDX(k, ip)), th_im = ro(a.theta + MOIST_IDX(k, im));
         const T flux_ip = (th_ip + th_i) * T(0.5) * u_p;
         const T flux_im = (th_i + th_im) * T(0.5) * u_m;
         advection = -(flux_ip - flux_im) / dx;
-        inc = dt_s * (a.R_rt[c] + advection);
-        const T rtp = a.rt_in[c];
+        inc = dt_s * (ro(a.R_rt + c) + advection);
+        const T rtp = ro(a.rt_in + c);
         const T rt_tp = (T)((double)rtp + fact_tp64 * (double)inc);
         a.rt_out[c] = rtp + inc;
         if (k >= 1) {
@@ -542,40 +553,35 @@ __device__ __forceinline__ void b_substep_col(DevParams<T> p, SubArgs<T, TT> a, 
             const size_t cj = c - P;
             const T buoyancy = (rt_tp - rt_tp_prev) / (z[k] - z[j]);
             const T grav = -p.GRAV * T(0.5) * (rho_tp + rho_tp_prev);
-            const T rt2pres_h = (a.rt2pres[cj] + a.rt2pres[c]) * T(0.5);
-            const T drho_w = dt_s * (a.R_rw[cj] - rt2pres_h * buoyancy + grav);
+            const T rt2pres_h = (ro(a.rt2pres + cj) + ro(a.rt2pres + c)) * T(0.5);
+            const T drho_w = dt_s * (ro(a.R_rw + cj) - rt2pres_h * buoyancy + grav);
             const T w_j = a.rw_p[cj];
+            const T aj = ro(a.ta + cj);
             T d = w_j + drho_w;
-            if (j > 0) d -= a.ta[cj] * fact * w_j;
-            d -= a.tb[cj] * fact * w_j;
-            if (j < n - 1) d -= a.tc[cj] * fact * a.rw_p[c];
+            if (j > 0) d -= aj * fact * w_j;
+            d -= ro(a.tb + cj) * fact * w_j;
+            if (j < n - 1) d -= ro(a.tc + cj) * fact * a.rw_p[c];
             TT dp;
             if (j == 0)
-                dp = (TT)d / a.tpiv[cj];
+                dp = (TT)d / ro(a.tpiv + cj);
             else
-                dp = ((TT)d - (TT)a.ta[cj] * dprev) / a.tpiv[cj];
+                dp = ((TT)d - (TT)aj * dprev) / ro(a.tpiv + cj);
             a.dprime[cj] = dp;
             dprev = dp;
         }
         rho_tp_prev = rho_tp;
         rt_tp_prev = rt_tp;
     }
-    // back substitution (moist.jl:968-970)
-    {
-        TT x = dprev;
-        a.rw_p[MOIST_IDX(n - 1, i)] = (T)x;
-        for (int j = n - 2; j >= 0; j--) {
-            x = a.dprime[MOIST_IDX(j, i)] - a.tcp[MOIST_IDX(j, i)] * x;
-            a.rw_p[MOIST_IDX(j, i)] = (T)x;
-        }
-    }
-    // vertical rho_p, rho_theta_p updates (1412-1446) and momentum flux averages (1452-1458)
+    // Back substitution (moist.jl:968-970) going down, fused with the vertical rho_p /
+    // rho_theta_p updates (1412-1446) and the momentum flux average (1452-1458) of cell j + 1,
+    // whose two face values rho_w_p[j + 1] (w_hi) and rho_w_p[j] are known once x_j is: every
+    // cell's arithmetic is that of separate passes.
     const T* th = a.theta;
-    for (int k = 0; k < nz; k++) {
+    auto vertical = [&](int k, T w_k, T w_km) {
         const size_t c = MOIST_IDX(k, i);
         {
-            const T flux_kp = k == ke ? T(0.0) : a.rw_p[c];
-            const T flux_km = k == 0 ? T(0.0) : a.rw_p[c - P];
+            const T flux_kp = k == ke ? T(0.0) : w_k;
+            const T flux_km = k == 0 ? T(0.0) : w_km;
             const T advection = -(flux_kp - flux_km) / dz[k];
             a.rho_p[c] = a.rho_p[c] + dt_s * advection;
         }
@@ -583,30 +589,42 @@ __device__ __forceinline__ void b_substep_col(DevParams<T> p, SubArgs<T, TT> a, 
         if (k == ke) {
             flux_kp = T(0.0);
         } else {
-            const T wp = a.rw_p[c];
+            const T wp = w_k;
             if (wp > EPS && k > 0)
-                flux_kp = up3(wp, th[c - P], th[c], th[c + P]);
-            else if (a.s_rw[c] < -EPS && k < ke - 1)  // selector on s.rho_w, as written (1426)
-                flux_kp = up3(wp, th[c + 2 * P], th[c + P], th[c]);
+                flux_kp = up3(wp, ro(th + c - P), ro(th + c), ro(th + c + P));
+            else if (ro(a.s_rw + c) < -EPS && k < ke - 1)  // selector on s.rho_w, as written (1426)
+                flux_kp = up3(wp, ro(th + c + 2 * P), ro(th + c + P), ro(th + c));
             else
-                flux_kp = wp * f2h(th[c], th[c + P], dz[k], dz[k + 1]);
+                flux_kp = wp * f2h(ro(th + c), ro(th + c + P), dz[k], dz[k + 1]);
         }
         if (k == 0) {
             flux_km = T(0.0);
         } else {
-            const T wp = a.rw_p[c - P];
-            const T sw = a.s_rw[c - P];
+            const T wp = w_km;
+            const T sw = ro(a.s_rw + c - P);
             if (sw > EPS && k > 1)
-                flux_km = up3(wp, th[c - 2 * P], th[c - P], th[c]);
+                flux_km = up3(wp, ro(th + c - 2 * P), ro(th + c - P), ro(th + c));
             else if (sw < -EPS && k < ke)
-                flux_km = up3(wp, th[c + P], th[c], th[c - P]);
+                flux_km = up3(wp, ro(th + c + P), ro(th + c), ro(th + c - P));
             else
-                flux_km = wp * f2h(th[c - P], th[c], dz[k - 1], dz[k]);
+                flux_km = wp * f2h(ro(th + c - P), ro(th + c), dz[k - 1], dz[k]);
         }
         const T advection = -(flux_kp - flux_km) / dz[k];
         a.rt_out[c] = a.rt_out[c] + dt_s * advection;
-        if (k < ke) a.mfz[c] = a.mfz[c] + a.rw_p[c] / ns_T;
+        if (k < ke) a.mfz[c] = a.mfz[c] + w_k / ns_T;
+    };
+    TT x = dprev;
+    T w_hi = (T)x;
+    a.rw_p[MOIST_IDX(n - 1, i)] = w_hi;
+    vertical(ke, T(0.0), w_hi);
+    for (int j = n - 2; j >= 0; j--) {
+        x = a.dprime[MOIST_IDX(j, i)] - ro(a.tcp + MOIST_IDX(j, i)) * x;
+        const T w_j = (T)x;
+        a.rw_p[MOIST_IDX(j, i)] = w_j;
+        vertical(j + 1, w_hi, w_j);
+        w_hi = w_j;
     }
+    vertical(0, w_hi, T(0.0));
 }
 
 
@@ -741,11 +759,11 @@ __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a
             const int k = e / nf, f = e - k * nf;
             const int cc = wrapx(i0 + f - 1, nx), cn = wrapx(cc + 1, nx);
             const size_t a0 = MOIST_IDX(k, cc), a1 = MOIST_IDX(k, cn);
-            T grad_x = (a.rt_in[a1] - a.rt_in[a0]) / dx;
-            const T grad_x_old = (a.rt_old[a1] - a.rt_old[a0]) / dx;
+            T grad_x = (ro(a.rt_in + a1) - ro(a.rt_in + a0)) / dx;
+            const T grad_x_old = (ro(a.rt_old + a1) - ro(a.rt_old + a0)) / dx;
             grad_x = grad_x + p.gamma_d * (grad_x - grad_x_old);
-            const T rt2pres_h = (a.rt2pres[a0] + a.rt2pres[a1]) * T(0.5);
-            sm.u[k * wf + f] = a.ru_in[a0] + dt_s * (a.R_ru[a0] - rt2pres_h * grad_x);
+            const T rt2pres_h = (ro(a.rt2pres + a0) + ro(a.rt2pres + a1)) * T(0.5);
+            sm.u[k * wf + f] = ro(a.ru_in + a0) + dt_s * (ro(a.R_ru + a0) - rt2pres_h * grad_x);
         }
     }
     __syncthreads();
@@ -761,16 +779,16 @@ __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a
         a.ru_out[c] = u_p;
         a.mfx[c] = a.mfx[c] + u_p / ns_T;
         T advection = -(u_p - u_m) / dx;
-        T inc = dt_s * (a.R_rho[c] + advection);
+        T inc = dt_s * (ro(a.R_rho + c) + advection);
         const T rho_old = a.rho_p[c];
         sm.rho_tp[k * wc + col] = (T)((double)rho_old + fact_tp64 * (double)inc);
         a.rho_p[c] = rho_old + inc;
-        const T th_i = a.theta[c], th_ip = a.theta[MOIST_IDX(k, ip)], th_im = a.theta[MOIST_IDX(k, im)];
+        const T th_i = ro(a.theta + c), th_ip = ro(a.theta + MOIST_IDX(k, ip)), th_im = ro(a.theta + MOIST_IDX(k, im));
         const T flux_ip = (th_ip + th_i) * T(0.5) * u_p;
         const T flux_im = (th_i + th_im) * T(0.5) * u_m;
         advection = -(flux_ip - flux_im) / dx;
-        inc = dt_s * (a.R_rt[c] + advection);
-        const T rtp = a.rt_in[c];
+        inc = dt_s * (ro(a.R_rt + c) + advection);
+        const T rtp = ro(a.rt_in + c);
         sm.rt_tp[k * wc + col] = (T)((double)rtp + fact_tp64 * (double)inc);
         a.rt_out[c] = rtp + inc;
     }
@@ -782,18 +800,18 @@ __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a
         const size_t c = MOIST_IDX(k, i), cj = c - P;
         const T buoyancy = (sm.rt_tp[k * wc + col] - sm.rt_tp[j * wc + col]) / (z[k] - z[j]);
         const T grav = -p.GRAV * T(0.5) * (sm.rho_tp[k * wc + col] + sm.rho_tp[j * wc + col]);
-        const T rt2pres_h = (a.rt2pres[cj] + a.rt2pres[c]) * T(0.5);
-        const T drho_w = dt_s * (a.R_rw[cj] - rt2pres_h * buoyancy + grav);
+        const T rt2pres_h = (ro(a.rt2pres + cj) + ro(a.rt2pres + c)) * T(0.5);
+        const T drho_w = dt_s * (ro(a.R_rw + cj) - rt2pres_h * buoyancy + grav);
         const T w_j = a.rw_p[cj];
-        const T aj = a.ta[cj];
+        const T aj = ro(a.ta + cj);
         T d = w_j + drho_w;
         if (j > 0) d -= aj * fact * w_j;
-        d -= a.tb[cj] * fact * w_j;
-        if (j < n - 1) d -= a.tc[cj] * fact * a.rw_p[c];
+        d -= ro(a.tb + cj) * fact * w_j;
+        if (j < n - 1) d -= ro(a.tc + cj) * fact * a.rw_p[c];
         sm.D[j * wc + col] = (TT)d;
         sm.a[j * wc + col] = aj;
-        sm.piv[j * wc + col] = a.tpiv[cj];
-        sm.cp[j * wc + col] = a.tcp[cj];
+        sm.piv[j * wc + col] = ro(a.tpiv + cj);
+        sm.cp[j * wc + col] = ro(a.tcp + cj);
     }
     __syncthreads();
     // (4) Thomas elimination per column (moist.jl:956-970)
@@ -834,23 +852,23 @@ __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a
         } else {
             const T wp = w_k;
             if (wp > EPS && k > 0)
-                flux_kp = up3(wp, th[c - P], th[c], th[c + P]);
-            else if (a.s_rw[c] < -EPS && k < ke - 1)  // selector on s.rho_w, as written (1426)
-                flux_kp = up3(wp, th[c + 2 * P], th[c + P], th[c]);
+                flux_kp = up3(wp, ro(th + c - P), ro(th + c), ro(th + c + P));
+            else if (ro(a.s_rw + c) < -EPS && k < ke - 1)  // selector on s.rho_w, as written (1426)
+                flux_kp = up3(wp, ro(th + c + 2 * P), ro(th + c + P), ro(th + c));
             else
-                flux_kp = wp * f2h(th[c], th[c + P], dz[k], dz[k + 1]);
+                flux_kp = wp * f2h(ro(th + c), ro(th + c + P), dz[k], dz[k + 1]);
         }
         if (k == 0) {
             flux_km = T(0.0);
         } else {
             const T wp = w_km;
-            const T sw = a.s_rw[c - P];
+            const T sw = ro(a.s_rw + c - P);
             if (sw > EPS && k > 1)
-                flux_km = up3(wp, th[c - 2 * P], th[c - P], th[c]);
+                flux_km = up3(wp, ro(th + c - 2 * P), ro(th + c - P), ro(th + c));
             else if (sw < -EPS && k < ke)
-                flux_km = up3(wp, th[c + P], th[c], th[c - P]);
+                flux_km = up3(wp, ro(th + c + P), ro(th + c), ro(th + c - P));
             else
-                flux_km = wp * f2h(th[c - P], th[c], dz[k - 1], dz[k]);
+                flux_km = wp * f2h(ro(th + c - P), ro(th + c), dz[k - 1], dz[k]);
         }
         const T advection = -(flux_kp - flux_km) / dz[k];
         a.rt_out[c] = a.rt_out[c] + dt_s * advection;
