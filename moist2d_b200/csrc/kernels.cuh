@@ -204,8 +204,8 @@ __device__ __forceinline__ void b_diag(DevParams<T> p, StateP<T> s, T* pres, T* 
     const int nx = p.nx, nz = p.nz, P = p.P;
     if (i >= nx || k >= nz || halted(err)) return;
     const size_t c = MOIST_IDX(k, i);
-    const T rho = s.rho[c], rt = s.rt[c];
-    const T qv = s.qv[c] / rho, qc = s.qc[c] / rho, qr = s.qr[c] / rho;
+    const T rho = ro(s.rho + c), rt = ro(s.rt + c);
+    const T qv = ro(s.qv + c) / rho, qc = ro(s.qc + c) / rho, qr = ro(s.qr + c) / rho;
     const T qd = T(1.0) - qv - qc - qr;
     const T r = p.Rd * qd + p.Rv * qv;
     const T cp = p.Cpd * qd + p.Cpv * qv + p.Cpl * (qc + qr);
@@ -215,8 +215,8 @@ __device__ __forceinline__ void b_diag(DevParams<T> p, StateP<T> s, T* pres, T* 
     theta[c] = rt / rho;
     rt2pres[c] = cp / cv * pr / rt;
     const int ip = wrapx(i + 1, nx);
-    u_face[c] = s.ru[c] * T(2.0) / (rho + s.rho[MOIST_IDX(k, ip)]);
-    if (k < nz - 1) w_face[c] = s.rw[c] / f2h(rho, s.rho[c + P], p.dz[k], p.dz[k + 1]);
+    u_face[c] = ro(s.ru + c) * T(2.0) / (rho + ro(s.rho + (MOIST_IDX(k, ip))));
+    if (k < nz - 1) w_face[c] = ro(s.rw + c) / f2h(rho, ro(s.rho + (c + P)), p.dz[k], p.dz[k + 1]);
 }
 template <class T>
 __global__ void k_diag(DevParams<T> p, StateP<T> s, T* pres, T* theta, T* rt2pres, T* u_face,                        T* w_face, const int* err) {
@@ -256,185 +256,185 @@ __device__ __forceinline__ void b_tend(DevParams<T> p, TendArgs<T> a, const int*
     auto R = [&](int kk, int ii) { return MOIST_IDX(kk, ii); };
 
     if (k == 0 && i == 0) {
-        *a.ru_left = ru[R(0, nx - 1)];
-        *a.rho_right = rho[R(0, 0)];
+        *a.ru_left = ro(ru + (R(0, nx - 1)));
+        *a.rho_right = ro(rho + (R(0, 0)));
     }
 
     // --- R_rho (1079-1086)
     {
-        const T flux_kp = k == ke ? T(0.0) : rw[c];
-        const T flux_km = k == 0 ? T(0.0) : rw[c - P];
-        const T advection = -((ru[c] - ru[R(k, im)]) / dx + (flux_kp - flux_km) / dz[k]);
-        a.R_rho[c] = advection + a.ph.d_rho[c];
+        const T flux_kp = k == ke ? T(0.0) : ro(rw + c);
+        const T flux_km = k == 0 ? T(0.0) : ro(rw + (c - P));
+        const T advection = -((ro(ru + c) - ro(ru + (R(k, im)))) / dx + (flux_kp - flux_km) / dz[k]);
+        a.R_rho[c] = advection + ro(a.ph.d_rho + c);
     }
     // --- R_rho_u (1098-1178)
     {
-        const T rho_u_ip = T(0.5) * (ru[c] + ru[R(k, ip)]);
+        const T rho_u_ip = T(0.5) * (ro(ru + c) + ro(ru + (R(k, ip))));
         T f_ip;
         if (rho_u_ip > EPS)
-            f_ip = up3(rho_u_ip, uf[R(k, im)], uf[c], uf[R(k, ip)]);
+            f_ip = up3(rho_u_ip, ro(uf + (R(k, im))), ro(uf + c), ro(uf + (R(k, ip))));
         else if (rho_u_ip < -EPS)
-            f_ip = up3(rho_u_ip, uf[R(k, ip2)], uf[R(k, ip)], uf[c]);
+            f_ip = up3(rho_u_ip, ro(uf + (R(k, ip2))), ro(uf + (R(k, ip))), ro(uf + c));
         else
-            f_ip = rho_u_ip * (uf[c] + uf[R(k, ip)]) * T(0.5);
-        const T rho_u_im = T(0.5) * (ru[R(k, im)] + ru[c]);
+            f_ip = rho_u_ip * (ro(uf + c) + ro(uf + (R(k, ip)))) * T(0.5);
+        const T rho_u_im = T(0.5) * (ro(ru + (R(k, im))) + ro(ru + c));
         T f_im;
         if (rho_u_im > EPS)
-            f_im = up3(rho_u_im, uf[R(k, im2)], uf[R(k, im)], uf[c]);
+            f_im = up3(rho_u_im, ro(uf + (R(k, im2))), ro(uf + (R(k, im))), ro(uf + c));
         else if (rho_u_im < -EPS)
-            f_im = up3(rho_u_im, uf[R(k, ip)], uf[c], uf[R(k, im)]);
+            f_im = up3(rho_u_im, ro(uf + (R(k, ip))), ro(uf + c), ro(uf + (R(k, im))));
         else
-            f_im = rho_u_im * (uf[R(k, im)] + uf[c]) * T(0.5);
+            f_im = rho_u_im * (ro(uf + (R(k, im))) + ro(uf + c)) * T(0.5);
         const T druudx = (f_ip - f_im) / dx;
         T f_kp;
         if (k == ke) {
             f_kp = T(0.0);
         } else {
-            const T rho_w_kp = T(0.5) * (rw[c] + rw[R(k, ip)]);
+            const T rho_w_kp = T(0.5) * (ro(rw + c) + ro(rw + (R(k, ip))));
             if (rho_w_kp > EPS && k > 0)
-                f_kp = up3(rho_w_kp, uf[c - P], uf[c], uf[c + P]);
+                f_kp = up3(rho_w_kp, ro(uf + (c - P)), ro(uf + c), ro(uf + (c + P)));
             else if (rho_w_kp < -EPS && k < ke - 1)
-                f_kp = up3(rho_w_kp, uf[c + 2 * P], uf[c + P], uf[c]);
+                f_kp = up3(rho_w_kp, ro(uf + (c + 2 * P)), ro(uf + (c + P)), ro(uf + c));
             else
-                f_kp = rho_w_kp * f2h(uf[c], uf[c + P], dz[k], dz[k + 1]);
+                f_kp = rho_w_kp * f2h(ro(uf + c), ro(uf + (c + P)), dz[k], dz[k + 1]);
         }
         T f_km;
         if (k == 0) {
             f_km = T(0.0);
         } else {
-            const T rho_w_km = T(0.5) * (rw[c - P] + rw[R(k - 1, ip)]);
+            const T rho_w_km = T(0.5) * (ro(rw + (c - P)) + ro(rw + (R(k - 1, ip))));
             if (rho_w_km > EPS && k > 1)
-                f_km = up3(rho_w_km, uf[c - 2 * P], uf[c - P], uf[c]);
+                f_km = up3(rho_w_km, ro(uf + (c - 2 * P)), ro(uf + (c - P)), ro(uf + c));
             else if (rho_w_km < -EPS && k < ke)
-                f_km = up3(rho_w_km, uf[c + P], uf[c], uf[c - P]);
+                f_km = up3(rho_w_km, ro(uf + (c + P)), ro(uf + c), ro(uf + (c - P)));
             else
-                f_km = rho_w_km * f2h(uf[c - P], uf[c], dz[k - 1], dz[k]);
+                f_km = rho_w_km * f2h(ro(uf + (c - P)), ro(uf + c), dz[k - 1], dz[k]);
         }
         const T drwudz = (f_kp - f_km) / dz[k];
         const T advection = -druudx - drwudz;
-        const T u_ip = (uf[R(k, ip)] - uf[c]) / dx;
-        const T u_im = (uf[c] - uf[R(k, im)]) / dx;
-        const T u_xx = (u_ip * rho[R(k, ip)] - u_im * rho[c]) / dx;
-        const T u_kp = k == ke ? T(0.0) : (uf[c + P] - uf[c]) / (z[k + 1] - z[k]);
-        const T u_km = k == 0 ? T(0.0) : (uf[c] - uf[c - P]) / (z[k] - z[k - 1]);
-        const T rho_kp = k == ke ? T(0.0) : T(0.25) * (rho[c] + rho[c + P] + rho[R(k, ip)] + rho[R(k + 1, ip)]);
-        const T rho_km = k == 0 ? T(0.0) : T(0.25) * (rho[c - P] + rho[c] + rho[R(k - 1, ip)] + rho[R(k, ip)]);
+        const T u_ip = (ro(uf + (R(k, ip))) - ro(uf + c)) / dx;
+        const T u_im = (ro(uf + c) - ro(uf + (R(k, im)))) / dx;
+        const T u_xx = (u_ip * ro(rho + (R(k, ip))) - u_im * ro(rho + c)) / dx;
+        const T u_kp = k == ke ? T(0.0) : (ro(uf + (c + P)) - ro(uf + c)) / (z[k + 1] - z[k]);
+        const T u_km = k == 0 ? T(0.0) : (ro(uf + c) - ro(uf + (c - P))) / (z[k] - z[k - 1]);
+        const T rho_kp = k == ke ? T(0.0) : T(0.25) * (ro(rho + c) + ro(rho + (c + P)) + ro(rho + (R(k, ip))) + ro(rho + (R(k + 1, ip))));
+        const T rho_km = k == 0 ? T(0.0) : T(0.25) * (ro(rho + (c - P)) + ro(rho + c) + ro(rho + (R(k - 1, ip))) + ro(rho + (R(k, ip))));
         const T u_zz = (u_kp * rho_kp - u_km * rho_km) / dz[k];
         const T diffusion = p.nu * (u_xx + u_zz);
-        const T dpdx = (a.pres[R(k, ip)] - a.pres[c]) / dx;
-        a.R_ru[c] = advection - dpdx + diffusion + a.ph.d_u[c];
+        const T dpdx = (ro(a.pres + (R(k, ip))) - ro(a.pres + c)) / dx;
+        a.R_ru[c] = advection - dpdx + diffusion + ro(a.ph.d_u + c);
     }
     // --- R_rho_w (1190-1278)
     if (k < ke) {
-        const T rho_u_ip = f2h(ru[c], ru[c + P], z[k], z[k + 1]);  // z weights, as written (1196)
+        const T rho_u_ip = f2h(ro(ru + c), ro(ru + (c + P)), z[k], z[k + 1]);  // z weights, as written (1196)
         T f_ip;
         if (rho_u_ip > EPS)
-            f_ip = up3(rho_u_ip, wf[R(k, im)], wf[c], wf[R(k, ip)]);
+            f_ip = up3(rho_u_ip, ro(wf + (R(k, im))), ro(wf + c), ro(wf + (R(k, ip))));
         else if (rho_u_ip < -EPS)
-            f_ip = up3(rho_u_ip, wf[R(k, ip2)], wf[R(k, ip)], wf[c]);
+            f_ip = up3(rho_u_ip, ro(wf + (R(k, ip2))), ro(wf + (R(k, ip))), ro(wf + c));
         else
-            f_ip = rho_u_ip * (wf[c] + wf[R(k, ip)]) * T(0.5);
-        const T rho_u_im = f2h(ru[R(k, im)], ru[R(k + 1, im)], dz[k], dz[k + 1]);
+            f_ip = rho_u_ip * (ro(wf + c) + ro(wf + (R(k, ip)))) * T(0.5);
+        const T rho_u_im = f2h(ro(ru + (R(k, im))), ro(ru + (R(k + 1, im))), dz[k], dz[k + 1]);
         T f_im;
         if (rho_u_im > EPS)
-            f_im = up3(rho_u_im, wf[R(k, im2)], wf[R(k, im)], wf[c]);
+            f_im = up3(rho_u_im, ro(wf + (R(k, im2))), ro(wf + (R(k, im))), ro(wf + c));
         else if (rho_u_im < -EPS)
-            f_im = up3(rho_u_im, wf[R(k, ip)], wf[c], wf[R(k, im)]);
+            f_im = up3(rho_u_im, ro(wf + (R(k, ip))), ro(wf + c), ro(wf + (R(k, im))));
         else
-            f_im = rho_u_im * (wf[R(k, im)] + wf[c]) * T(0.5);
+            f_im = rho_u_im * (ro(wf + (R(k, im))) + ro(wf + c)) * T(0.5);
         const T drwudx = (f_ip - f_im) / dx;
         T f_kp;
         if (k == ke - 1) {
             f_kp = T(0.0);
         } else {
-            const T rho_w_kp = f2h(rw[c], rw[c + P], dz[k], dz[k + 1]);
+            const T rho_w_kp = f2h(ro(rw + c), ro(rw + (c + P)), dz[k], dz[k + 1]);
             if (rho_w_kp > EPS && k > 0)
-                f_kp = up3(rho_w_kp, wf[c - P], wf[c], wf[c + P]);
+                f_kp = up3(rho_w_kp, ro(wf + (c - P)), ro(wf + c), ro(wf + (c + P)));
             else if (rho_w_kp < -EPS && k < ke - 2)
-                f_kp = up3(rho_w_kp, wf[c + 2 * P], wf[c + P], wf[c]);
+                f_kp = up3(rho_w_kp, ro(wf + (c + 2 * P)), ro(wf + (c + P)), ro(wf + c));
             else
-                f_kp = rho_w_kp * f2h(wf[c], wf[c + P], dz[k], dz[k + 1]);
+                f_kp = rho_w_kp * f2h(ro(wf + c), ro(wf + (c + P)), dz[k], dz[k + 1]);
         }
         T f_km;
         if (k == 0) {
             f_km = T(0.0);
         } else {
-            const T rho_w_km = f2h(rw[c - P], rw[c], dz[k - 1], dz[k]);
+            const T rho_w_km = f2h(ro(rw + (c - P)), ro(rw + c), dz[k - 1], dz[k]);
             if (rho_w_km > EPS && k > 1)
-                f_km = up3(rho_w_km, wf[c - 2 * P], wf[c - P], wf[c]);
+                f_km = up3(rho_w_km, ro(wf + (c - 2 * P)), ro(wf + (c - P)), ro(wf + c));
             else if (rho_w_km < -EPS && k < ke - 1)
-                f_km = up3(rho_w_km, wf[c + P], wf[c], wf[c - P]);
+                f_km = up3(rho_w_km, ro(wf + (c + P)), ro(wf + c), ro(wf + (c - P)));
             else
-                f_km = rho_w_km * f2h(wf[c - P], wf[c], dz[k - 1], dz[k]);
+                f_km = rho_w_km * f2h(ro(wf + (c - P)), ro(wf + c), dz[k - 1], dz[k]);
         }
         const T drwwdz = (f_kp - f_km) / (z[k + 1] - z[k]);
         const T advection = -drwudx - drwwdz;
-        const T w_ip = (wf[R(k, ip)] - wf[c]) / dx;
-        const T w_im = (wf[c] - wf[R(k, im)]) / dx;
-        const T rho_ip = T(0.25) * (rho[c] + rho[c + P] + rho[R(k, ip)] + rho[R(k + 1, ip)]);
-        const T rho_im = T(0.25) * (rho[R(k, im)] + rho[R(k + 1, im)] + rho[c] + rho[c + P]);
+        const T w_ip = (ro(wf + (R(k, ip))) - ro(wf + c)) / dx;
+        const T w_im = (ro(wf + c) - ro(wf + (R(k, im)))) / dx;
+        const T rho_ip = T(0.25) * (ro(rho + c) + ro(rho + (c + P)) + ro(rho + (R(k, ip))) + ro(rho + (R(k + 1, ip))));
+        const T rho_im = T(0.25) * (ro(rho + (R(k, im))) + ro(rho + (R(k + 1, im))) + ro(rho + c) + ro(rho + (c + P)));
         const T w_xx = (w_ip * rho_ip - w_im * rho_im) / dx;
-        const T w_kp = k == ke - 1 ? T(0.0) : (wf[c + P] - wf[c]) / dz[k + 1];
-        const T w_km = k == 0 ? T(0.0) : (wf[c] - wf[c - P]) / dz[k];
-        const T w_zz = (w_kp * rho[c + P] - w_km * rho[c]) / (z[k + 1] - z[k]);
+        const T w_kp = k == ke - 1 ? T(0.0) : (ro(wf + (c + P)) - ro(wf + c)) / dz[k + 1];
+        const T w_km = k == 0 ? T(0.0) : (ro(wf + c) - ro(wf + (c - P))) / dz[k];
+        const T w_zz = (w_kp * ro(rho + (c + P)) - w_km * ro(rho + c)) / (z[k + 1] - z[k]);
         const T diffusion = p.nu * (w_xx + w_zz);
         T sigma = T(0.0);
         const T zfk = p.zf[k];
         if (zfk > (T(1.0) - p.zf_sponge) * p.H)
             sigma = (GRAV / T(30.0)) * ((zfk - (T(1.0) - p.zf_sponge) * p.H) / (p.zf_sponge * p.H));
-        const T sponge = -sigma * rw[c];
-        const T dpdz = (a.pres[c + P] - a.pres[c]) / (z[k + 1] - z[k]);
-        const T buoyancy = -GRAV * (rho[c] + rho[c + P]) * T(0.5);
+        const T sponge = -sigma * ro(rw + c);
+        const T dpdz = (ro(a.pres + (c + P)) - ro(a.pres + c)) / (z[k + 1] - z[k]);
+        const T buoyancy = -GRAV * (ro(rho + c) + ro(rho + (c + P))) * T(0.5);
         a.R_rw[c] = advection - dpdz + buoyancy + diffusion + sponge;
     }
     // --- R_rho_theta (1284-1331)
     {
-        const T ru_i = ru[c], ru_m = ru[R(k, im)];
+        const T ru_i = ro(ru + c), ru_m = ro(ru + (R(k, im)));
         T f_ip, f_im, f_kp, f_km;
         if (ru_i > EPS)
-            f_ip = up3(ru_i, th[R(k, im)], th[c], th[R(k, ip)]);
+            f_ip = up3(ru_i, ro(th + (R(k, im))), ro(th + c), ro(th + (R(k, ip))));
         else if (ru_i < -EPS)
-            f_ip = up3(ru_i, th[R(k, ip2)], th[R(k, ip)], th[c]);
+            f_ip = up3(ru_i, ro(th + (R(k, ip2))), ro(th + (R(k, ip))), ro(th + c));
         else
-            f_ip = ru_i * (th[c] + th[R(k, ip)]) * T(0.5);
+            f_ip = ru_i * (ro(th + c) + ro(th + (R(k, ip)))) * T(0.5);
         if (ru_m > EPS)
-            f_im = up3(ru_m, th[R(k, im2)], th[R(k, im)], th[c]);
+            f_im = up3(ru_m, ro(th + (R(k, im2))), ro(th + (R(k, im))), ro(th + c));
         else if (ru_m < -EPS)
-            f_im = up3(ru_m, th[R(k, ip)], th[c], th[R(k, im)]);
+            f_im = up3(ru_m, ro(th + (R(k, ip))), ro(th + c), ro(th + (R(k, im))));
         else
-            f_im = ru_m * (th[R(k, im)] + th[c]) * T(0.5);
+            f_im = ru_m * (ro(th + (R(k, im))) + ro(th + c)) * T(0.5);
         if (k == ke) {
             f_kp = T(0.0);
         } else {
-            const T w = rw[c];
+            const T w = ro(rw + c);
             if (w > EPS && k > 0)
-                f_kp = up3(w, th[c - P], th[c], th[c + P]);
+                f_kp = up3(w, ro(th + (c - P)), ro(th + c), ro(th + (c + P)));
             else if (w < -EPS && k < ke - 1)
-                f_kp = up3(w, th[c + 2 * P], th[c + P], th[c]);
+                f_kp = up3(w, ro(th + (c + 2 * P)), ro(th + (c + P)), ro(th + c));
             else
-                f_kp = w * f2h(th[c], th[c + P], dz[k], dz[k + 1]);
+                f_kp = w * f2h(ro(th + c), ro(th + (c + P)), dz[k], dz[k + 1]);
         }
         if (k == 0) {
             f_km = T(0.0);
         } else {
-            const T w = rw[c - P];
+            const T w = ro(rw + (c - P));
             if (w > EPS && k > 1)
-                f_km = up3(w, th[c - 2 * P], th[c - P], th[c]);
+                f_km = up3(w, ro(th + (c - 2 * P)), ro(th + (c - P)), ro(th + c));
             else if (w < -EPS && k < ke)
-                f_km = up3(w, th[c + P], th[c], th[c - P]);
+                f_km = up3(w, ro(th + (c + P)), ro(th + c), ro(th + (c - P)));
             else
-                f_km = w * f2h(th[c - P], th[c], dz[k - 1], dz[k]);
+                f_km = w * f2h(ro(th + (c - P)), ro(th + c), dz[k - 1], dz[k]);
         }
         const T advection = -((f_ip - f_im) / dx + (f_kp - f_km) / dz[k]);
-        a.R_rt[c] = advection + a.ph.d_th[c];
+        a.R_rt[c] = advection + ro(a.ph.d_th + c);
     }
     // --- perturbations and saved momentum fluxes (1339-1348)
-    a.rho_p[c] = a.s0.rho[c] - rho[c];
-    a.ru_p[c] = a.s0.ru[c] - ru[c];
-    a.rw_p[c] = a.s0.rw[c] - rw[c];
-    a.rt_p[c] = a.s0.rt[c] - a.s.rt[c];
-    a.mfx[c] = ru[c];
-    a.mfz[c] = rw[c];
+    a.rho_p[c] = ro(a.s0.rho + c) - ro(rho + c);
+    a.ru_p[c] = ro(a.s0.ru + c) - ro(ru + c);
+    a.rw_p[c] = ro(a.s0.rw + c) - ro(rw + c);
+    a.rt_p[c] = ro(a.s0.rt + c) - ro(a.s.rt + c);
+    a.mfx[c] = ro(ru + c);
+    a.mfz[c] = ro(rw + c);
 }
 template <class T>
 __global__ void k_tend(DevParams<T> p, TendArgs<T> a, const int* err) {
