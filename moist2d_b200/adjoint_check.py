@@ -58,6 +58,42 @@ def controls(p, s, g):
     return {"theta": rho * g["rho_theta"][:, c], "qv": rho * g["rho_qv"][:, c]}
 
 
+def directions(seed, n, nz, nx, white=False):
+    """n seeded (d_theta, d_qv) pairs of (nz, nx) fields: each a random combination of four
+    large-scale modes sin(2 pi kx x / Lx + phase) sin(pi kz (k + 1/2) / nz) (kx in 1..5, kz in
+    1..3), or white noise; d_qv scaled by 1e-4. Drawn in the order d_theta, d_qv, d_theta, ..."""
+    rng = np.random.default_rng(seed)
+    zz, xx = np.meshgrid(np.arange(nz), np.arange(nx), indexing="ij")
+
+    def field():
+        if white:
+            return rng.standard_normal((nz, nx))
+        d = np.zeros((nz, nx))
+        for _ in range(4):
+            kx, kz, ph = rng.integers(1, 6), rng.integers(1, 4), rng.uniform(0.0, 2.0 * np.pi)
+            d += rng.standard_normal() * np.sin(2 * np.pi * kx * xx / nx + ph) * np.sin(np.pi * kz * (zz + 0.5) / nz)
+        return d
+
+    out = []
+    for _ in range(n):
+        d_th = field()
+        out.append((d_th, 1e-4 * field()))
+    return out
+
+
+def state_direction(p, s, d_theta, d_qv):
+    """The State-space direction of (d_theta, d_qv) at fixed rho: d rho_theta = rho d_theta,
+    d rho_qv = rho d_qv on the interior, as (ka, ia) arrays with zero halo columns."""
+    c = slice(p.is_ - 1, p.ie)
+    rho = s.rho[:, c].astype(np.float64)
+    out = {}
+    for f, d in (("rho_theta", d_theta), ("rho_qv", d_qv)):
+        a = np.zeros((p.ka, p.ia))
+        a[:, c] = rho * d
+        out[f] = a
+    return out
+
+
 def perturbed(p, s, d_theta, d_qv, h):
     a = s.copy()
     c = slice(p.is_ - 1, p.ie)
@@ -85,23 +121,8 @@ def main():
     g32 = run(p32, s32, args.steps, args.ckpt)
     cg64, cg32 = controls(p64, s64, g64), controls(p32, s32, g32)
 
-    rng = np.random.default_rng(args.seed)
-    nz, nx = p64.Nz, p64.Nx
-    zz, xx = np.meshgrid(np.arange(nz), np.arange(nx), indexing="ij")
-
-    def field():
-        if args.white:
-            return rng.standard_normal((nz, nx))
-        d = np.zeros((nz, nx))
-        for _ in range(4):
-            kx, kz, ph = rng.integers(1, 6), rng.integers(1, 4), rng.uniform(0.0, 2.0 * np.pi)
-            d += rng.standard_normal() * np.sin(2 * np.pi * kx * xx / nx + ph) * np.sin(np.pi * kz * (zz + 0.5) / nz)
-        return d
-
     errs = []
-    for _ in range(args.dirs):
-        d_th = field()
-        d_qv = 1e-4 * field()
+    for d_th, d_qv in directions(args.seed, args.dirs, p64.Nz, p64.Nx, args.white):
         ad = float(np.sum(cg64["theta"] * d_th) + np.sum(cg64["qv"] * d_qv))
         h = args.h
         fd = (objective(p64, perturbed(p64, s64, d_th, d_qv, h), args.steps)

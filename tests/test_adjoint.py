@@ -275,3 +275,43 @@ def test_adjoint_tiny_shapes_forward_mode(nx, nz):
     seeds = state_seeds(p, s, 13)
     g, _ = run_adjoint(p, s, 3, 2, prec_w, seeds)
     tangent_check(p, s, 3, prec_w, seeds, g, ndir=3, seed=nx * 10 + nz)
+
+
+FIXTURE_RTOL = 1e-12
+
+
+def fixture_errors(fx, p, s, g):
+    """Relative differences of the adjoint from the fixture's forward-mode derivatives: per
+    direction |<grad, v> - dJ| / sum |grad * v|, per parameter |g - dJ| / |dJ|."""
+    from moist2d_b200.adjoint_check import controls, directions
+    cg = controls(p, s, g)
+    errs = []
+    for (d_th, d_qv), ref in zip(directions(fx["seed"], fx["dirs"], p.Nz, p.Nx), fx["directions"]):
+        assert np.isclose(float(np.sum(d_th * d_th)), ref["norm2_theta"], rtol=1e-12, atol=0.0)
+        assert np.isclose(float(np.sum(d_qv * d_qv)), ref["norm2_qv"], rtol=1e-12, atol=0.0)
+        ad = float(np.sum(cg["theta"] * d_th) + np.sum(cg["qv"] * d_qv))
+        scale = float(np.sum(np.abs(cg["theta"] * d_th)) + np.sum(np.abs(cg["qv"] * d_qv)))
+        errs.append(abs(ad - ref["dJ"]) / scale)
+    par = {k: abs(g[k] - v) / abs(v) for k, v in fx["params"].items()}
+    return errs, par
+
+
+def test_adjoint_single_bubble_matches_forward_mode_fixture():
+    """The adjoint workload (512 x 96 single bubble, Float64, rain objective) over the configured
+    600 steps against the exact directional derivatives of the oracle's step in forward mode
+    (tests/golden/tangent_single_bubble.json, made by tests/golden/make_tangent_single_bubble.py):
+    <grad, v> in 16 seeded large-scale directions of theta' and qv, and both parameter gradients.
+    Central differences cannot serve here (over 600 steps they scatter on some directions); the
+    forward-mode derivative has no truncation error."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tangent_single_bubble.json")) as f:
+        fx = json.load(f)
+    p, s = single_bubble(np.float64)
+    g, _ = run_adjoint(p, s, fx["steps"], 50, rain_weight(p), {})
+    assert fx["J"] > 0.0
+    assert np.isclose(g["objective"], fx["J"], rtol=1e-13, atol=0.0)
+    errs, par = fixture_errors(fx, p, s, g)
+    assert max(errs) <= FIXTURE_RTOL, errs
+    for k, e in par.items():
+        assert e <= FIXTURE_RTOL, (k, e)
