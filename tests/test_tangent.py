@@ -71,3 +71,18 @@ def test_tangent_rejects_float32():
     p, s = bubble_case(np.float32, nx=8, nz=6)
     with pytest.raises(ValueError):
         bind.tangent(p, s, 1)
+
+
+def test_golden_fixture_directions_regenerate():
+    """tests/golden/tangent_single_bubble.json names its directions by seed; they must
+    regenerate to the same fields (squared norms to 1e-12) for the GPU comparison to mean
+    anything."""
+    import json
+    import os
+    from moist2d_b200.adjoint_check import directions
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "tangent_single_bubble.json")) as f:
+        fx = json.load(f)
+    assert fx["steps"] == 600 and fx["J"] > 0.0 and len(fx["directions"]) == fx["dirs"]
+    for (d_th, d_qv), ref in zip(directions(fx["seed"], fx["dirs"], 96, 512), fx["directions"]):
+        assert np.isclose(float(np.sum(d_th * d_th)), ref["norm2_theta"], rtol=1e-12, atol=0.0)
+        assert np.isclose(float(np.sum(d_qv * d_qv)), ref["norm2_qv"], rtol=1e-12, atol=0.0)
