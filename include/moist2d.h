@@ -51,7 +51,9 @@ enum {
     MOIST_ERR_CUDA = 3,         /* a CUDA runtime call failed; text in moist_last_error */
     MOIST_ERR_TIMEOUT = 4,      /* a bounded device-side wait ran out */
     MOIST_ERR_UNSUPPORTED = 5,  /* valid in the reference but not provided by this library */
-    MOIST_ERR_NOMEM = 6         /* device allocation failed */
+    MOIST_ERR_NOMEM = 6,        /* device allocation failed */
+    MOIST_ERR_IO = 7            /* a history or restart file could not be written or read;
+                                   text in moist_io_last_error */
 };
 
 /* field indices reported by moist_nan_field(), in the order compute_step! checks them */
@@ -313,7 +315,8 @@ int moist_batch_adjoint_run(moist_batch* b, int nsteps, int ckpt_every, const mo
 /* output_history's primitive variables (moist.jl:1795-1835) computed on the device from the
  * context State, so that a run_sim-style driver reads only what it writes to its history file:
  * out[f] (f = MOIST_DIAG_*, NULL to skip) receives field f as a host (Nz, Nx) array of the
- * context precision, z fastest, interior only (the file's layout); summary (if not NULL)
+ * context precision, z fastest, interior only (output_history's arrays before the transpose
+ * of its writes; moist_history_append puts them in the file's x-fastest order); summary (if not NULL)
  * receives the run log's min w, max w (m/s), max qc, max qr (g/kg), min RH, max RH (%)
  * (moist.jl:1838-1843). The energy sums of the log come from moist_budget. */
 enum {
@@ -330,6 +333,37 @@ enum {
     MOIST_NDIAG = 10
 };
 int moist_history_diagnostics(moist_ctx* ctx, void* const out[MOIST_NDIAG], double summary[6]);
+
+/* History and restart files: init_history / output_history (moist.jl:1686-1891) and the
+ * restart read of run_sim (moist.jl:1905-1919). The reference writes through NCDatasets; this
+ * library writes the NetCDF classic format with 64-bit offsets (CDF-2) itself, which every
+ * NetCDF reader opens: dimensions x (Nx), z (Nz) and the unlimited time; the variables of
+ * init_history in its order (x, z, zf, time, rho, rhou, rhow, u, w, theta, qv, qc, qr, RH,
+ * temp, pres, thetae, prec, mflux, shflux, lhflux, d_rho_theta_mp, d_rho_qv_mp, d_rho_qc_mp,
+ * d_rho_qr_mp, d_rho_qr_sed, d_rho_u_sf, d_rho_theta_sf, d_rho_qv_sf, d_rho_theta_rd), each of
+ * the context precision with its "units" attribute; a Julia (x, z, time) variable is
+ * (time, z, x) in the file. Failures return MOIST_ERR_IO with the reason in
+ * moist_io_last_error (per host thread). */
+typedef struct moist_history moist_history;
+const char* moist_io_last_error(void);
+/* init_history (moist.jl:1716-1793): creates (replaces) path and writes the header and x, z,
+ * zf. precision: MOIST_F32 or MOIST_F64. */
+int moist_history_create(const char* path, const moist_params* p, int precision, moist_history** out);
+/* output_history (moist.jl:1795-1889): appends one record at time t from the context's State,
+ * with the diagnostics computed on the device (moist_history_diagnostics); pres in hPa. */
+int moist_history_append(moist_history* h, double t, moist_ctx* ctx);
+/* The same record from host arrays: s in the reference layout (NULL fields are written as 0),
+ * diag[f] as moist_history_diagnostics returns them. Needs no device. */
+int moist_history_append_host(moist_history* h, double t, const moist_state_host* s,
+                              const void* const diag[MOIST_NDIAG]);
+int moist_history_close(moist_history* h);
+/* The restart of run_sim (moist.jl:1905-1919): from the last record of a history file, fills
+ * the interior of s->rho, rho_u, rho_w (as stored), rho_theta, rho_qv, rho_qc, rho_qr (theta,
+ * qv, qc, qr times rho in the file's type, then rounded to the context precision) and prec,
+ * and the halo columns of the seven prognostic fields periodically (exchange_halo!). NULL
+ * fields are skipped. rho_qr is read from "qr" (the reference reads "qc" there,
+ * moist.jl:1917). Needs no device. */
+int moist_restart_read(const char* path, const moist_params* p, int precision, moist_state_host* s);
 
 /* ---- Autotuner (no counterpart in the reference). moist_autotune times nsteps large steps of
  * the context for every strip width of the factorisation and acoustic-substep kernels (1, 2, 4

@@ -19,7 +19,9 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_batch_destroy", "moist_batch_member", "moist_batch_upload", "moist_batch_download",
            "moist_batch_step", "moist_batch_time_steps", "moist_batch_last_error", "moist_batch_nan_member",
            "moist_batch_profile", "moist_adjoint_run", "moist_batch_adjoint_run",
-           "moist_autotune", "moist_batch_autotune", "moist_history_diagnostics")
+           "moist_autotune", "moist_batch_autotune", "moist_history_diagnostics", "moist_io_last_error",
+           "moist_history_create", "moist_history_append", "moist_history_append_host",
+           "moist_history_close", "moist_restart_read")
 
 
 def lib():
@@ -77,5 +79,12 @@ def lib():
         L.moist_history_diagnostics.argtypes = [Ctx, C.POINTER(V), C.POINTER(D)]
         L.moist_batch_autotune.argtypes = [B, I, C.c_char_p, C.c_size_t]
         L.moist_batch_adjoint_run.argtypes = [B, I, I, C.POINTER(moist_adjoint_seed), C.POINTER(moist_adjoint_grad), I]
+        H = C.c_void_p
+        L.moist_io_last_error.restype = C.c_char_p
+        L.moist_history_create.argtypes = [C.c_char_p, P, I, C.POINTER(H)]
+        L.moist_history_append.argtypes = [H, D, Ctx]
+        L.moist_history_append_host.argtypes = [H, D, S, C.POINTER(V)]
+        L.moist_history_close.argtypes = [H]
+        L.moist_restart_read.argtypes = [C.c_char_p, P, I, S]
         _lib = L
     return _lib

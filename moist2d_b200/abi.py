@@ -14,6 +14,7 @@ MOIST_ERR_CUDA = 3
 MOIST_ERR_TIMEOUT = 4
 MOIST_ERR_UNSUPPORTED = 5
 MOIST_ERR_NOMEM = 6
+MOIST_ERR_IO = 7
 
 MOIST_FLAG_TRI_NATIVE = 1
 MOIST_FLAG_TRACER_WAVEFRONT = 2

@@ -2157,6 +2157,7 @@ const char* moist_status_string(int s) {
         case MOIST_ERR_TIMEOUT: return "device wait timed out";
         case MOIST_ERR_UNSUPPORTED: return "unsupported";
         case MOIST_ERR_NOMEM: return "out of device memory";
+        case MOIST_ERR_IO: return "file error";
         default: return "unknown status";
     }
 }

@@ -29,6 +29,8 @@ def _raise(rc, ctx=None, what=""):
         raise ValueError("%s: invalid argument %s" % (what, msg))
     if rc == abi.MOIST_ERR_UNSUPPORTED:
         raise NotImplementedError("%s: %s" % (what, msg))
+    if rc == abi.MOIST_ERR_IO:
+        raise OSError("%s: %s" % (what, L.moist_io_last_error().decode()))
     raise RuntimeError("%s failed (%s): %s" % (what, L.moist_status_string(rc).decode(), msg))
 
 
@@ -343,3 +345,65 @@ class Ensemble:
         ctx = self.member(i)
         _raise(lib().moist_budget(ctx, out), ctx, "moist_budget")
         return np.array(out[:])
+
+
+class History:
+    """init_history / output_history (moist.jl:1716-1891): a NetCDF history file (classic format
+    with 64-bit offsets, written by the library) with the reference's dimensions, variables,
+    units and element type. `append(t, model)` writes one record from a Model's device State
+    (diagnostics computed on the device); `append_host(t, s, diag)` writes it from a host State
+    and the ten diagnostics as Model.history returns them."""
+
+    FIELDS = Model.HISTORY_FIELDS
+
+    def __init__(self, path, p):
+        self.p = p
+        self._cp = p.to_c()
+        self.h = C.c_void_p()
+        _raise(lib().moist_history_create(str(path).encode(), C.byref(self._cp), p.precision, C.byref(self.h)),
+               None, "moist_history_create")
+
+    def append(self, t, model):
+        _raise(lib().moist_history_append(self.h, float(t), model.ctx), model.ctx, "moist_history_append")
+
+    def append_host(self, t, s, diag):
+        p = self.p
+        keep = []
+
+        def arr(f):
+            a = np.asfortranarray(np.asarray(diag[f], dtype=p.T))
+            if a.shape != (p.Nz, p.Nx):
+                raise ValueError("diagnostic %s of shape %s, expected %s" % (f, a.shape, (p.Nz, p.Nx)))
+            keep.append(a)
+            return a.ctypes.data
+
+        d = (C.c_void_p * abi.MOIST_NDIAG)(*[arr(f) for f in self.FIELDS])
+        h = s.to_c()
+        _raise(lib().moist_history_append_host(self.h, float(t), C.byref(h), d), None, "moist_history_append_host")
+
+    def close(self):
+        if self.h:
+            rc = lib().moist_history_close(self.h)
+            self.h = C.c_void_p()
+            _raise(rc, None, "moist_history_close")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def restart_read(path, p, s=None):
+    """The restart of run_sim (moist.jl:1905-1919): the State of the last record of a history
+    file (rho, rho_u, rho_w, rho_theta = theta * rho, rho_qv, rho_qc, rho_qr = q * rho, prec;
+    periodic halo columns), into s or a new zero State. rho_qr comes from "qr" (the reference
+    reads "qc" there, moist.jl:1917)."""
+    from .params import State
+    if s is None:
+        s = State(p)
+    cp = p.to_c()
+    h = s.to_c()
+    _raise(lib().moist_restart_read(str(path).encode(), C.byref(cp), p.precision, C.byref(h)), None,
+           "moist_restart_read")
+    return s
