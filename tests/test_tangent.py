@@ -86,3 +86,18 @@ def test_golden_fixture_directions_regenerate():
     for (d_th, d_qv), ref in zip(directions(fx["seed"], fx["dirs"], 96, 512), fx["directions"]):
         assert np.isclose(float(np.sum(d_th * d_th)), ref["norm2_theta"], rtol=1e-12, atol=0.0)
         assert np.isclose(float(np.sum(d_qv * d_qv)), ref["norm2_qv"], rtol=1e-12, atol=0.0)
+
+
+def test_tangent_with_surface_fluxes_and_radiation():
+    """surface_fluxes! and gray_radiation! on (the Params defaults): the dual instantiation of
+    their bulk formulas, x^4 and tanh against central differences."""
+    p, s = small_case(np.float64, 12, 9, do_sf=True, do_rd=True)
+    assert p.do_sf and p.do_rd
+    prec_w = rain_weight(p)
+    seeds = state_seeds(p, s, 17)
+    v = direction(p, s, np.random.default_rng(19))
+    J, dJ = bind.tangent(p, s, 3, direction=v, prec_weight=prec_w, state_weight=seeds)
+    assert np.isclose(J, oracle_J(p, s, 3, prec_w, seeds), rtol=1e-14, atol=0.0)
+    fd = central(p, s, 3, prec_w, seeds, v, 1e-8)
+    assert dJ != 0.0
+    assert abs(dJ - fd) <= 1e-6 * abs(fd), (dJ, fd)
