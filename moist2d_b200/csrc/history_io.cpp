@@ -554,6 +554,8 @@ int moist_history_create(const char* path, const moist_params* p, int precision,
     if (!path || !p || !p->z || !p->zf || p->nx < 1 || p->nz < 1 || p->halo < 0 ||
         (precision != MOIST_F32 && precision != MOIST_F64))
         return MOIST_ERR_ARG;
+    // a CDF-2 variable's per-record size is a 32-bit field
+    if ((uint64_t)p->nx * (uint64_t)p->nz * (precision == MOIST_F64 ? 8u : 4u) >= 0xFFFFFFFCull) return MOIST_ERR_ARG;
     moist_history* h = new moist_history;
     h->path = path;
     h->prec = precision;

@@ -250,3 +250,14 @@ def test_history_record_from_the_device(tmp_path, T):
     r = model.restart_read(path, p)
     for fld in ("rho", "rho_u", "rho_w"):
         assert np.array_equal(getattr(r, fld)[:, c], getattr(fin, fld)[:, c]), fld
+
+
+def test_history_rejects_records_beyond_the_format(tmp_path):
+    """A CDF-2 variable's per-record size is a 32-bit field: 2^17 x 2^13 Float32 cells (4 GiB
+    per record of a (time, z, x) variable) are refused before anything is written."""
+    from moist2d_b200.params import Params
+    p = Params(np.float32, Nx=1 << 17, Nz=1 << 13, H=100.0 * (1 << 13), dz0=100.0, z_fact=1.0,
+               Lx=100.0 * (1 << 17))
+    with pytest.raises(ValueError):
+        model.History(tmp_path / "big.nc", p)
+    assert not (tmp_path / "big.nc").exists()
