@@ -350,7 +350,9 @@ const char* moist_io_last_error(void);
  * zf. precision: MOIST_F32 or MOIST_F64. */
 int moist_history_create(const char* path, const moist_params* p, int precision, moist_history** out);
 /* output_history (moist.jl:1795-1889): appends one record at time t from the context's State,
- * with the diagnostics computed on the device (moist_history_diagnostics); pres in hPa. */
+ * with the diagnostics computed on the device (moist_history_diagnostics); pres in hPa. For
+ * member m of an ensemble pass moist_batch_member(b, m) (moist_batch_step returns with the
+ * batch's work finished, so the member context holds its current State). */
 int moist_history_append(moist_history* h, double t, moist_ctx* ctx);
 /* The same record from host arrays: s in the reference layout (NULL fields are written as 0),
  * diag[f] as moist_history_diagnostics returns them. Needs no device. */

@@ -366,6 +366,11 @@ class History:
     def append(self, t, model):
         _raise(lib().moist_history_append(self.h, float(t), model.ctx), model.ctx, "moist_history_append")
 
+    def append_member(self, t, ensemble, i):
+        """One record from member i of an Ensemble (its member context, after Ensemble.step)."""
+        ctx = ensemble.member(i)
+        _raise(lib().moist_history_append(self.h, float(t), ctx), ctx, "moist_history_append")
+
     def append_host(self, t, s, diag):
         p = self.p
         keep = []

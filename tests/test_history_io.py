@@ -261,3 +261,23 @@ def test_history_rejects_records_beyond_the_format(tmp_path):
     with pytest.raises(ValueError):
         model.History(tmp_path / "big.nc", p)
     assert not (tmp_path / "big.nc").exists()
+
+
+@pytest.mark.gpu
+def test_history_record_of_an_ensemble_member(tmp_path):
+    """A record from member 1 of a two-member Ensemble after batch steps: the member's State as
+    moist_batch_download returns it."""
+    p0, s0 = bubble_case(np.float32, nx=24, nz=16)
+    p1, s1 = bubble_case(np.float32, seed=9, nx=32, nz=12)
+    path = tmp_path / "member.nc"
+    with model.Ensemble([p0, p1]) as e, model.History(path, p1) as h:
+        e.upload(0, s0)
+        e.upload(1, s1)
+        e.step(3)
+        h.append_member(6.0, e, 1)
+        fin = e.download(1, s1.copy())
+    f = {v[0]: v[4] for v in read(path)["vars"]}
+    c = slice(p1.is_ - 1, p1.ie)
+    for name, fld in (("rho", "rho"), ("rhou", "rho_u"), ("rhow", "rho_w")):
+        assert np.array_equal(f[name][0], getattr(fin, fld)[:, c]), name
+    assert np.array_equal(f["prec"][0], fin.prec[c])
