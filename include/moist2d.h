@@ -193,6 +193,17 @@ int moist_cloud_microphysics(moist_ctx* ctx);
  * d_rho_qr_sed in the context and, if d_prec is not NULL, the host array d_prec (ia, type T). */
 int moist_rain_sedimentation(moist_ctx* ctx, void* d_prec);
 
+/* surface_fluxes!(d_rho_u_sf, d_rho_theta_sf, d_rho_qv_sf, mflux, shflux, lhflux, rho, rho_u,
+ * rho_theta, rho_qv, rho_qc, rho_qr, p) (moist.jl:710-752) on the context state: fills
+ * d_rho_{u,theta,qv}_sf, mflux, shflux and lhflux (download them with moist_download_state).
+ * Its reads of rho_u[ks, is-1] and rho[ks, ie+1] see the halo columns of the last upload (or
+ * of the last RK stage's exchange). Needs halo >= 1. */
+int moist_surface_fluxes(moist_ctx* ctx);
+
+/* gray_radiation!(d_rho_theta_rd, rho, rho_theta, rho_qv, rho_qc, rho_qr, theta_ref, p)
+ * (moist.jl:776-840) on the context state with its uploaded theta_ref: fills d_rho_theta_rd. */
+int moist_gray_radiation(moist_ctx* ctx);
+
 /* implicit_correction!(rho_w, drho_w, theta, rt2pres, dt, p) (moist.jl:974-1030) for one
  * column on the device: host arrays of length nz and type T; rho_w is updated in place.
  * Only p->nz, p->dz, p->z, p->grav and p->beta_offcenter are read. */

@@ -21,7 +21,7 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_batch_profile", "moist_adjoint_run", "moist_batch_adjoint_run",
            "moist_autotune", "moist_batch_autotune", "moist_history_diagnostics", "moist_io_last_error",
            "moist_history_create", "moist_history_append", "moist_history_append_host",
-           "moist_history_close", "moist_restart_read")
+           "moist_history_close", "moist_restart_read", "moist_surface_fluxes", "moist_gray_radiation")
 
 
 def lib():
@@ -47,6 +47,8 @@ def lib():
         L.moist_compute_step.argtypes = [Ctx, C.POINTER(V), S, D, I]
         L.moist_cloud_microphysics.argtypes = [Ctx]
         L.moist_rain_sedimentation.argtypes = [Ctx, V]
+        L.moist_surface_fluxes.argtypes = [Ctx]
+        L.moist_gray_radiation.argtypes = [Ctx]
         L.moist_implicit_correction.argtypes = [P, I, I, V, V, V, V, D]
         L.moist_eval_helper.argtypes = [P, I, I, I, C.POINTER(D), C.POINTER(D)]
         L.moist_budget.argtypes = [Ctx, C.POINTER(D)]

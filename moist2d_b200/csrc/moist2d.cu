@@ -47,6 +47,8 @@ struct CtxBase {
     virtual int compute_step(const void* const phys[6], const moist_state_host* s0, double dt, int ns) = 0;
     virtual int microphysics() = 0;
     virtual int sedimentation(void* d_prec) = 0;
+    virtual int surface_fluxes() = 0;
+    virtual int gray_radiation() = 0;
     virtual int budget(double out[4]) = 0;
     virtual int time_steps(int nsteps, float* ms) = 0;
     virtual int profile(int nsteps, float* total_ms, float* group_ms, long long* group_launches) = 0;
@@ -916,6 +918,26 @@ struct Ctx : CtxBase {
             CK(cudaStreamSynchronize(st));
             std::memcpy((T*)host_d_prec + halo, tmp.data() + halo, nx * sizeof(T));
         }
+        return finish();
+    }
+
+    // surface_fluxes! (moist.jl:710-752) on the current state alone: the halo reads
+    // rho_u[ks, is-1] and rho[ks, ie+1] are the uploaded halo columns (or the last exchange's)
+    int surface_fluxes() override {
+        if (halo < 1) return set_err(owner, MOIST_ERR_ARG, "surface_fluxes! reads one halo column: halo >= 1");
+        CK(reset_err());
+        k_surface_fluxes<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, cur, halo_vals, halo_vals + 1, d_u_sf, d_th_sf,
+                                                          d_qv_sf, mflux, shflux, lhflux, err);
+        CKL();
+        return finish();
+    }
+
+    // gray_radiation! (moist.jl:776-840) on the current state alone, with the uploaded theta_ref
+    int gray_radiation() override {
+        CK(reset_err());
+        k_gray_radiation<T><<<cdiv(nx, 128), 128, 0, st>>>(dp, cur, theta_ref, lw_up, lw_dn, d_th_rd, err);
+        CKL();
+        rd_dirty = true;
         return finish();
     }
 
@@ -2389,6 +2411,16 @@ int moist_rain_sedimentation(moist_ctx* c, void* d_prec) {
     if (!c) return MOIST_ERR_ARG;
     CTX_DEVICE(c);
     return c->impl->sedimentation(d_prec);
+}
+int moist_surface_fluxes(moist_ctx* c) {
+    if (!c) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
+    return c->impl->surface_fluxes();
+}
+int moist_gray_radiation(moist_ctx* c) {
+    if (!c) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
+    return c->impl->gray_radiation();
 }
 int moist_budget(moist_ctx* c, double out[4]) {
     if (!c || !out) return MOIST_ERR_ARG;

@@ -186,6 +186,25 @@ def cloud_microphysics(s, p):
     return s
 
 
+def surface_fluxes(s, p):
+    """surface_fluxes!(d_rho_u_sf, d_rho_theta_sf, d_rho_qv_sf, mflux, shflux, lhflux, rho, ...,
+    p): fills those six fields of s (the halo columns of s are the reads at is-1 and ie+1)."""
+    with Model(p) as m:
+        m.upload(s)
+        _raise(lib().moist_surface_fluxes(m.ctx), m.ctx, "moist_surface_fluxes")
+        m.download(s)
+    return s
+
+
+def gray_radiation(s, p):
+    """gray_radiation!(d_rho_theta_rd, rho, ..., theta_ref, p): fills s.d_rho_theta_rd."""
+    with Model(p) as m:
+        m.upload(s)
+        _raise(lib().moist_gray_radiation(m.ctx), m.ctx, "moist_gray_radiation")
+        m.download(s)
+    return s
+
+
 def rain_sedimentation(s, p):
     """rain_sedimentation!(d_rho_qr_sed, d_prec, rho_qr, rho, p): fills s.d_rho_qr_sed and
     returns d_prec."""

@@ -36,6 +36,8 @@ def lib():
         L.oracle_compute_step.argtypes = [P, I, I, C.POINTER(V), S, S, D, I]
         L.oracle_cloud_microphysics.argtypes = [P, I, S]
         L.oracle_rain_sedimentation.argtypes = [P, I, S, V]
+        L.oracle_surface_fluxes.argtypes = [P, I, S]
+        L.oracle_gray_radiation.argtypes = [P, I, S]
         L.oracle_implicit_correction.argtypes = [P, I, I, V, V, V, V, D]
         L.oracle_eval_helper.argtypes = [P, I, I, I, C.POINTER(D), C.POINTER(D)]
         L.oracle_limited_flux.argtypes = [P, I, I, V, V, V, I, I, C.POINTER(D)]
@@ -142,6 +144,20 @@ def cloud_microphysics(s, p):
     cp = p.to_c()
     h = s.to_c()
     _check(lib().oracle_cloud_microphysics(C.byref(cp), p.precision, C.byref(h)))
+
+
+def surface_fluxes(s, p):
+    """surface_fluxes!(...) on s (moist.jl:710-752)."""
+    cp = p.to_c()
+    h = s.to_c()
+    _check(lib().oracle_surface_fluxes(C.byref(cp), p.precision, C.byref(h)))
+
+
+def gray_radiation(s, p):
+    """gray_radiation!(...) on s with s.theta_ref (moist.jl:776-840)."""
+    cp = p.to_c()
+    h = s.to_c()
+    _check(lib().oracle_gray_radiation(C.byref(cp), p.precision, C.byref(h)))
 
 
 def rain_sedimentation(s, p):

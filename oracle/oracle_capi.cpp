@@ -114,6 +114,29 @@ int compute_step_t(const moist_params* cp, const void* const phys[6], moist_stat
 }
 
 template <class T>
+int sf_t(const moist_params* cp, moist_state_host* hs) {
+    const Par<T> p = Par<T>::from_c(*cp);
+    State<T> s(p);
+    load(s, hs);
+    surface_fluxes(s.d_rho_u_sf.data(), s.d_rho_theta_sf.data(), s.d_rho_qv_sf.data(), s.mflux.data(),
+                   s.shflux.data(), s.lhflux.data(), s.rho.a(), s.rho_u.a(), s.rho_theta.a(), s.rho_qv.a(),
+                   s.rho_qc.a(), s.rho_qr.a(), p);
+    store(s, hs);
+    return -1;
+}
+
+template <class T>
+int rd_t(const moist_params* cp, moist_state_host* hs) {
+    const Par<T> p = Par<T>::from_c(*cp);
+    State<T> s(p);
+    load(s, hs);
+    gray_radiation(s.d_rho_theta_rd.a(), s.rho.a(), s.rho_theta.a(), s.rho_qv.a(), s.rho_qc.a(), s.rho_qr.a(),
+                   s.theta_ref.data(), p);
+    store(s, hs);
+    return -1;
+}
+
+template <class T>
 int micro_t(const moist_params* cp, moist_state_host* hs) {
     const Par<T> p = Par<T>::from_c(*cp);
     State<T> s(p);
@@ -313,6 +336,16 @@ int oracle_compute_step(const moist_params* cp, int prec, int tri64, const void*
 int oracle_cloud_microphysics(const moist_params* cp, int prec, moist_state_host* s) {
     if (!params_ok(cp) || !s) return -2;
     return prec == MOIST_F32 ? micro_t<float>(cp, s) : micro_t<double>(cp, s);
+}
+
+int oracle_surface_fluxes(const moist_params* cp, int prec, moist_state_host* s) {
+    if (!params_ok(cp) || !s || cp->halo < 1) return -2;
+    return prec == MOIST_F32 ? sf_t<float>(cp, s) : sf_t<double>(cp, s);
+}
+
+int oracle_gray_radiation(const moist_params* cp, int prec, moist_state_host* s) {
+    if (!params_ok(cp) || !s) return -2;
+    return prec == MOIST_F32 ? rd_t<float>(cp, s) : rd_t<double>(cp, s);
 }
 
 int oracle_rain_sedimentation(const moist_params* cp, int prec, moist_state_host* s, void* d_prec) {
