@@ -2229,7 +2229,7 @@ int moist_ctx_create(const moist_params* p, int precision, int flags, moist_ctx*
 
 int moist_ctx_destroy(moist_ctx* c) {
     if (!c) return MOIST_ERR_ARG;
-    cudaSetDevice(c->device);
+    cudaSetDevice(c->device);  // best effort: the context is released either way
     delete c->impl;
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -2242,7 +2242,7 @@ const char* moist_last_error(const moist_ctx* c) { return c ? c->err.c_str() : "
 
 int moist_batch_destroy(moist_batch* b) {
     if (!b) return MOIST_ERR_ARG;
-    cudaSetDevice(b->device);
+    cudaSetDevice(b->device);  // best effort: the batch is released either way
     delete b->impl;
     for (moist_ctx* c : b->members) moist_ctx_destroy(c);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -2321,7 +2321,7 @@ int moist_batch_download(moist_batch* b, int member, moist_state_host* s) {
 int moist_batch_adjoint_run(moist_batch* b, int nsteps, int ckpt_every, const moist_adjoint_seed* seeds,
                             moist_adjoint_grad* out, int nthreads) {
     if (!b) return MOIST_ERR_ARG;
-    cudaSetDevice(b->device);
+    if (cudaSetDevice(b->device) != cudaSuccess) return MOIST_ERR_CUDA;
     return b->impl->adjoint(nsteps, ckpt_every, seeds, out, nthreads);
 }
 
@@ -2342,7 +2342,7 @@ int moist_autotune(moist_ctx* c, int nsteps, char* report, size_t report_len) {
 
 int moist_batch_autotune(moist_batch* b, int nsteps, char* report, size_t report_len) {
     if (!b) return MOIST_ERR_ARG;
-    cudaSetDevice(b->device);
+    if (cudaSetDevice(b->device) != cudaSuccess) return MOIST_ERR_CUDA;
     std::string rep;
     const int r = b->impl->autotune(nsteps, rep);
     if (report && report_len) snprintf(report, report_len, "%s", rep.c_str());
