@@ -281,3 +281,31 @@ def test_history_record_of_an_ensemble_member(tmp_path):
     for name, fld in (("rho", "rho"), ("rhou", "rho_u"), ("rhow", "rho_w")):
         assert np.array_equal(f[name][0], getattr(fin, fld)[:, c]), name
     assert np.array_equal(f["prec"][0], fin.prec[c])
+
+
+@pytest.mark.parametrize("T", [np.float32, np.float64], ids=["f32", "f64"])
+def test_history_record_of_the_oracle_run_and_restart_continuation(tmp_path, T):
+    """The oracle's own run: a record written from its State and its output_history diagnostics
+    holds them as output_history would (pres in hPa); restarting from it and stepping on gives
+    the uninterrupted run's State to within the rounding of the restart's theta * rho and
+    q * rho products, as the reference's restart does."""
+    from oracle import bind
+    p, s = bubble_case(T, nx=24, nz=16)
+    bind.rk3_step(s, p, 4, tri64=True)
+    d = bind.history_diag(s, p)
+    path = tmp_path / "oracle.nc"
+    write(path, p, [(8.0, s, {f: d[f] for f in DIAG})])
+    f = {v[0]: v[4] for v in read(path)["vars"]}
+    c = slice(p.is_ - 1, p.ie)
+    assert np.array_equal(f["pres"][0], d["pres"] / T(100.0))
+    assert np.array_equal(f["theta"][0], d["theta"]) and np.array_equal(f["rho"][0], s.rho[:, c])
+    r = model.restart_read(path, p)
+    # interiors as stored; the halos are the restart's exchange, not the step's last one
+    assert np.array_equal(r.rho[:, c], s.rho[:, c]) and np.array_equal(r.rho_u[:, c], s.rho_u[:, c])
+    direct = s.copy()
+    bind.rk3_step(direct, p, 3, tri64=True)
+    bind.rk3_step(r, p, 3, tri64=True)
+    tol = 1e-4 if T is np.float32 else 1e-12
+    for fld in ("rho", "rho_u", "rho_w", "rho_theta", "rho_qv"):
+        x, y = getattr(r, fld)[:, c].astype(np.float64), getattr(direct, fld)[:, c].astype(np.float64)
+        assert np.linalg.norm(x - y) <= tol * np.linalg.norm(y), fld
