@@ -8,6 +8,10 @@ theta = rho_theta / rho, u and w at the cell centres (as output_history forms th
 moist.jl:1797-1810), qv, qc, qr (mixing ratios) and the accumulated surface rain prec (also
 the relative error of its domain total).
 
+A run that stops with "NaN detected in ..." before N steps (the 2048 x 128 sounding workload does
+near step 900 in both precisions) is reported as such, per precision, with the step at which the
+end-of-stage check fired, instead of a comparison.
+
     python -m moist2d_b200.precision --workload bubble --steps 1800
 """
 import argparse
@@ -46,18 +50,28 @@ def compare(d32, d64):
 
 
 def run(builder, nsteps):
-    """builder(T) -> (Params, State); returns the per-field comparison after nsteps."""
+    """builder(T) -> (Params, State); returns the per-field comparison after nsteps, or
+    {"nan": {precision: {"step": n, "error": message}}} if a run stopped at a NaN."""
     from moist2d_b200 import model
     from moist2d_b200.params import exchange_halo
-    diags = {}
+    diags, nan = {}, {}
     for T in (np.float32, np.float64):
         p, s = builder(T)
         with model.Model(p) as m:
             m.upload(s)
-            m.step(nsteps)
+            done = 0
+            try:
+                for _ in range(nsteps):  # one large step per call: the same launches as m.step(nsteps)
+                    m.step(1)
+                    done += 1
+            except FloatingPointError as e:
+                nan[np.dtype(T).name] = {"step": done + 1, "error": str(e)}
+                continue
             m.download(s)
         exchange_halo(s.rho_u, p)
         diags[T] = diagnostics(s, p)
+    if nan:
+        return {"nan": nan}
     return compare(diags[np.float32], diags[np.float64])
 
 
