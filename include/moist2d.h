@@ -11,8 +11,7 @@
  *                                                    moist.jl:974-1030   -> moist_implicit_correction
  *   device(x)  (the CuArray hook)                    moist.jl:227-228    -> moist_ctx_create + moist_upload_state
  *   output_history(...) field computation            moist.jl:1795-1843  -> moist_history_diagnostics
- * A Julia caller binds them with ccall; Python binds them with ctypes
- * (moist2d_b200/_lib.py).
+ * A Julia caller binds them with ccall; Python binds them with ctypes (moist2d_b200/_lib.py).
  *
  * Conventions
  *  - Every call returns an int status (MOIST_OK = 0). Errors the reference raises as Julia
@@ -211,23 +210,29 @@ int moist_implicit_correction(const moist_params* p, int precision, int flags, v
                               const void* drho_w, const void* theta, const void* rt2pres,
                               double dt);
 
-/* Allocation-free variant of moist_implicit_correction for callers that must not have a
- * library allocate device memory behind them (a host that routes all device memory through its
- * own pool, such as Julia's CUDA.jl; code running while its stream is captured into a CUDA
- * graph; fixed device-memory budgets). It has no counterpart in the reference.
+/* Allocation-free variant of moist_implicit_correction. It has no counterpart in the
+ * reference; it is for callers that must not have a library allocate device memory behind
+ * them: a host whose device memory all comes from its own pool (Julia's CUDA.jl, which
+ * reclaims pool memory under pressure), a host that reserves a fixed device-memory budget up
+ * front and cannot meet an out-of-memory failure mid-run, and a host that keeps other streams
+ * busy and cannot afford cudaFree, which waits for the whole device.
  * Solves implicit_correction! for ncols columns at once. rho_w (updated in place), drho_w,
  * theta and rt2pres are DEVICE arrays of type T laid out (nz, ncols) with z fastest (column j
- * starts at element j*nz); p->dz, p->z (host) give the grid; p->grav and p->beta_offcenter
- * are read. The work is queued on `stream` (a cudaStream_t, NULL = default stream) and the
- * call returns without waiting. It calls no cudaMalloc or cudaFree: its scratch is one
- * fixed array of MOIST_NOALLOC_SCRATCH_BYTES per device, held by every GPU that loads the
- * library until exit. Limit: 2*(nz-1)*ncols*sizeof(elimination type) + 2*nz*sizeof(T)
- * (rounded up to 256) <= MOIST_NOALLOC_SCRATCH_BYTES (e.g. 2048 columns of 128 levels with the
- * FP64 elimination); larger calls return MOIST_ERR_ARG and write the reason to err (if not
- * NULL). The first call on a device looks up the scratch array's device address; make that
- * first call before any stream capture. All calls share the array and nothing in it needs to
- * start at zero (every element is written before it is read); calls that overlap on the same
- * GPU (for example on two streams) race on it, so serialise them. */
+ * starts at element j*nz); p->dz, p->z (host) give the grid and travel in the kernel's
+ * parameter block; p->grav and p->beta_offcenter are read. The work is queued on `stream` (a
+ * cudaStream_t, NULL = default stream) and the call returns without waiting; it issues no
+ * memory copy. It calls no cudaMalloc or cudaFree: its scratch is one fixed array of
+ * MOIST_NOALLOC_SCRATCH_BYTES per device, held by every GPU that loads the library until exit.
+ * Limits: nz <= MOIST_NOALLOC_MAX_NZ, and 2*(nz-1)*ncols*sizeof(elimination type) <=
+ * MOIST_NOALLOC_SCRATCH_BYTES (e.g. 2048 columns of 128 levels with the FP64 elimination);
+ * larger calls return MOIST_ERR_ARG before queuing anything and write the reason to err (if not
+ * NULL). The first call on a device looks up the scratch array's device address with that
+ * device current and keeps it for the life of the process: make that first call before any
+ * stream capture, and make no call after a cudaDeviceReset of the device. All calls share the
+ * array and keep the last call's contents; nothing in it needs to start at zero (every element
+ * is written before it is read). Calls that overlap on the same GPU (for example on two
+ * streams) race on it, so serialise them. */
+#define MOIST_NOALLOC_MAX_NZ 1024
 #define MOIST_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)
 int moist_implicit_correction_noalloc(const moist_params* p, int precision, int flags, int ncols,
                                       void* rho_w, const void* drho_w, const void* theta,
@@ -283,7 +288,7 @@ const char* moist_batch_last_error(const moist_batch* b);
 int moist_batch_nan_member(const moist_batch* b);
 
 /* ---- Adjoint (no counterpart in the reference, which has no derivatives; a Julia caller
- * exposes it as the pullback of a ChainRulesCore.rrule around rk3_step!, see INTEGRATION.md).
+ * exposes it as the pullback of a ChainRulesCore.rrule around rk3_step!).
  *
  * moist_adjoint_run advances the context State nsteps large steps (as moist_rk3_step does, the
  * context is left at the final State) and returns the gradient of the objective
@@ -410,6 +415,15 @@ int moist_step_profile(moist_ctx* ctx, int nsteps, float* total_ms, float* group
  * that reached their bitwise fixed point after p passes; the counters are reset.
  * MOIST_ERR_UNSUPPORTED when the context runs the wavefront sweep. */
 int moist_tracer_pass_counts(moist_ctx* ctx, int* counts, int n);
+
+/* Bound of the device-side waits of the context's kernels (no counterpart in the reference,
+ * whose threads never wait on one another). The tiled tracer sweep's blocks wait for each
+ * other between repair passes; every such wait gives up after `cycles` SM clock cycles
+ * (cycles <= 0 restores the default, about two seconds), and the step then returns
+ * MOIST_ERR_TIMEOUT, leaving the context's State undefined (upload a State before stepping
+ * again). Meant for tests of that path. MOIST_ERR_UNSUPPORTED when the context's tracer sweep
+ * does not wait (the streaming or wavefront sweep). */
+int moist_set_wait_limit(moist_ctx* ctx, long long cycles);
 
 /* Stream of the context (a cudaStream_t), for callers that order their own work after it. */
 void* moist_stream(moist_ctx* ctx);

@@ -21,7 +21,8 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_batch_profile", "moist_adjoint_run", "moist_batch_adjoint_run",
            "moist_autotune", "moist_batch_autotune", "moist_history_diagnostics", "moist_io_last_error",
            "moist_history_create", "moist_history_append", "moist_history_append_host",
-           "moist_history_close", "moist_restart_read", "moist_surface_fluxes", "moist_gray_radiation")
+           "moist_history_close", "moist_restart_read", "moist_surface_fluxes", "moist_gray_radiation",
+           "moist_set_wait_limit")
 
 
 def lib():
@@ -59,6 +60,7 @@ def lib():
         L.moist_rk3_step_host.argtypes = [Ctx, S, I]
         L.moist_set_device.argtypes = [I]
         L.moist_tracer_pass_counts.argtypes = [Ctx, C.POINTER(I), I]
+        L.moist_set_wait_limit.argtypes = [Ctx, C.c_longlong]
         L.moist_implicit_correction_noalloc.argtypes = [P, I, I, I, V, V, V, V, D, V, C.c_char_p,
                                                         C.c_size_t]
         L.moist_step_profile.argtypes = [Ctx, I, C.POINTER(C.c_float), C.POINTER(C.c_float),

@@ -54,6 +54,7 @@ struct CtxBase {
     virtual int profile(int nsteps, float* total_ms, float* group_ms, long long* group_launches) = 0;
     virtual int rk3_host(moist_state_host* s, int nsteps) = 0;
     virtual int pass_counts(int* counts, int n) = 0;
+    virtual int set_wait_limit(long long cycles) = 0;
     virtual int adjoint_run(int nsteps, int ckpt, const moist_adjoint_seed* seed, moist_adjoint_grad* out) = 0;
     virtual int autotune(int nsteps, std::string& report) = 0;
     virtual int history(void* const out[MOIST_NDIAG], double summary[6]) = 0;
@@ -442,6 +443,7 @@ struct Ctx : CtxBase {
         int clk = 0;
         CK(cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, dev));  // kHz
         tctl.spin_limit = (long long)clk * 1000LL * 2;                 // about two seconds
+        wait_default = tctl.spin_limit;
         use_tiles = true;
         return MOIST_OK;
     }
@@ -452,8 +454,14 @@ struct Ctx : CtxBase {
         CK(cudaMemcpyAsync(h, err, sizeof h, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         CKL();
-        if (h[2] != 0)
+        if (h[2] != 0) {
+            // the blocks that gave up left the barrier words mid-count: clear them and the flag
+            // so that the context can step again (from a State uploaded anew)
+            if (tctl.bar) CK(cudaMemsetAsync(tctl.bar, 0, 2 * sizeof(unsigned), st));
+            CK(reset_err());
+            CK(cudaStreamSynchronize(st));
             return set_err(owner, MOIST_ERR_TIMEOUT, "a grid barrier of the tiled tracer sweep timed out");
+        }
         if (h[0] != INT_MAX) {
             owner->nan_field = h[0];
             static const char* names[12] = {"rho", "rho_u", "rho_w", "rho_theta", "rho_qv", "rho_qc", "rho_qr",
@@ -851,6 +859,16 @@ struct Ctx : CtxBase {
         }
         if (total_ms) *total_ms = tot;
         return finish();
+    }
+
+    // bound of every device-side wait of the context's kernels, in SM clock cycles (<= 0: the
+    // default of about two seconds)
+    long long wait_default = 0;
+    int set_wait_limit(long long cycles) override {
+        if (!use_tiles)
+            return set_err(owner, MOIST_ERR_UNSUPPORTED, "the context runs no kernel that waits on other blocks");
+        tctl.spin_limit = cycles > 0 ? cycles : wait_default;
+        return MOIST_OK;
     }
 
     int pass_counts(int* counts, int n) override {
@@ -1653,6 +1671,9 @@ struct BatchImpl : BatchBase {
     int col_threads = BATCH_COL_THREADS;  // threads per block of the per-column kernels
     bool sub_strips = false;               // factorisation and substep over column strips instead
     int stream_minb = 1;                   // register bound of the streaming tracer sweep (1 or 2)
+    // per-column substep body: 0 b_substep_col (64 registers), 1 and 2 b_substep_col_pf (loads one
+    // level ahead; 128 and 85 registers)
+    int sub_form = 1;
     std::vector<std::array<T*, 8>> tune_save;  // the members' States saved by autotune
     std::vector<T*> tune_halo;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
@@ -1763,6 +1784,12 @@ struct BatchImpl : BatchBase {
                 if (sub_strips)
                     k_batched<BSub<T, TT>, FSubStrip<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
                         s.items, (const BSub<T, TT>*)s.args, FSubStrip<T, TT>{});
+                else if (sub_form == 1)
+                    k_batched<BSub<T, TT>, FSubPf<T, TT>, 2><<<s.nitems, s.block, s.smem, st>>>(
+                        s.items, (const BSub<T, TT>*)s.args, FSubPf<T, TT>{});
+                else if (sub_form == 2)
+                    k_batched<BSub<T, TT>, FSubPf<T, TT>, 3><<<s.nitems, s.block, s.smem, st>>>(
+                        s.items, (const BSub<T, TT>*)s.args, FSubPf<T, TT>{});
                 else
                     k_batched<BSub<T, TT>, FSub<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
                         s.items, (const BSub<T, TT>*)s.args, FSub<T, TT>{});
@@ -1997,7 +2024,16 @@ struct BatchImpl : BatchBase {
         if (int r = dalloc(&hb, 1)) return r;
         unsigned long long h0 = 0;
         bool first = true;
-        for (int ct : {0, 32, 64, 128, 256}) {
+        int bform = sub_form;
+        struct SubCand {
+            int ct, form;
+        };
+        std::vector<SubCand> sub_cands{{0, 0}};
+        for (int form : {1, 2, 0})
+            for (int ct : {32, 64, 128, 256}) sub_cands.push_back({ct, form});
+        for (const SubCand& sc : sub_cands) {
+            const int ct = sc.ct;
+            sub_form = sc.form;
             if (int r = set_col_threads(ct)) return r;
             if (int r = copy_all(false)) return r;
             float ms = 0.f;
@@ -2017,20 +2053,23 @@ struct BatchImpl : BatchBase {
                 h0 = h;
                 first = false;
             } else if (h != h0) {
-                return set_berr(owner, MOIST_ERR_CUDA, "autotune: column block %d gives other States than column strips",
-                                ct);
+                return set_berr(owner, MOIST_ERR_CUDA,
+                                "autotune: column block %d form %d gives other States than column strips", ct, sc.form);
             }
             ms /= nsteps;
             if (ct == 0)
                 snprintf(buf, sizeof buf, "%scolumn strips: %.2f ms", report.empty() ? "" : "; ", ms);
             else
-                snprintf(buf, sizeof buf, "%scolumn block %d: %.2f ms", report.empty() ? "" : "; ", ct, ms);
+                snprintf(buf, sizeof buf, "%scolumn block %d form %d: %.2f ms", report.empty() ? "" : "; ", ct,
+                         sc.form, ms);
             report += buf;
             if (ms < best) {
                 best = ms;
                 bct = ct;
+                bform = sc.form;
             }
         }
+        sub_form = bform;
         // then, with that form, the register bound of the streaming tracer sweep
         int bmb = stream_minb;
         float best_mb = 1e30f;
@@ -2068,7 +2107,8 @@ struct BatchImpl : BatchBase {
         if (bct == 0)
             snprintf(buf, sizeof buf, " -> column strips, tracer bound %d (%.2f ms per step)", bmb, best);
         else
-            snprintf(buf, sizeof buf, " -> column block %d, tracer bound %d (%.2f ms per step)", bct, bmb, best);
+            snprintf(buf, sizeof buf, " -> column block %d form %d, tracer bound %d (%.2f ms per step)", bct, sub_form,
+                     bmb, best);
         report += buf;
         return MOIST_OK;
     }
@@ -2454,6 +2494,12 @@ int moist_tracer_pass_counts(moist_ctx* c, int* counts, int n) {
     if (!c || !counts || n < 0) return MOIST_ERR_ARG;
     CTX_DEVICE(c);
     return c->impl->pass_counts(counts, n);
+}
+
+int moist_set_wait_limit(moist_ctx* c, long long cycles) {
+    if (!c) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
+    return c->impl->set_wait_limit(cycles);
 }
 
 int moist_step_profile(moist_ctx* c, int nsteps, float* total_ms, float* group_ms, long long* group_launches) {
