@@ -1,14 +1,16 @@
 // noalloc.cu - an allocation-free entry point: the vertically implicit w-p column solve
 // (implicit_correction!) for many columns at once, on device buffers the caller owns.
 //
-// Who needs it: callers that must not allocate device memory themselves. A Julia host that
-// routes every device allocation through CUDA.jl's memory pool, a code path that runs while
-// its stream is being captured into a CUDA graph (cudaMalloc is not allowed there), and
-// embedded users with a fixed device-memory budget cannot let a library call cudaMalloc
-// behind their back. moist_implicit_correction allocates its column buffers per call; this
-// variant allocates nothing: its scratch (the modified super-diagonal and right-hand side of
-// the elimination, plus the grid vectors) lives in one file-scope __device__ array of fixed
-// size that every GPU loading the library holds until the process exits.
+// Who needs it: callers that must not have a library allocate device memory behind them. A
+// Julia host routes every device allocation through CUDA.jl's memory pool and counts on it to
+// reclaim memory under pressure; a host with a fixed device-memory budget reserves all of it
+// up front and cannot meet an out-of-memory failure in the middle of a run; and a host that
+// keeps other streams busy cannot afford cudaFree, which waits for the whole device.
+// moist_implicit_correction allocates its column buffers on every call; this variant
+// allocates nothing. The grid vectors travel in the kernel's parameter block (so the call
+// issues no host-to-device copy either), and the scratch of the elimination (the modified
+// super-diagonal and right-hand side of every column) lives in one file-scope __device__ array
+// of fixed size that every GPU loading the library holds until the process exits.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -22,6 +24,14 @@ namespace {
 
 constexpr size_t kScratchDoubles = MOIST_NOALLOC_SCRATCH_BYTES / sizeof(double);
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
+
+// the grid vectors dz and z, passed by value in the kernel's parameter block (at most
+// MOIST_NOALLOC_MAX_NZ levels: 16 KiB in Float64, within the 32 KiB parameter limit)
+template <class T>
+struct ColumnGrid {
+    T dz[MOIST_NOALLOC_MAX_NZ];
+    T z[MOIST_NOALLOC_MAX_NZ];
+};
 
 // device address of g_noalloc_scratch, looked up once per device with that device current
 constexpr int kMaxDevices = 64;
@@ -40,10 +50,12 @@ void put_msg(char* err, size_t errlen, const char* msg) {
 // solve_tridiagonal! (moist.jl:952-971), with the elimination in TT.
 template <class T, class TT>
 __global__ void k_implicit_columns_noalloc(int nz, int ncols, T grav, T beta, T* rho_w, const T* drho_w,
-                                          const T* theta, const T* rt2pres, T dt, const T* dz, const T* z,
-                                          TT* work) {
+                                          const T* theta, const T* rt2pres, T dt,
+                                          const __grid_constant__ ColumnGrid<T> grid, TT* work) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ncols) return;
+    const T* dz = grid.dz;  // every thread reads the same level at the same time: broadcast
+    const T* z = grid.z;
     const int n = nz - 1, ke = nz - 1;
     T* w = rho_w + (size_t)j * nz;
     const T* dw = drho_w + (size_t)j * nz;
@@ -95,32 +107,27 @@ template <class T, class TT>
 int run_noalloc(const moist_params* p, int ncols, void* rho_w, const void* drho_w, const void* theta,
                 const void* rt2pres, double dt, cudaStream_t st, double* base, char* err, size_t errlen) {
     const int nz = p->nz;
-    // scratch layout: [grid: dz (T, nz), z (T, nz), padded to 256 B][elimination work (TT, 2 (nz-1) ncols)]
-    const size_t grid_bytes = ((2 * (size_t)nz * sizeof(T)) + 255) / 256 * 256;
+    // scratch: the elimination work (TT, 2 (nz-1) per column)
     const size_t work_bytes = 2 * (size_t)(nz - 1) * ncols * sizeof(TT);
-    if (grid_bytes + work_bytes > MOIST_NOALLOC_SCRATCH_BYTES) {
+    if (work_bytes > MOIST_NOALLOC_SCRATCH_BYTES) {
         char msg[256];
         std::snprintf(msg, sizeof msg,
                       "moist_implicit_correction_noalloc: %d columns of %d levels need %zu scratch bytes, "
                       "more than the fixed %d-byte scratch array",
-                      ncols, nz, grid_bytes + work_bytes, (int)MOIST_NOALLOC_SCRATCH_BYTES);
+                      ncols, nz, work_bytes, (int)MOIST_NOALLOC_SCRATCH_BYTES);
         put_msg(err, errlen, msg);
         return MOIST_ERR_ARG;
     }
-    T* gdz = reinterpret_cast<T*>(base);
-    T* gz = gdz + nz;
-    TT* work = reinterpret_cast<TT*>(reinterpret_cast<char*>(base) + grid_bytes);
-    cudaError_t e = cudaMemcpyAsync(gdz, p->dz, nz * sizeof(T), cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(gz, p->z, nz * sizeof(T), cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) {
-        put_msg(err, errlen, cudaGetErrorString(e));
-        return MOIST_ERR_CUDA;
-    }
+    ColumnGrid<T> grid;
+    std::memset(&grid, 0, sizeof grid);
+    std::memcpy(grid.dz, p->dz, nz * sizeof(T));
+    std::memcpy(grid.z, p->z, nz * sizeof(T));
+    TT* work = reinterpret_cast<TT*>(base);
     const int threads = 128;
     k_implicit_columns_noalloc<T, TT><<<(ncols + threads - 1) / threads, threads, 0, st>>>(
         nz, ncols, (T)p->grav, (T)p->beta_offcenter, (T*)rho_w, (const T*)drho_w, (const T*)theta,
-        (const T*)rt2pres, (T)dt, gdz, gz, work);
-    e = cudaGetLastError();
+        (const T*)rt2pres, (T)dt, grid, work);
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         put_msg(err, errlen, cudaGetErrorString(e));
         return MOIST_ERR_CUDA;
@@ -141,6 +148,13 @@ int moist_implicit_correction_noalloc(const moist_params* p, int precision, int 
         put_msg(err, errlen, "moist_implicit_correction_noalloc: invalid argument");
         return MOIST_ERR_ARG;
     }
+    if (p->nz > MOIST_NOALLOC_MAX_NZ) {
+        char msg[160];
+        std::snprintf(msg, sizeof msg, "moist_implicit_correction_noalloc: nz = %d is above the limit of %d levels",
+                      p->nz, (int)MOIST_NOALLOC_MAX_NZ);
+        put_msg(err, errlen, msg);
+        return MOIST_ERR_ARG;
+    }
     if (precision != MOIST_F32 && precision != MOIST_F64) {
         put_msg(err, errlen, "moist_implicit_correction_noalloc: unknown precision");
         return MOIST_ERR_ARG;
@@ -154,8 +168,10 @@ int moist_implicit_correction_noalloc(const moist_params* p, int precision, int 
     }
     void* base;
     {
-        // first call on this device: look up the scratch array's device address (the host-side
-        // symbol is only a stand-in and must never reach a kernel)
+        // first call on this device: look up the scratch array's device address with the device
+        // current (the host-side symbol is only a stand-in and must never reach a kernel). The
+        // address is kept for the life of the process; it is not looked up again after a
+        // cudaDeviceReset, so no call may follow a reset of the device.
         std::lock_guard<std::mutex> lock(g_scratch_mutex);
         if (!g_scratch_addr[dev]) {
             void* ptr = nullptr;
