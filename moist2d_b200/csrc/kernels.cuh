@@ -628,6 +628,209 @@ __device__ __forceinline__ void b_substep_col(DevParams<T> p, SubArgs<T, TT> a, 
 }
 
 
+// b_substep_col with its loads issued one level ahead. A column walk spends most of its time
+// waiting for each level's loads: the loads of level k + 1 cannot move above the stores of level
+// k to the arrays the walk updates in place (rho_p, mfx, rt_out, ...), so every level waits a
+// full memory latency. Here every input of the next level is read into registers before the
+// current level's arithmetic and stores (the addresses differ, so the values are those the
+// walk would read later), and the values a level shares with its neighbour level (rho_w_p,
+// rt2pres going up; theta, s.rho_w going down) stay in registers. The arithmetic is that of
+// b_substep_col, operation for operation.
+template <class T, class TT>
+struct SubUpLevel {
+    T rt_m, rt_c, rt_p, ro_m, ro_c, ro_p, r2_m, r2_c, r2_p, ru_m, ru_c, Ru_m, Ru_c;
+    T mfx, Rrho, rhop, th_c, th_p, th_m, Rrt;
+    T Rrw, rwp, ta, tb, tc;  // face k: R_rho_w, rho_w_p and the factors (used by level k + 1)
+    TT piv;
+};
+
+template <class T, class TT>
+__device__ __forceinline__ void b_substep_col_pf(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T, double fact_tp64,
+                                                 const int* err, int bx) {
+    const int i = bx * blockDim.x + threadIdx.x;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    if (i >= nx || halted(err)) return;
+    const T dx = p.dx, EPS = p.EPS;
+    const T* dz = p.dz;
+    const T* z = p.z;
+    const int im = wrapx(i - 1, nx), ip = wrapx(i + 1, nx);
+    const int ke = nz - 1, n = nz - 1;
+    const T fact_tpT = T(0.5) * (T(1.0) + p.beta);
+    const T fact_tmT = T(0.5) * (T(1.0) - p.beta);
+    const T fact = fact_tmT / fact_tpT;
+    using L = SubUpLevel<T, TT>;
+    auto load_up = [&](int k, L& v) {
+        const size_t c = MOIST_IDX(k, i), cm = MOIST_IDX(k, im), cp = MOIST_IDX(k, ip);
+        v.rt_m = ro(a.rt_in + cm);
+        v.rt_c = ro(a.rt_in + c);
+        v.rt_p = ro(a.rt_in + cp);
+        v.ro_m = ro(a.rt_old + cm);
+        v.ro_c = ro(a.rt_old + c);
+        v.ro_p = ro(a.rt_old + cp);
+        v.r2_m = ro(a.rt2pres + cm);
+        v.r2_c = ro(a.rt2pres + c);
+        v.r2_p = ro(a.rt2pres + cp);
+        v.ru_m = ro(a.ru_in + cm);
+        v.ru_c = ro(a.ru_in + c);
+        v.Ru_m = ro(a.R_ru + cm);
+        v.Ru_c = ro(a.R_ru + c);
+        v.mfx = a.mfx[c];
+        v.Rrho = ro(a.R_rho + c);
+        v.rhop = a.rho_p[c];
+        v.th_c = ro(a.theta + c);
+        v.th_p = ro(a.theta + cp);
+        v.th_m = ro(a.theta + cm);
+        v.Rrt = ro(a.R_rt + c);
+        v.Rrw = ro(a.R_rw + c);
+        v.rwp = a.rw_p[c];
+        v.ta = ro(a.ta + c);
+        v.tb = ro(a.tb + c);
+        v.tc = ro(a.tc + c);
+        v.piv = ro(a.tpiv + c);
+    };
+    L cur, nxt, prv;
+    load_up(0, cur);
+    T rho_tp_prev = T(0), rt_tp_prev = T(0);
+    TT dprev = TT(0);
+    for (int k = 0; k < nz; k++) {
+        if (k + 1 < nz) load_up(k + 1, nxt);
+        const size_t c = MOIST_IDX(k, i);
+        // u_update at faces i-1/2 (column im) and i+1/2 (column i)
+        T grad_m = (cur.rt_c - cur.rt_m) / dx;
+        const T grad_m_old = (cur.ro_c - cur.ro_m) / dx;
+        grad_m = grad_m + p.gamma_d * (grad_m - grad_m_old);
+        const T rh_m = (cur.r2_m + cur.r2_c) * T(0.5);
+        const T u_m = cur.ru_m + dt_s * (cur.Ru_m - rh_m * grad_m);
+        T grad_p = (cur.rt_p - cur.rt_c) / dx;
+        const T grad_p_old = (cur.ro_p - cur.ro_c) / dx;
+        grad_p = grad_p + p.gamma_d * (grad_p - grad_p_old);
+        const T rh_p = (cur.r2_c + cur.r2_p) * T(0.5);
+        const T u_p = cur.ru_c + dt_s * (cur.Ru_c - rh_p * grad_p);
+        a.ru_out[c] = u_p;
+        a.mfx[c] = cur.mfx + u_p / ns_T;
+        T advection = -(u_p - u_m) / dx;
+        T inc = dt_s * (cur.Rrho + advection);
+        const T rho_tp = (T)((double)cur.rhop + fact_tp64 * (double)inc);
+        a.rho_p[c] = cur.rhop + inc;
+        const T flux_ip = (cur.th_p + cur.th_c) * T(0.5) * u_p;
+        const T flux_im = (cur.th_c + cur.th_m) * T(0.5) * u_m;
+        advection = -(flux_ip - flux_im) / dx;
+        inc = dt_s * (cur.Rrt + advection);
+        const T rt_tp = (T)((double)cur.rt_c + fact_tp64 * (double)inc);
+        a.rt_out[c] = cur.rt_c + inc;
+        if (k >= 1) {
+            const int j = k - 1;
+            const size_t cj = c - P;
+            const T buoyancy = (rt_tp - rt_tp_prev) / (ro(z + k) - ro(z + j));
+            const T grav = -p.GRAV * T(0.5) * (rho_tp + rho_tp_prev);
+            const T rt2pres_h = (prv.r2_c + cur.r2_c) * T(0.5);
+            const T drho_w = dt_s * (prv.Rrw - rt2pres_h * buoyancy + grav);
+            const T w_j = prv.rwp;
+            const T aj = prv.ta;
+            T d = w_j + drho_w;
+            if (j > 0) d -= aj * fact * w_j;
+            d -= prv.tb * fact * w_j;
+            if (j < n - 1) d -= prv.tc * fact * cur.rwp;
+            TT dp;
+            if (j == 0)
+                dp = (TT)d / prv.piv;
+            else
+                dp = ((TT)d - (TT)aj * dprev) / prv.piv;
+            a.dprime[cj] = dp;
+            dprev = dp;
+        }
+        rho_tp_prev = rho_tp;
+        rt_tp_prev = rt_tp;
+        prv = cur;
+        cur = nxt;
+    }
+    // Back substitution going down fused with the vertical updates of cell k (moist.jl:
+    // 968-970, 1412-1446, 1452-1458), as in b_substep_col: at level k the faces k (w_k, known
+    // from level k + 1) and k - 1 (x_{k-1} = d'_{k-1} - c'_{k-1} x_k, computed here).
+    const T* th = a.theta;
+    // theta at k-2 .. k+2 and s.rho_w at k-1, k, kept in registers as k falls
+    T t_m2 = ke >= 2 ? ro(th + MOIST_IDX(ke - 2, i)) : T(0);
+    T t_m1 = ke >= 1 ? ro(th + MOIST_IDX(ke - 1, i)) : T(0);
+    T t_0 = ro(th + MOIST_IDX(ke, i)), t_p1 = T(0), t_p2 = T(0);
+    T sw_0 = ro(a.s_rw + MOIST_IDX(ke, i)), sw_m1 = ro(a.s_rw + MOIST_IDX(ke - 1, i));
+    T v_rho = a.rho_p[MOIST_IDX(ke, i)], v_rt = a.rt_out[MOIST_IDX(ke, i)], v_mfz = a.mfz[MOIST_IDX(ke, i)];
+    TT v_dp = dprev, v_cp = TT(0);  // d' and c' of face k - 1 (x_{ke-1} = d'_{ke-1} itself)
+    TT x = TT(0);
+    T w_k = T(0);
+    for (int k = ke; k >= 0; k--) {
+        // next level's inputs: cell k - 1 and face k - 2
+        T n_rho = T(0), n_rt = T(0), n_mfz = T(0), n_t = T(0), n_sw = T(0);
+        TT n_dp = TT(0), n_cp = TT(0);
+        if (k >= 1) {
+            const size_t cn = MOIST_IDX(k - 1, i);
+            n_rho = a.rho_p[cn];
+            n_rt = a.rt_out[cn];
+            n_mfz = a.mfz[cn];
+            if (k >= 3) n_t = ro(th + MOIST_IDX(k - 3, i));
+            if (k >= 2) {
+                n_sw = ro(a.s_rw + MOIST_IDX(k - 2, i));
+                n_dp = a.dprime[MOIST_IDX(k - 2, i)];
+                n_cp = ro(a.tcp + MOIST_IDX(k - 2, i));
+            }
+        }
+        T w_km = T(0);
+        if (k >= 1) {
+            x = (k == ke) ? v_dp : v_dp - v_cp * x;
+            w_km = (T)x;
+            a.rw_p[MOIST_IDX(k - 1, i)] = w_km;
+        }
+        const size_t c = MOIST_IDX(k, i);
+        {
+            const T flux_kp = k == ke ? T(0.0) : w_k;
+            const T flux_km = k == 0 ? T(0.0) : w_km;
+            const T adv = -(flux_kp - flux_km) / ro(dz + k);
+            a.rho_p[c] = v_rho + dt_s * adv;
+        }
+        T flux_kp, flux_km;
+        if (k == ke) {
+            flux_kp = T(0.0);
+        } else {
+            const T wp = w_k;
+            if (wp > EPS && k > 0)
+                flux_kp = up3(wp, t_m1, t_0, t_p1);
+            else if (sw_0 < -EPS && k < ke - 1)  // selector on s.rho_w, as written (1426)
+                flux_kp = up3(wp, t_p2, t_p1, t_0);
+            else
+                flux_kp = wp * f2h(t_0, t_p1, ro(dz + k), ro(dz + k + 1));
+        }
+        if (k == 0) {
+            flux_km = T(0.0);
+        } else {
+            const T wp = w_km;
+            const T sw = sw_m1;
+            if (sw > EPS && k > 1)
+                flux_km = up3(wp, t_m2, t_m1, t_0);
+            else if (sw < -EPS && k < ke)
+                flux_km = up3(wp, t_p1, t_0, t_m1);
+            else
+                flux_km = wp * f2h(t_m1, t_0, ro(dz + k - 1), ro(dz + k));
+        }
+        const T adv = -(flux_kp - flux_km) / ro(dz + k);
+        a.rt_out[c] = v_rt + dt_s * adv;
+        if (k < ke) a.mfz[c] = v_mfz + w_k / ns_T;
+        // slide the windows down one level
+        w_k = w_km;
+        t_p2 = t_p1;
+        t_p1 = t_0;
+        t_0 = t_m1;
+        t_m1 = t_m2;
+        t_m2 = n_t;
+        sw_0 = sw_m1;
+        sw_m1 = n_sw;
+        v_rho = n_rho;
+        v_rt = n_rt;
+        v_mfz = n_mfz;
+        v_dp = n_dp;
+        v_cp = n_cp;
+    }
+}
+
+
 // ----------------------------------------------------------------------------- column strips
 //
 // Strip form of the per-stage factorisation and of the acoustic substep. A block of
