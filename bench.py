@@ -156,7 +156,7 @@ class Clocks:
 
 def cpu_baseline(workload, T, budget_s=12.0, max_steps=40):
     """The oracle's threaded build timed on the host cores on a bounded sample of the workload."""
-    from oracle import bind  # noqa: F401  (builds the oracle if needed)
+    from oracle import bind  # builds the oracle if needed
     so = os.path.join(ROOT, "oracle", "libmoist_oracle_omp.so")
     if not os.path.exists(so):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
@@ -172,9 +172,24 @@ def cpu_baseline(workload, T, budget_s=12.0, max_steps=40):
         n += 1
     dt = time.perf_counter() - t0
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {"value": cells * n / dt, "unit": "cell-steps/s", "cores": cores, "kind": "port",
-            "sample": "%d large steps of the %dx%d domain after 1 warm-up step (%.1f s), threaded "
-                      "C++ restatement of rk3_step! (OpenMP over columns)" % (n, p.Nx, p.Nz, dt)}
+    out = {"value": cells * n / dt, "unit": "cell-steps/s", "cores": cores, "kind": "port",
+           "sample": "%d large steps of the %dx%d domain after 1 warm-up step (%.1f s), threaded "
+                     "C++ restatement of rk3_step! (OpenMP over columns)" % (n, p.Nx, p.Nz, dt)}
+    # one thread in the reference's loop order (the serial oracle, JULIA_NUM_THREADS=1)
+    L1 = bind.lib()
+    p, s, _ = make_workload(workload, T)
+    cp = p.to_c()
+    h = s.to_c()
+    L1.oracle_rk3_step(C.byref(cp), p.precision, 1, C.byref(h), 1)
+    n1, t1 = 0, time.perf_counter()
+    while n1 < max_steps and time.perf_counter() - t1 < budget_s / 2:
+        L1.oracle_rk3_step(C.byref(cp), p.precision, 1, C.byref(h), 1)
+        n1 += 1
+    dt1 = time.perf_counter() - t1
+    out["single_thread"] = {"value": cells * n1 / dt1, "unit": "cell-steps/s", "cores": 1,
+                            "sample": "%d large steps after 1 warm-up step (%.1f s), serial C++ "
+                                      "restatement in the reference's loop order" % (n1, dt1)}
+    return out
 
 
 def measure_ensemble(nmem, steps, warmup, peak, plain_value):
@@ -197,14 +212,35 @@ def measure_ensemble(nmem, steps, warmup, peak, plain_value):
         ms = e.time_steps(steps) / steps
         tot, g = e.profile(2)
     value = cells / (ms / 1e3)
+    one = one_domain_per_launch(mem)
     return {"members": nmem, "cells": cells, "steps": steps, "warmup": warmup, "ms_per_step": ms,
             "value": value, "unit": "cell-steps/s", "vs_plain": value / plain_value,
+            "one_domain_per_launch": one, "vs_one_domain_per_launch": one["ms_per_step"] / ms,
             "hbm_frac": cells * words * 4 / (ms / 1e3) / 1e9 / peak,
             "group_ms_per_step": {k: float(x) / 2 for k, x in zip(GROUPS, g)},
             "setup_s": setup_s, "autotune": tune,
             "workload": "%d members, nx in {256,...,2048}, nz in {64,96,128}, dx=250 m, dz=125 m, "
                         "dt=2 s, ns=8, one seeded bubble each on the analytic sounding, Float32 "
                         "state with fp64 w-p elimination" % nmem}
+
+
+def one_domain_per_launch(mem, steps=3):
+    """The ensemble's members advanced the plain way, one domain per launch: each member in its
+    own context (its own kernels, autotuned like the single-domain workload), one member after
+    the other; the device time of a large step of every member, summed over the members."""
+    from moist2d_b200 import model
+    total = 0.0
+    for p, s in mem:
+        with model.Model(p) as m:
+            m.upload(s)
+            m.autotune(1)
+            m.time_steps(1)  # warm-up
+            total += m.time_steps(steps) / steps
+    cells = sum(p.Nx * p.Nz for p, _ in mem)
+    return {"ms_per_step": total, "value": cells / (total / 1e3), "unit": "cell-steps/s",
+            "how": "each member in its own context (single-domain kernels, autotuned), members one "
+                   "after the other, device time of %d large steps per member (CUDA events), "
+                   "summed" % steps}
 
 
 def measure_adjoint(nsteps, ckpt):

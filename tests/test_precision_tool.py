@@ -53,3 +53,22 @@ def test_precision_compares_runs_that_finish(monkeypatch):
     assert set(out) == set(precision.FIELDS)
     for f in ("theta", "qv"):
         assert 0.0 < out[f]["rel_l2"] < 1e-6, (f, out[f])
+
+
+def test_control_run_starts_one_ulp_away(monkeypatch):
+    """--control: the first run is Float64 from a start whose rho_theta differs from the other's
+    by exactly one ulp in every interior cell (the stand-in steps nothing, so the comparison sees
+    the start itself)."""
+    p, s = bubble_case(np.float64, nx=8, nz=6)
+    t = s.copy()
+    precision.last_bit_perturbed(t, p)
+    c = slice(p.is_ - 1, p.ie)
+    a, b = s.rho_theta[:, c], t.rho_theta[:, c]
+    ulps = np.abs(a.view(np.int64) - b.view(np.int64))
+    assert np.all(ulps == 1)
+    assert 0 < np.mean(b > a) < 1  # both directions occur
+    monkeypatch.setattr(model, "Model", FakeModel)
+    monkeypatch.setattr(FakeModel, "nan_at", {})
+    out = precision.run(lambda T: bubble_case(T, nx=8, nz=6), 3, control=True)
+    assert 0.0 < out["theta"]["rel_l2"] < 1e-15
+    assert out["qv"]["rel_l2"] == 0.0
