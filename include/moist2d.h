@@ -383,6 +383,52 @@ int moist_history_close(moist_history* h);
  * moist.jl:1917). Needs no device. */
 int moist_restart_read(const char* path, const moist_params* p, int precision, moist_state_host* s);
 
+/* ---- Seeded initial States (host only: no device is needed). The reference builds its State
+ * with init_state! (moist.jl:351-450), whose theta noise comes from per-thread Xoshiro streams
+ * (moist.jl:374-375) and so depends on the thread schedule. These generators draw from the
+ * counter-based Philox4x32-10 generator keyed by (seed, stream), so a State depends on the seed
+ * alone, and build the base columns in the model's discrete hydrostatic balance (the iteration of
+ * moist.jl:413-431), in double precision, rounded once to the State precision. They fill the
+ * seven prognostic fields (halo columns periodic), theta_ref, and zero the rest of the State
+ * (NULL fields are skipped). The Python mirror is moist2d_b200/init.py (the same algorithms in
+ * numpy; states agree to the last bits of double-precision exp/pow). */
+typedef struct moist_bubble {
+    double xc, zc;   /* centre (m); the x distance is periodic in moist_init_sounding */
+    double radius;   /* m */
+    double amp;      /* theta perturbation (K) at the centre, cos^2 shape */
+} moist_bubble;
+/* the fields of Params{T} that init_state! reads (moist.jl:136-148) */
+typedef struct moist_init_profile {
+    double theta0, bndlayer_depth, z_tropopause, dtheta_dz_trop, dtheta_dz_stra, theta_pert;
+    double rel_hum_surf, rel_hum_decay, u0;
+} moist_init_profile;
+/* out[j] = uniform (0, 1) double of index idx[j] (or j when idx is NULL) in stream
+ * (seed, stream): Philox4x32-10 of the counter (idx low, idx high, stream, 0) and the key
+ * (seed, 0x6D6F6973), first word + 1/2 over 2^32 */
+int moist_uniform(uint32_t seed, uint32_t stream, int64_t n, const uint64_t* idx, double* out);
+/* init_state!(s, p, rngs) (moist.jl:351-450) with the noise of stream 0, index i*nz + k */
+int moist_init_state(const moist_params* p, int precision, const moist_init_profile* profile, uint32_t seed,
+                     moist_state_host* s);
+/* warm moist bubble: theta = 300 K neutral, surface pressure 1000 hPa, RH 20 % outside and 95 %
+ * inside a cos^2 bubble of 2 K, radius 2 km, centred at x = 10 km * nx / 200, z = 2 km, uniform
+ * +-0.01 K theta noise (stream 0, index i*nz + k), u = 0 */
+int moist_init_warm_bubble(const moist_params* p, int precision, uint32_t seed, moist_state_host* s);
+/* analytic sounding: theta = 300 + 43 (z/12 km)^1.25 K below 12 km, isothermal above; RH =
+ * 1 - 0.75 (z/12 km)^1.25, 0.25 above; u = 12 tanh(z / 3 km) m/s; plus the given warm bubbles
+ * applied at constant pressure */
+int moist_init_sounding(const moist_params* p, int precision, const moist_bubble* bubbles, int nbubbles,
+                        moist_state_host* s);
+/* the seeded bubble row of the sounding workload: bubble j at x = (j + 1/2) lx / n, z = zc,
+ * amplitude and radius uniform in the ranges (stream 1, indices 2j and 2j + 1) */
+int moist_sounding_bubble_row(uint32_t seed, int nbubbles, double lx, double amp_lo, double amp_hi,
+                              double rad_lo, double rad_hi, double zc, moist_bubble* out);
+/* member `member` of the uneven ensemble: nx and nz drawn from the choices, one bubble at a
+ * seeded x in (0, nx*dx), z = zc, amplitude and radius uniform in the ranges (stream
+ * 1000 + member, indices 0..4) */
+int moist_ensemble_member_draw(uint32_t seed, int member, const int* nx_choices, int n_nx, const int* nz_choices,
+                               int n_nz, double dx, double amp_lo, double amp_hi, double rad_lo, double rad_hi,
+                               double zc, int* nx, int* nz, moist_bubble* bubble);
+
 /* ---- Autotuner (no counterpart in the reference). moist_autotune times nsteps large steps of
  * the context for every strip width of the factorisation and acoustic-substep kernels (1, 2, 4
  * or 8 columns per block) and every exact tracer sweep the context can run (tiled; streaming

@@ -3,7 +3,8 @@ library or a CUDA device is missing, calls raise."""
 import ctypes as C
 import os
 
-from .abi import moist_adjoint_grad, moist_adjoint_seed, moist_params, moist_state_host
+from .abi import (moist_adjoint_grad, moist_adjoint_seed, moist_bubble, moist_init_profile, moist_params,
+                  moist_state_host)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 SO_PATH = os.path.join(_HERE, "libmoist2d_sm100a.so")
@@ -22,7 +23,8 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_autotune", "moist_batch_autotune", "moist_history_diagnostics", "moist_io_last_error",
            "moist_history_create", "moist_history_append", "moist_history_append_host",
            "moist_history_close", "moist_restart_read", "moist_surface_fluxes", "moist_gray_radiation",
-           "moist_set_wait_limit")
+           "moist_set_wait_limit", "moist_uniform", "moist_init_state", "moist_init_warm_bubble",
+           "moist_init_sounding", "moist_sounding_bubble_row", "moist_ensemble_member_draw")
 
 
 def lib():
@@ -90,5 +92,14 @@ def lib():
         L.moist_history_append_host.argtypes = [H, D, S, C.POINTER(V)]
         L.moist_history_close.argtypes = [H]
         L.moist_restart_read.argtypes = [C.c_char_p, P, I, S]
+        U32 = C.c_uint32
+        Bp = C.POINTER(moist_bubble)
+        L.moist_uniform.argtypes = [U32, U32, C.c_int64, C.POINTER(C.c_uint64), C.POINTER(D)]
+        L.moist_init_state.argtypes = [P, I, C.POINTER(moist_init_profile), U32, S]
+        L.moist_init_warm_bubble.argtypes = [P, I, U32, S]
+        L.moist_init_sounding.argtypes = [P, I, Bp, I, S]
+        L.moist_sounding_bubble_row.argtypes = [U32, I, D, D, D, D, D, D, Bp]
+        L.moist_ensemble_member_draw.argtypes = [U32, I, C.POINTER(I), I, C.POINTER(I), I, D, D, D, D, D, D,
+                                                 C.POINTER(I), C.POINTER(I), Bp]
         _lib = L
     return _lib

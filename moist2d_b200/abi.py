@@ -89,3 +89,13 @@ class moist_adjoint_grad(C.Structure):
     _fields_ = [("state", C.c_void_p * 7), ("prec", C.c_void_p), ("k_auto", C.c_double),
                 ("qc_threshold", C.c_double), ("objective", C.c_double), ("forward_ms", C.c_double),
                 ("reverse_ms", C.c_double)]
+
+
+class moist_bubble(C.Structure):
+    _fields_ = [("xc", C.c_double), ("zc", C.c_double), ("radius", C.c_double), ("amp", C.c_double)]
+
+
+class moist_init_profile(C.Structure):
+    _fields_ = [(f, C.c_double) for f in ("theta0", "bndlayer_depth", "z_tropopause", "dtheta_dz_trop",
+                                          "dtheta_dz_stra", "theta_pert", "rel_hum_surf", "rel_hum_decay",
+                                          "u0")]

@@ -359,3 +359,97 @@ def ensemble_member(T=np.float32, seed=3, member=0, nx_choices=tuple(range(256, 
     bub = [(u[2] * float(p.Lx), 1.5e3, rad[0] + (rad[1] - rad[0]) * u[4],
             amp[0] + (amp[1] - amp[0]) * u[3])]
     return p, _bubbles_state(p, base, bub, distinct_columns=True)
+
+
+# ---------------------------------------------------------------- the library's generators
+#
+# The same workloads built by the C-ABI generators (moist_init_*, include/moist2d.h), which a
+# caller of the shared library without Python (a Julia host) uses. They agree with the numpy
+# versions above to the last bits of double-precision exp / pow before the final rounding.
+
+def _lib():
+    from ._lib import lib
+    return lib()
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise ValueError("%s failed with status %d" % (what, rc))
+
+
+def uniform_lib(seed, stream, idx):
+    """uniform(seed, stream, idx) through moist_uniform."""
+    import ctypes as C
+    idx = np.ascontiguousarray(np.asarray(idx, dtype=np.uint64).ravel())
+    out = np.zeros(idx.size)
+    _check(_lib().moist_uniform(int(seed), int(stream), idx.size, idx.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                out.ctypes.data_as(C.POINTER(C.c_double))), "moist_uniform")
+    return out
+
+
+def warm_bubble_lib(T=np.float32, seed=1, nx=200, nz=100):
+    """warm_bubble through moist_init_warm_bubble."""
+    p = _grid_params(T, nx, nz, 100.0, 100.0, 6, 1.0)
+    s = State(p)
+    cp = p.to_c()
+    h = s.to_c()
+    import ctypes as C
+    _check(_lib().moist_init_warm_bubble(C.byref(cp), p.precision, int(seed), C.byref(h)), "moist_init_warm_bubble")
+    return p, s
+
+
+def _bubbles_lib(p, bubbles):
+    import ctypes as C
+    from .abi import moist_bubble
+    arr = (moist_bubble * max(1, len(bubbles)))()
+    for j, (xc, zc, rad, amp) in enumerate(bubbles):
+        arr[j].xc, arr[j].zc, arr[j].radius, arr[j].amp = xc, zc, rad, amp
+    s = State(p)
+    cp = p.to_c()
+    h = s.to_c()
+    _check(_lib().moist_init_sounding(C.byref(cp), p.precision, arr, len(bubbles), C.byref(h)),
+           "moist_init_sounding")
+    return s
+
+
+def sounding_bubbles_lib(T=np.float32, seed=2, nx=2048, nz=128, dx=250.0, dz=125.0, nbub=5,
+                         amp=(1.5, 2.5), rad=(1.5e3, 3e3), zc=1.5e3, ns=8, dt=2.0):
+    """sounding_bubbles through moist_sounding_bubble_row and moist_init_sounding."""
+    import ctypes as C
+    from .abi import moist_bubble
+    p = _grid_params(T, nx, nz, dx, dz, ns, dt)
+    row = (moist_bubble * nbub)()
+    _check(_lib().moist_sounding_bubble_row(int(seed), nbub, float(p.Lx), amp[0], amp[1], rad[0], rad[1], zc, row),
+           "moist_sounding_bubble_row")
+    return p, _bubbles_lib(p, [(b.xc, b.zc, b.radius, b.amp) for b in row])
+
+
+def ensemble_member_lib(T=np.float32, seed=3, member=0, nx_choices=tuple(range(256, 2049, 256)),
+                        nz_choices=(64, 96, 128), ns=8, dt=2.0, amp=(1.0, 3.0), rad=(1e3, 3e3)):
+    """ensemble_member through moist_ensemble_member_draw and moist_init_sounding."""
+    import ctypes as C
+    from .abi import moist_bubble
+    nxc = (C.c_int * len(nx_choices))(*nx_choices)
+    nzc = (C.c_int * len(nz_choices))(*nz_choices)
+    nx, nz, b = C.c_int(), C.c_int(), moist_bubble()
+    _check(_lib().moist_ensemble_member_draw(int(seed), int(member), nxc, len(nx_choices), nzc, len(nz_choices),
+                                             250.0, amp[0], amp[1], rad[0], rad[1], 1.5e3, C.byref(nx),
+                                             C.byref(nz), C.byref(b)), "moist_ensemble_member_draw")
+    p = _grid_params(T, nx.value, nz.value, 250.0, 125.0, ns, dt)
+    return p, _bubbles_lib(p, [(b.xc, b.zc, b.radius, b.amp)])
+
+
+def init_state_lib(s, p, seed=1):
+    """init_state through moist_init_state (the fields of p that init_state! reads)."""
+    import ctypes as C
+    from .abi import moist_init_profile
+    prof = moist_init_profile()
+    for f, g in (("theta0", "theta0"), ("bndlayer_depth", "bndlayer_depth"), ("z_tropopause", "z_tropopose"),
+                 ("dtheta_dz_trop", "dtheta_dz_trop"), ("dtheta_dz_stra", "dtheta_dz_stra"),
+                 ("theta_pert", "theta_pert"), ("rel_hum_surf", "rel_hum_surf"),
+                 ("rel_hum_decay", "rel_hum_decay"), ("u0", "u0")):
+        setattr(prof, f, float(getattr(p, g)))
+    cp = p.to_c()
+    h = s.to_c()
+    _check(_lib().moist_init_state(C.byref(cp), p.precision, C.byref(prof), int(seed), C.byref(h)), "moist_init_state")
+    return s
