@@ -7,6 +7,7 @@
 
 #include <climits>
 
+#include "fastdiv.cuh"
 #include "model.cuh"
 
 namespace moist {
@@ -223,6 +224,21 @@ __global__ void k_diag(DevParams<T> p, StateP<T> s, T* pres, T* theta, T* rt2pre
     b_diag(p, s, pres, theta, rt2pres, u_face, w_face, err, blockIdx.x, blockIdx.y);
 }
 
+// columns of the per-row reciprocal table DevParams::trcp (filled by the host in double
+// precision from the denominators as the type T forms them)
+enum {
+    TR_DX = 0,     // 1 / dx
+    TR_SIX,        // 1 / 6 (third-order upwind faces)
+    TR_DZ,         // 1 / dz[k]
+    TR_DZ_KP1,     // 1 / dz[k+1]
+    TR_SUM_KP,     // 1 / (dz[k] + dz[k+1])
+    TR_SUM_KM,     // 1 / (dz[k-1] + dz[k])
+    TR_ZD_KP,      // 1 / (z[k+1] - z[k])
+    TR_ZD_KM,      // 1 / (z[k] - z[k-1])
+    TR_ZSUM,       // 1 / (z[k] + z[k+1])
+    TEND_NRCP
+};
+
 template <class T>
 struct TendArgs {
     StateP<T> s, s0;
@@ -233,15 +249,22 @@ struct TendArgs {
     T *ru_left, *rho_right;  // halo values of the stage's exchange, for surface_fluxes!
 };
 
-// slow tendencies R_rho, R_rho_u, R_rho_w, R_rho_theta (moist.jl:1079-1332), perturbation
-// initialisation and the saved momentum fluxes (1339-1348)
-template <class T>
-__device__ __forceinline__ void b_tend(DevParams<T> p, TendArgs<T> a, const int* err, int bx, int by) {
-    const int i = bx * blockDim.x + threadIdx.x;
-    const int k = by * blockDim.y + threadIdx.y;
+// slow tendencies R_rho, R_rho_u, R_rho_w, R_rho_theta (moist.jl:1079-1332) of cell (k, i)
+// into out[0..3] (out[2] only for k < ke), every division through the policy D
+template <class T, class D>
+__device__ __forceinline__ void tend_cell(const DevParams<T>& p, const TendArgs<T>& a, int i, int k, D& dv, T out[4]) {
     const int nx = p.nx, nz = p.nz, P = p.P;
-    if (i >= nx || k >= nz || halted(err)) return;
     const T EPS = p.EPS, dx = p.dx, GRAV = p.GRAV;
+    const double* rc = p.trcp + (size_t)k * TEND_NRCP;
+    // quotient x / d with the denominator's reciprocal rc[j]
+    auto Q = [&](T x, T d, int j) { return dv.q(x, d, rc[j]); };
+    auto up3q = [&](T flux, T a_, T b_, T c_) {  // up3 (model.cuh) with its division by 6
+        return Q(flux * (-a_ + T(5.0) * b_ + T(2.0) * c_), T(6.0), TR_SIX);
+    };
+    // f2h (moist.jl:249) over the faces of this cell: (dz[k], dz[k+1]), (dz[k-1], dz[k]), (z[k], z[k+1])
+    auto f2h_kp = [&](T v1, T v2, T d1, T d2) { return Q(v1 * d2 + v2 * d1, d1 + d2, TR_SUM_KP); };
+    auto f2h_km = [&](T v1, T v2, T d1, T d2) { return Q(v1 * d2 + v2 * d1, d1 + d2, TR_SUM_KM); };
+    auto f2h_z = [&](T v1, T v2, T d1, T d2) { return Q(v1 * d2 + v2 * d1, d1 + d2, TR_ZSUM); };
     const T* dz = p.dz;
     const T* z = p.z;
     const int im = wrapx(i - 1, nx), im2 = wrapx(i - 2, nx), ip = wrapx(i + 1, nx), ip2 = wrapx(i + 2, nx);
@@ -255,48 +278,43 @@ __device__ __forceinline__ void b_tend(DevParams<T> p, TendArgs<T> a, const int*
     const T* th = a.theta;
     auto R = [&](int kk, int ii) { return MOIST_IDX(kk, ii); };
 
-    if (k == 0 && i == 0) {
-        *a.ru_left = ro(ru + (R(0, nx - 1)));
-        *a.rho_right = ro(rho + (R(0, 0)));
-    }
-
     // --- R_rho (1079-1086)
     {
         const T flux_kp = k == ke ? T(0.0) : ro(rw + c);
         const T flux_km = k == 0 ? T(0.0) : ro(rw + (c - P));
-        const T advection = -((ro(ru + c) - ro(ru + (R(k, im)))) / dx + (flux_kp - flux_km) / dz[k]);
-        a.R_rho[c] = advection + ro(a.ph.d_rho + c);
+        const T advection = -(Q(ro(ru + c) - ro(ru + (R(k, im))), dx, TR_DX) + Q(flux_kp - flux_km, dz[k], TR_DZ));
+        out[0] = advection + ro(a.ph.d_rho + c);
     }
     // --- R_rho_u (1098-1178)
     {
         const T rho_u_ip = T(0.5) * (ro(ru + c) + ro(ru + (R(k, ip))));
         T f_ip;
         if (rho_u_ip > EPS)
-            f_ip = up3(rho_u_ip, ro(uf + (R(k, im))), ro(uf + c), ro(uf + (R(k, ip))));
+            f_ip = up3q(rho_u_ip, ro(uf + (R(k, im))), ro(uf + c), ro(uf + (R(k, ip))));
         else if (rho_u_ip < -EPS)
-            f_ip = up3(rho_u_ip, ro(uf + (R(k, ip2))), ro(uf + (R(k, ip))), ro(uf + c));
+            f_ip = up3q(rho_u_ip, ro(uf + (R(k, ip2))), ro(uf + (R(k, ip))), ro(uf + c));
         else
             f_ip = rho_u_ip * (ro(uf + c) + ro(uf + (R(k, ip)))) * T(0.5);
         const T rho_u_im = T(0.5) * (ro(ru + (R(k, im))) + ro(ru + c));
         T f_im;
         if (rho_u_im > EPS)
-            f_im = up3(rho_u_im, ro(uf + (R(k, im2))), ro(uf + (R(k, im))), ro(uf + c));
+            f_im = up3q(rho_u_im, ro(uf + (R(k, im2))), ro(uf + (R(k, im))), ro(uf + c));
         else if (rho_u_im < -EPS)
-            f_im = up3(rho_u_im, ro(uf + (R(k, ip))), ro(uf + c), ro(uf + (R(k, im))));
+            f_im = up3q(rho_u_im, ro(uf + (R(k, ip))), ro(uf + c), ro(uf + (R(k, im))));
         else
             f_im = rho_u_im * (ro(uf + (R(k, im))) + ro(uf + c)) * T(0.5);
-        const T druudx = (f_ip - f_im) / dx;
+        const T druudx = Q(f_ip - f_im, dx, TR_DX);
         T f_kp;
         if (k == ke) {
             f_kp = T(0.0);
         } else {
             const T rho_w_kp = T(0.5) * (ro(rw + c) + ro(rw + (R(k, ip))));
             if (rho_w_kp > EPS && k > 0)
-                f_kp = up3(rho_w_kp, ro(uf + (c - P)), ro(uf + c), ro(uf + (c + P)));
+                f_kp = up3q(rho_w_kp, ro(uf + (c - P)), ro(uf + c), ro(uf + (c + P)));
             else if (rho_w_kp < -EPS && k < ke - 1)
-                f_kp = up3(rho_w_kp, ro(uf + (c + 2 * P)), ro(uf + (c + P)), ro(uf + c));
+                f_kp = up3q(rho_w_kp, ro(uf + (c + 2 * P)), ro(uf + (c + P)), ro(uf + c));
             else
-                f_kp = rho_w_kp * f2h(ro(uf + c), ro(uf + (c + P)), dz[k], dz[k + 1]);
+                f_kp = rho_w_kp * f2h_kp(ro(uf + c), ro(uf + (c + P)), dz[k], dz[k + 1]);
         }
         T f_km;
         if (k == 0) {
@@ -304,103 +322,103 @@ __device__ __forceinline__ void b_tend(DevParams<T> p, TendArgs<T> a, const int*
         } else {
             const T rho_w_km = T(0.5) * (ro(rw + (c - P)) + ro(rw + (R(k - 1, ip))));
             if (rho_w_km > EPS && k > 1)
-                f_km = up3(rho_w_km, ro(uf + (c - 2 * P)), ro(uf + (c - P)), ro(uf + c));
+                f_km = up3q(rho_w_km, ro(uf + (c - 2 * P)), ro(uf + (c - P)), ro(uf + c));
             else if (rho_w_km < -EPS && k < ke)
-                f_km = up3(rho_w_km, ro(uf + (c + P)), ro(uf + c), ro(uf + (c - P)));
+                f_km = up3q(rho_w_km, ro(uf + (c + P)), ro(uf + c), ro(uf + (c - P)));
             else
-                f_km = rho_w_km * f2h(ro(uf + (c - P)), ro(uf + c), dz[k - 1], dz[k]);
+                f_km = rho_w_km * f2h_km(ro(uf + (c - P)), ro(uf + c), dz[k - 1], dz[k]);
         }
-        const T drwudz = (f_kp - f_km) / dz[k];
+        const T drwudz = Q(f_kp - f_km, dz[k], TR_DZ);
         const T advection = -druudx - drwudz;
-        const T u_ip = (ro(uf + (R(k, ip))) - ro(uf + c)) / dx;
-        const T u_im = (ro(uf + c) - ro(uf + (R(k, im)))) / dx;
-        const T u_xx = (u_ip * ro(rho + (R(k, ip))) - u_im * ro(rho + c)) / dx;
-        const T u_kp = k == ke ? T(0.0) : (ro(uf + (c + P)) - ro(uf + c)) / (z[k + 1] - z[k]);
-        const T u_km = k == 0 ? T(0.0) : (ro(uf + c) - ro(uf + (c - P))) / (z[k] - z[k - 1]);
+        const T u_ip = Q(ro(uf + (R(k, ip))) - ro(uf + c), dx, TR_DX);
+        const T u_im = Q(ro(uf + c) - ro(uf + (R(k, im))), dx, TR_DX);
+        const T u_xx = Q(u_ip * ro(rho + (R(k, ip))) - u_im * ro(rho + c), dx, TR_DX);
+        const T u_kp = k == ke ? T(0.0) : Q(ro(uf + (c + P)) - ro(uf + c), z[k + 1] - z[k], TR_ZD_KP);
+        const T u_km = k == 0 ? T(0.0) : Q(ro(uf + c) - ro(uf + (c - P)), z[k] - z[k - 1], TR_ZD_KM);
         const T rho_kp = k == ke ? T(0.0) : T(0.25) * (ro(rho + c) + ro(rho + (c + P)) + ro(rho + (R(k, ip))) + ro(rho + (R(k + 1, ip))));
         const T rho_km = k == 0 ? T(0.0) : T(0.25) * (ro(rho + (c - P)) + ro(rho + c) + ro(rho + (R(k - 1, ip))) + ro(rho + (R(k, ip))));
-        const T u_zz = (u_kp * rho_kp - u_km * rho_km) / dz[k];
+        const T u_zz = Q(u_kp * rho_kp - u_km * rho_km, dz[k], TR_DZ);
         const T diffusion = p.nu * (u_xx + u_zz);
-        const T dpdx = (ro(a.pres + (R(k, ip))) - ro(a.pres + c)) / dx;
-        a.R_ru[c] = advection - dpdx + diffusion + ro(a.ph.d_u + c);
+        const T dpdx = Q(ro(a.pres + (R(k, ip))) - ro(a.pres + c), dx, TR_DX);
+        out[1] = advection - dpdx + diffusion + ro(a.ph.d_u + c);
     }
     // --- R_rho_w (1190-1278)
     if (k < ke) {
-        const T rho_u_ip = f2h(ro(ru + c), ro(ru + (c + P)), z[k], z[k + 1]);  // z weights, as written (1196)
+        const T rho_u_ip = f2h_z(ro(ru + c), ro(ru + (c + P)), z[k], z[k + 1]);  // z weights, as written (1196)
         T f_ip;
         if (rho_u_ip > EPS)
-            f_ip = up3(rho_u_ip, ro(wf + (R(k, im))), ro(wf + c), ro(wf + (R(k, ip))));
+            f_ip = up3q(rho_u_ip, ro(wf + (R(k, im))), ro(wf + c), ro(wf + (R(k, ip))));
         else if (rho_u_ip < -EPS)
-            f_ip = up3(rho_u_ip, ro(wf + (R(k, ip2))), ro(wf + (R(k, ip))), ro(wf + c));
+            f_ip = up3q(rho_u_ip, ro(wf + (R(k, ip2))), ro(wf + (R(k, ip))), ro(wf + c));
         else
             f_ip = rho_u_ip * (ro(wf + c) + ro(wf + (R(k, ip)))) * T(0.5);
-        const T rho_u_im = f2h(ro(ru + (R(k, im))), ro(ru + (R(k + 1, im))), dz[k], dz[k + 1]);
+        const T rho_u_im = f2h_kp(ro(ru + (R(k, im))), ro(ru + (R(k + 1, im))), dz[k], dz[k + 1]);
         T f_im;
         if (rho_u_im > EPS)
-            f_im = up3(rho_u_im, ro(wf + (R(k, im2))), ro(wf + (R(k, im))), ro(wf + c));
+            f_im = up3q(rho_u_im, ro(wf + (R(k, im2))), ro(wf + (R(k, im))), ro(wf + c));
         else if (rho_u_im < -EPS)
-            f_im = up3(rho_u_im, ro(wf + (R(k, ip))), ro(wf + c), ro(wf + (R(k, im))));
+            f_im = up3q(rho_u_im, ro(wf + (R(k, ip))), ro(wf + c), ro(wf + (R(k, im))));
         else
             f_im = rho_u_im * (ro(wf + (R(k, im))) + ro(wf + c)) * T(0.5);
-        const T drwudx = (f_ip - f_im) / dx;
+        const T drwudx = Q(f_ip - f_im, dx, TR_DX);
         T f_kp;
         if (k == ke - 1) {
             f_kp = T(0.0);
         } else {
-            const T rho_w_kp = f2h(ro(rw + c), ro(rw + (c + P)), dz[k], dz[k + 1]);
+            const T rho_w_kp = f2h_kp(ro(rw + c), ro(rw + (c + P)), dz[k], dz[k + 1]);
             if (rho_w_kp > EPS && k > 0)
-                f_kp = up3(rho_w_kp, ro(wf + (c - P)), ro(wf + c), ro(wf + (c + P)));
+                f_kp = up3q(rho_w_kp, ro(wf + (c - P)), ro(wf + c), ro(wf + (c + P)));
             else if (rho_w_kp < -EPS && k < ke - 2)
-                f_kp = up3(rho_w_kp, ro(wf + (c + 2 * P)), ro(wf + (c + P)), ro(wf + c));
+                f_kp = up3q(rho_w_kp, ro(wf + (c + 2 * P)), ro(wf + (c + P)), ro(wf + c));
             else
-                f_kp = rho_w_kp * f2h(ro(wf + c), ro(wf + (c + P)), dz[k], dz[k + 1]);
+                f_kp = rho_w_kp * f2h_kp(ro(wf + c), ro(wf + (c + P)), dz[k], dz[k + 1]);
         }
         T f_km;
         if (k == 0) {
             f_km = T(0.0);
         } else {
-            const T rho_w_km = f2h(ro(rw + (c - P)), ro(rw + c), dz[k - 1], dz[k]);
+            const T rho_w_km = f2h_km(ro(rw + (c - P)), ro(rw + c), dz[k - 1], dz[k]);
             if (rho_w_km > EPS && k > 1)
-                f_km = up3(rho_w_km, ro(wf + (c - 2 * P)), ro(wf + (c - P)), ro(wf + c));
+                f_km = up3q(rho_w_km, ro(wf + (c - 2 * P)), ro(wf + (c - P)), ro(wf + c));
             else if (rho_w_km < -EPS && k < ke - 1)
-                f_km = up3(rho_w_km, ro(wf + (c + P)), ro(wf + c), ro(wf + (c - P)));
+                f_km = up3q(rho_w_km, ro(wf + (c + P)), ro(wf + c), ro(wf + (c - P)));
             else
-                f_km = rho_w_km * f2h(ro(wf + (c - P)), ro(wf + c), dz[k - 1], dz[k]);
+                f_km = rho_w_km * f2h_km(ro(wf + (c - P)), ro(wf + c), dz[k - 1], dz[k]);
         }
-        const T drwwdz = (f_kp - f_km) / (z[k + 1] - z[k]);
+        const T drwwdz = Q(f_kp - f_km, z[k + 1] - z[k], TR_ZD_KP);
         const T advection = -drwudx - drwwdz;
-        const T w_ip = (ro(wf + (R(k, ip))) - ro(wf + c)) / dx;
-        const T w_im = (ro(wf + c) - ro(wf + (R(k, im)))) / dx;
+        const T w_ip = Q(ro(wf + (R(k, ip))) - ro(wf + c), dx, TR_DX);
+        const T w_im = Q(ro(wf + c) - ro(wf + (R(k, im))), dx, TR_DX);
         const T rho_ip = T(0.25) * (ro(rho + c) + ro(rho + (c + P)) + ro(rho + (R(k, ip))) + ro(rho + (R(k + 1, ip))));
         const T rho_im = T(0.25) * (ro(rho + (R(k, im))) + ro(rho + (R(k + 1, im))) + ro(rho + c) + ro(rho + (c + P)));
-        const T w_xx = (w_ip * rho_ip - w_im * rho_im) / dx;
-        const T w_kp = k == ke - 1 ? T(0.0) : (ro(wf + (c + P)) - ro(wf + c)) / dz[k + 1];
-        const T w_km = k == 0 ? T(0.0) : (ro(wf + c) - ro(wf + (c - P))) / dz[k];
-        const T w_zz = (w_kp * ro(rho + (c + P)) - w_km * ro(rho + c)) / (z[k + 1] - z[k]);
+        const T w_xx = Q(w_ip * rho_ip - w_im * rho_im, dx, TR_DX);
+        const T w_kp = k == ke - 1 ? T(0.0) : Q(ro(wf + (c + P)) - ro(wf + c), dz[k + 1], TR_DZ_KP1);
+        const T w_km = k == 0 ? T(0.0) : Q(ro(wf + c) - ro(wf + (c - P)), dz[k], TR_DZ);
+        const T w_zz = Q(w_kp * ro(rho + (c + P)) - w_km * ro(rho + c), z[k + 1] - z[k], TR_ZD_KP);
         const T diffusion = p.nu * (w_xx + w_zz);
         T sigma = T(0.0);
         const T zfk = p.zf[k];
         if (zfk > (T(1.0) - p.zf_sponge) * p.H)
             sigma = (GRAV / T(30.0)) * ((zfk - (T(1.0) - p.zf_sponge) * p.H) / (p.zf_sponge * p.H));
         const T sponge = -sigma * ro(rw + c);
-        const T dpdz = (ro(a.pres + (c + P)) - ro(a.pres + c)) / (z[k + 1] - z[k]);
+        const T dpdz = Q(ro(a.pres + (c + P)) - ro(a.pres + c), z[k + 1] - z[k], TR_ZD_KP);
         const T buoyancy = -GRAV * (ro(rho + c) + ro(rho + (c + P))) * T(0.5);
-        a.R_rw[c] = advection - dpdz + buoyancy + diffusion + sponge;
+        out[2] = advection - dpdz + buoyancy + diffusion + sponge;
     }
     // --- R_rho_theta (1284-1331)
     {
         const T ru_i = ro(ru + c), ru_m = ro(ru + (R(k, im)));
         T f_ip, f_im, f_kp, f_km;
         if (ru_i > EPS)
-            f_ip = up3(ru_i, ro(th + (R(k, im))), ro(th + c), ro(th + (R(k, ip))));
+            f_ip = up3q(ru_i, ro(th + (R(k, im))), ro(th + c), ro(th + (R(k, ip))));
         else if (ru_i < -EPS)
-            f_ip = up3(ru_i, ro(th + (R(k, ip2))), ro(th + (R(k, ip))), ro(th + c));
+            f_ip = up3q(ru_i, ro(th + (R(k, ip2))), ro(th + (R(k, ip))), ro(th + c));
         else
             f_ip = ru_i * (ro(th + c) + ro(th + (R(k, ip)))) * T(0.5);
         if (ru_m > EPS)
-            f_im = up3(ru_m, ro(th + (R(k, im2))), ro(th + (R(k, im))), ro(th + c));
+            f_im = up3q(ru_m, ro(th + (R(k, im2))), ro(th + (R(k, im))), ro(th + c));
         else if (ru_m < -EPS)
-            f_im = up3(ru_m, ro(th + (R(k, ip))), ro(th + c), ro(th + (R(k, im))));
+            f_im = up3q(ru_m, ro(th + (R(k, ip))), ro(th + c), ro(th + (R(k, im))));
         else
             f_im = ru_m * (ro(th + (R(k, im))) + ro(th + c)) * T(0.5);
         if (k == ke) {
@@ -408,33 +426,83 @@ __device__ __forceinline__ void b_tend(DevParams<T> p, TendArgs<T> a, const int*
         } else {
             const T w = ro(rw + c);
             if (w > EPS && k > 0)
-                f_kp = up3(w, ro(th + (c - P)), ro(th + c), ro(th + (c + P)));
+                f_kp = up3q(w, ro(th + (c - P)), ro(th + c), ro(th + (c + P)));
             else if (w < -EPS && k < ke - 1)
-                f_kp = up3(w, ro(th + (c + 2 * P)), ro(th + (c + P)), ro(th + c));
+                f_kp = up3q(w, ro(th + (c + 2 * P)), ro(th + (c + P)), ro(th + c));
             else
-                f_kp = w * f2h(ro(th + c), ro(th + (c + P)), dz[k], dz[k + 1]);
+                f_kp = w * f2h_kp(ro(th + c), ro(th + (c + P)), dz[k], dz[k + 1]);
         }
         if (k == 0) {
             f_km = T(0.0);
         } else {
             const T w = ro(rw + (c - P));
             if (w > EPS && k > 1)
-                f_km = up3(w, ro(th + (c - 2 * P)), ro(th + (c - P)), ro(th + c));
+                f_km = up3q(w, ro(th + (c - 2 * P)), ro(th + (c - P)), ro(th + c));
             else if (w < -EPS && k < ke)
-                f_km = up3(w, ro(th + (c + P)), ro(th + c), ro(th + (c - P)));
+                f_km = up3q(w, ro(th + (c + P)), ro(th + c), ro(th + (c - P)));
             else
-                f_km = w * f2h(ro(th + (c - P)), ro(th + c), dz[k - 1], dz[k]);
+                f_km = w * f2h_km(ro(th + (c - P)), ro(th + c), dz[k - 1], dz[k]);
         }
-        const T advection = -((f_ip - f_im) / dx + (f_kp - f_km) / dz[k]);
-        a.R_rt[c] = advection + ro(a.ph.d_th + c);
+        const T advection = -(Q(f_ip - f_im, dx, TR_DX) + Q(f_kp - f_km, dz[k], TR_DZ));
+        out[3] = advection + ro(a.ph.d_th + c);
     }
+}
+
+// Division policies of tend_cell: q(x, d, y) = x / d with y = 1/d in double precision. Every
+// denominator of the slow tendencies is a grid constant (dx, 6, dz and z differences and sums
+// of the cell's row), whose reciprocals are tabulated once per context (TEND_NRCP per row).
+template <class T>
+struct TendDivIEEE {
+    __device__ __forceinline__ T q(T x, T d, double) const { return x / d; }
+};
+// Float32: RN32(RN64(x * y)), the IEEE quotient except at subnormal ties (fastdiv.cuh), with
+// every quotient in 0 < |q| <= 2^-126 recorded in the guard word; such a cell is recomputed
+// with IEEE division.
+struct TendDiv64 {
+    unsigned g = ~0u;
+    __device__ __forceinline__ float q(float x, float, double y) {
+        const float r = div64(x, y);
+        subnormal_guard(g, r);
+        return r;
+    }
+};
+
+// slow tendencies (moist.jl:1079-1332), perturbation initialisation and the saved momentum
+// fluxes (1339-1348) of one cell
+template <class T>
+__device__ __forceinline__ void b_tend(DevParams<T> p, TendArgs<T> a, const int* err, int bx, int by) {
+    const int i = bx * blockDim.x + threadIdx.x;
+    const int k = by * blockDim.y + threadIdx.y;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    if (i >= nx || k >= nz || halted(err)) return;
+    const size_t c = MOIST_IDX(k, i);
+    if (k == 0 && i == 0) {
+        *a.ru_left = ro(a.s.ru + MOIST_IDX(0, nx - 1));
+        *a.rho_right = ro(a.s.rho + MOIST_IDX(0, 0));
+    }
+    T out[4];
+    if constexpr (sizeof(T) == 4) {
+        TendDiv64 dv;
+        tend_cell(p, a, i, k, dv, out);
+        if (guard_hit(dv.g)) {  // rare: recompute the cell with IEEE division
+            TendDivIEEE<T> di;
+            tend_cell(p, a, i, k, di, out);
+        }
+    } else {
+        TendDivIEEE<T> di;
+        tend_cell(p, a, i, k, di, out);
+    }
+    a.R_rho[c] = out[0];
+    a.R_ru[c] = out[1];
+    if (k < nz - 1) a.R_rw[c] = out[2];
+    a.R_rt[c] = out[3];
     // --- perturbations and saved momentum fluxes (1339-1348)
-    a.rho_p[c] = ro(a.s0.rho + c) - ro(rho + c);
-    a.ru_p[c] = ro(a.s0.ru + c) - ro(ru + c);
-    a.rw_p[c] = ro(a.s0.rw + c) - ro(rw + c);
+    a.rho_p[c] = ro(a.s0.rho + c) - ro(a.s.rho + c);
+    a.ru_p[c] = ro(a.s0.ru + c) - ro(a.s.ru + c);
+    a.rw_p[c] = ro(a.s0.rw + c) - ro(a.s.rw + c);
     a.rt_p[c] = ro(a.s0.rt + c) - ro(a.s.rt + c);
-    a.mfx[c] = ro(ru + c);
-    a.mfz[c] = ro(rw + c);
+    a.mfx[c] = ro(a.s.ru + c);
+    a.mfz[c] = ro(a.s.rw + c);
 }
 template <class T>
 __global__ void k_tend(DevParams<T> p, TendArgs<T> a, const int* err) {

@@ -33,6 +33,7 @@ struct DevParams {
     const T* dz;
     const T* z;
     const T* zf;
+    const double* trcp;  // [nz][TEND_NRCP] reciprocals of the slow tendencies' denominators (kernels.cuh)
 };
 
 __device__ __forceinline__ int wrapx(int i, int nx) { return i < 0 ? i + nx : (i >= nx ? i - nx : i); }

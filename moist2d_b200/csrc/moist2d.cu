@@ -55,6 +55,7 @@ struct CtxBase {
     virtual int rk3_host(moist_state_host* s, int nsteps) = 0;
     virtual int pass_counts(int* counts, int n) = 0;
     virtual int set_wait_limit(long long cycles) = 0;
+    virtual int pass_trace(int nsteps, int maxrec, long long* pass_ns, int* pass_tiles, int* npasses) = 0;
     virtual int adjoint_run(int nsteps, int ckpt, const moist_adjoint_seed* seed, moist_adjoint_grad* out) = 0;
     virtual int autotune(int nsteps, std::string& report) = 0;
     virtual int history(void* const out[MOIST_NDIAG], double summary[6]) = 0;
@@ -221,6 +222,7 @@ struct Ctx : CtxBase {
     T *prec, *d_prec, *mflux, *shflux, *lhflux, *d_u_sf, *d_th_sf, *d_qv_sf, *theta_ref;
     T *halo_vals;  // [0] = rho_u[ks, is-1], [1] = rho[ks, ie+1] as of the last exchange
     T *g_dz, *g_z, *g_zf;
+    double* g_trcp = nullptr;  // [nz][TEND_NRCP] reciprocals of the slow tendencies (kernels.cuh)
     T* staging;
     int* err;
     CSum* bud_part;   // [BUDGET_BLOCKS][4] block sums of the budgets
@@ -371,6 +373,33 @@ struct Ctx : CtxBase {
         dp.dz = g_dz;
         dp.z = g_z;
         dp.zf = g_zf;
+        {
+            // reciprocals of the slow tendencies' denominators, each formed in T as the kernels
+            // form it, then inverted in double (IEEE, as the device would)
+            const T* hdz = (const T*)c->dz;
+            const T* hz = (const T*)c->z;
+            std::vector<double> tab((size_t)nz * TEND_NRCP, 1.0);
+            for (int k = 0; k < nz; k++) {
+                double* r = &tab[(size_t)k * TEND_NRCP];
+                r[TR_DX] = 1.0 / (double)dp.dx;
+                r[TR_SIX] = 1.0 / 6.0;
+                r[TR_DZ] = 1.0 / (double)hdz[k];
+                if (k + 1 < nz) {
+                    r[TR_DZ_KP1] = 1.0 / (double)hdz[k + 1];
+                    r[TR_SUM_KP] = 1.0 / (double)(T)(hdz[k] + hdz[k + 1]);
+                    r[TR_ZD_KP] = 1.0 / (double)(T)(hz[k + 1] - hz[k]);
+                    r[TR_ZSUM] = 1.0 / (double)(T)(hz[k] + hz[k + 1]);
+                }
+                if (k >= 1) {
+                    r[TR_SUM_KM] = 1.0 / (double)(T)(hdz[k - 1] + hdz[k]);
+                    r[TR_ZD_KM] = 1.0 / (double)(T)(hz[k] - hz[k - 1]);
+                }
+            }
+            AL(g_trcp, tab.size());
+            CK(cudaMemcpyAsync(g_trcp, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+            CK(cudaStreamSynchronize(st));  // tab is a host temporary
+            dp.trcp = g_trcp;
+        }
         if (int r = init_strips()) return r;
         if (owner->flags & MOIST_FLAG_TRACER_STREAM) {
             if (nz > STREAM_MAX_ROWS)
@@ -734,6 +763,12 @@ struct Ctx : CtxBase {
         } else if (use_tiles) {
             CK(cudaMemsetAsync(tctl.any_changed, 0, (tctl.max_pass + 2) * sizeof(int), st));
             TileCtl c = tctl;
+            if (trace_ts && trace_n < trace_cap) {  // moist_tracer_pass_trace
+                const size_t stride = (size_t)tctl.max_pass + 3;
+                c.pass_ts = trace_ts + trace_n * stride;
+                c.pass_work = trace_work + trace_n * stride;
+                trace_n++;
+            }
             T* sp = strips;
             int* e = err;
             void* args[] = {&dp, &tr, &c, &sp, &e};
@@ -858,6 +893,58 @@ struct Ctx : CtxBase {
             tot += ms;
         }
         if (total_ms) *total_ms = tot;
+        return finish();
+    }
+
+    // moist_tracer_pass_trace: per-sweep pass timestamps and working tiles
+    unsigned long long* trace_ts = nullptr;
+    int* trace_work = nullptr;
+    int trace_n = 0, trace_cap = 0;
+    int pass_trace(int nsteps, int maxrec, long long* pass_ns, int* pass_tiles, int* npasses) override {
+        if (int r = check_stage_shape()) return r;
+        if (!use_tiles) return set_err(owner, MOIST_ERR_UNSUPPORTED, "the tiled tracer sweep is not in use");
+        const size_t stride = (size_t)tctl.max_pass + 3, nsw = (size_t)3 * nsteps;
+        unsigned long long* ts = nullptr;
+        int* wk = nullptr;
+        CK(cudaMalloc(&ts, nsw * stride * sizeof(unsigned long long)));
+        CK(cudaMalloc(&wk, nsw * stride * sizeof(int)));
+        CK(cudaMemsetAsync(ts, 0, nsw * stride * sizeof(unsigned long long), st));
+        CK(cudaMemsetAsync(wk, 0, nsw * stride * sizeof(int), st));
+        trace_ts = ts;
+        trace_work = wk;
+        trace_n = 0;
+        trace_cap = (int)nsw;
+        CK(reset_err());
+        int r = MOIST_OK;
+        for (int n = 0; n < nsteps && r == MOIST_OK; n++) r = launch_step();
+        trace_ts = nullptr;
+        trace_work = nullptr;
+        std::vector<unsigned long long> hts(nsw * stride);
+        std::vector<int> hwk(nsw * stride);
+        CK(cudaMemcpyAsync(hts.data(), ts, hts.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hwk.data(), wk, hwk.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        cudaFree(ts);
+        cudaFree(wk);
+        if (r != MOIST_OK) return r;
+        // per sweep: the passes run, each pass's duration (start of the next pass, or block 0
+        // leaving, minus its start) and the tile-tracer warps that recomputed in it
+        for (size_t w = 0; w < nsw; w++) {
+            const unsigned long long* t = &hts[w * stride];
+            const int* k = &hwk[w * stride];
+            int np = 0;
+            while (np + 1 <= tctl.max_pass && t[np + 1] != 0) np++;
+            if (npasses) npasses[w] = np;
+            for (int q = 0; q < maxrec; q++) {
+                long long d = 0;
+                if (q + 1 <= np) {
+                    const unsigned long long t1 = (q + 2 <= np) ? t[q + 2] : t[tctl.max_pass + 2];
+                    d = (long long)(t1 - t[q + 1]);
+                }
+                if (pass_ns) pass_ns[w * maxrec + q] = d;
+                if (pass_tiles) pass_tiles[w * maxrec + q] = (q + 1 <= np) ? k[q + 1] : 0;
+            }
+        }
         return finish();
     }
 
@@ -1771,7 +1858,7 @@ struct BatchImpl : BatchBase {
             BATCH_LAUNCH(BK_RD, BRd<T>, FRd<T>, 1)
             BATCH_LAUNCH(BK_PHYS, BPhys<T>, FPhys<T>, 3)
             BATCH_LAUNCH(BK_DIAG, BDiag<T>, FDiag<T>, 4)
-            BATCH_LAUNCH(BK_TEND, BTend<T>, FTend<T>, 4)
+            BATCH_LAUNCH(BK_TEND, BTend<T>, FTend<T>, 3)
             case BK_THOMAS:
                 if (sub_strips)
                     k_batched<BThomas<T, TT>, FThomasStrip<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
@@ -2494,6 +2581,13 @@ int moist_tracer_pass_counts(moist_ctx* c, int* counts, int n) {
     if (!c || !counts || n < 0) return MOIST_ERR_ARG;
     CTX_DEVICE(c);
     return c->impl->pass_counts(counts, n);
+}
+
+int moist_tracer_pass_trace(moist_ctx* c, int nsteps, int maxrec, long long* pass_ns, int* pass_tiles,
+                            int* npasses) {
+    if (!c || nsteps < 1 || maxrec < 0) return MOIST_ERR_ARG;
+    CTX_DEVICE(c);
+    return c->impl->pass_trace(nsteps, maxrec, pass_ns, pass_tiles, npasses);
 }
 
 int moist_set_wait_limit(moist_ctx* c, long long cycles) {
