@@ -471,6 +471,15 @@ int moist_tracer_pass_counts(moist_ctx* ctx, int* counts, int n);
  * does not wait (the streaming or wavefront sweep). */
 int moist_set_wait_limit(moist_ctx* ctx, long long cycles);
 
+/* Diagnostic of the tiled tracer sweep (no counterpart in the reference): runs nsteps large
+ * steps (3 sweeps each) with every pass timed on the device. For sweep w (0 .. 3*nsteps-1):
+ * npasses[w] = passes run; pass_ns[w*maxrec + q] = duration of pass q+1 in ns (from its start to
+ * the next pass's start, the last one to the moment block 0 leaves the sweep);
+ * pass_tiles[w*maxrec + q] = tile-tracer warps that recomputed in that pass (3 per tile at most).
+ * Any output pointer may be NULL. Allocates its timing buffers per call. */
+int moist_tracer_pass_trace(moist_ctx* ctx, int nsteps, int maxrec, long long* pass_ns, int* pass_tiles,
+                            int* npasses);
+
 /* Stream of the context (a cudaStream_t), for callers that order their own work after it. */
 void* moist_stream(moist_ctx* ctx);
 /* Block until the context stream is idle. */

@@ -24,7 +24,8 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_history_create", "moist_history_append", "moist_history_append_host",
            "moist_history_close", "moist_restart_read", "moist_surface_fluxes", "moist_gray_radiation",
            "moist_set_wait_limit", "moist_uniform", "moist_init_state", "moist_init_warm_bubble",
-           "moist_init_sounding", "moist_sounding_bubble_row", "moist_ensemble_member_draw")
+           "moist_init_sounding", "moist_sounding_bubble_row", "moist_ensemble_member_draw",
+           "moist_tracer_pass_trace")
 
 
 def lib():
@@ -63,6 +64,7 @@ def lib():
         L.moist_set_device.argtypes = [I]
         L.moist_tracer_pass_counts.argtypes = [Ctx, C.POINTER(I), I]
         L.moist_set_wait_limit.argtypes = [Ctx, C.c_longlong]
+        L.moist_tracer_pass_trace.argtypes = [Ctx, I, I, C.POINTER(C.c_longlong), C.POINTER(I), C.POINTER(I)]
         L.moist_implicit_correction_noalloc.argtypes = [P, I, I, I, V, V, V, V, D, V, C.c_char_p,
                                                         C.c_size_t]
         L.moist_step_profile.argtypes = [Ctx, I, C.POINTER(C.c_float), C.POINTER(C.c_float),

@@ -36,7 +36,8 @@ struct TileCtl {
     int* passes;        // out: passes run
     int* timeout;       // out: barrier timeout flag
     long long spin_limit;
-    unsigned long long* pass_ts;  // optional diagnostic: globaltimer at the start of each pass
+    unsigned long long* pass_ts;  // optional diagnostic [max_pass + 3]: globaltimer at the start of each
+                                  // pass, and at [max_pass + 2] when block 0 leaves
     int* pass_work;               // optional diagnostic: [pass] warps that recomputed their tile
 };
 
@@ -662,7 +663,10 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
         if (!grid_barrier(ctl, nblocks)) return;
         if (__ldcg(ctl.any_changed + pass) == 0) break;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) *ctl.passes = pass;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *ctl.passes = pass;
+        if (ctl.pass_ts) ctl.pass_ts[ctl.max_pass + 2] = globaltimer_ns();  // block 0 leaves the sweep
+    }
 }
 
 // histogram of pass counts (diagnostic)

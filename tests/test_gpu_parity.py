@@ -170,3 +170,32 @@ def test_tiled_sweep_pass_counts_are_recorded():
         hist = list(counts)
     assert sum(hist) == 6  # 3 stages x 2 steps
     assert hist[0] == 0 and max(i for i, v in enumerate(hist) if v) <= 8 + 2 + 2
+
+
+def test_tiled_sweep_pass_trace():
+    """moist_tracer_pass_trace: one entry per sweep, positive pass durations, pass 1 recomputes
+    every tile of every tracer, and the pass counts agree with moist_tracer_pass_counts."""
+    import ctypes as C
+    from moist2d_b200._lib import lib
+    from moist2d_b200.init import sounding_bubbles
+    p, s = sounding_bubbles(np.float32, nx=256, nz=64, nbub=2)
+    maxrec = 32
+    with model.Model(p) as m:
+        m.upload(s)
+        lib().moist_tracer_pass_counts(m.ctx, (C.c_int * 64)(), 64)  # reset the counters
+        ns_ = (C.c_longlong * (6 * maxrec))()
+        tiles = (C.c_int * (6 * maxrec))()
+        npass = (C.c_int * 6)()
+        assert lib().moist_tracer_pass_trace(m.ctx, 2, maxrec, ns_, tiles, npass) == 0
+        counts = (C.c_int * 64)()
+        assert lib().moist_tracer_pass_counts(m.ctx, counts, 64) == 0
+    ntiles = (256 // 32) * (64 // 32)
+    hist = [0] * 64
+    for w in range(6):
+        n = npass[w]
+        hist[n] += 1
+        assert 1 <= n <= maxrec
+        assert all(ns_[w * maxrec + q] > 0 for q in range(n))
+        assert tiles[w * maxrec] == 3 * ntiles
+        assert all(tiles[w * maxrec + q] <= 3 * ntiles for q in range(n))
+    assert hist == list(counts)
