@@ -236,6 +236,14 @@ __global__ void __launch_bounds__(256, MINB) k_batched(const BItem* __restrict__
     f(args[it.m], it.bx, it.by);
 }
 
+// the same with a block of at most MAXT threads, MINB of them per SM
+template <class A, class F, int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_batched_b(const BItem* __restrict__ items,
+                                                           const A* __restrict__ args, F f) {
+    const BItem it = items[blockIdx.x];
+    f(args[it.m], it.bx, it.by);
+}
+
 // the members' error words gathered into one array: out[m][4]
 __global__ void k_gather_err(int* const* errs, int n, int* out) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;

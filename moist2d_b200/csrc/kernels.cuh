@@ -239,6 +239,10 @@ enum {
     TEND_NRCP
 };
 
+// the stencil fields of the slow tendencies (tend_cell reads them through an accessor)
+enum { TS_RU = 0, TS_RW, TS_UF, TS_WF, TS_TH, TS_RHO, TS_PRES, TS_NF };
+constexpr int TEND_TX = 32, TEND_TY = 8, TEND_H = 2;
+
 template <class T>
 struct TendArgs {
     StateP<T> s, s0;
@@ -250,9 +254,11 @@ struct TendArgs {
 };
 
 // slow tendencies R_rho, R_rho_u, R_rho_w, R_rho_theta (moist.jl:1079-1332) of cell (k, i)
-// into out[0..3] (out[2] only for k < ke), every division through the policy D
-template <class T, class D>
-__device__ __forceinline__ void tend_cell(const DevParams<T>& p, const TendArgs<T>& a, int i, int k, D& dv, T out[4]) {
+// into out[0..3] (out[2] only for k < ke), every division through the policy D and every read of
+// the stencil fields through st(field, dk, di) = field at (k + dk, i + di), x periodic
+template <class T, class D, class S>
+__device__ __forceinline__ void tend_cell(const DevParams<T>& p, const TendArgs<T>& a, const S& st, int i, int k, D& dv,
+                                          T out[4]) {
     const int nx = p.nx, nz = p.nz, P = p.P;
     const T EPS = p.EPS, dx = p.dx, GRAV = p.GRAV;
     const double* rc = p.trcp + (size_t)k * TEND_NRCP;
@@ -267,181 +273,173 @@ __device__ __forceinline__ void tend_cell(const DevParams<T>& p, const TendArgs<
     auto f2h_z = [&](T v1, T v2, T d1, T d2) { return Q(v1 * d2 + v2 * d1, d1 + d2, TR_ZSUM); };
     const T* dz = p.dz;
     const T* z = p.z;
-    const int im = wrapx(i - 1, nx), im2 = wrapx(i - 2, nx), ip = wrapx(i + 1, nx), ip2 = wrapx(i + 2, nx);
     const int ke = nz - 1;
     const size_t c = MOIST_IDX(k, i);
-    const T* rho = a.s.rho;
-    const T* ru = a.s.ru;
-    const T* rw = a.s.rw;
-    const T* uf = a.u_face;
-    const T* wf = a.w_face;
-    const T* th = a.theta;
-    auto R = [&](int kk, int ii) { return MOIST_IDX(kk, ii); };
 
     // --- R_rho (1079-1086)
     {
-        const T flux_kp = k == ke ? T(0.0) : ro(rw + c);
-        const T flux_km = k == 0 ? T(0.0) : ro(rw + (c - P));
-        const T advection = -(Q(ro(ru + c) - ro(ru + (R(k, im))), dx, TR_DX) + Q(flux_kp - flux_km, dz[k], TR_DZ));
+        const T flux_kp = k == ke ? T(0.0) : st(TS_RW, 0, 0);
+        const T flux_km = k == 0 ? T(0.0) : st(TS_RW, -1, 0);
+        const T advection = -(Q(st(TS_RU, 0, 0) - st(TS_RU, 0, -1), dx, TR_DX) + Q(flux_kp - flux_km, dz[k], TR_DZ));
         out[0] = advection + ro(a.ph.d_rho + c);
     }
     // --- R_rho_u (1098-1178)
     {
-        const T rho_u_ip = T(0.5) * (ro(ru + c) + ro(ru + (R(k, ip))));
+        const T rho_u_ip = T(0.5) * (st(TS_RU, 0, 0) + st(TS_RU, 0, 1));
         T f_ip;
         if (rho_u_ip > EPS)
-            f_ip = up3q(rho_u_ip, ro(uf + (R(k, im))), ro(uf + c), ro(uf + (R(k, ip))));
+            f_ip = up3q(rho_u_ip, st(TS_UF, 0, -1), st(TS_UF, 0, 0), st(TS_UF, 0, 1));
         else if (rho_u_ip < -EPS)
-            f_ip = up3q(rho_u_ip, ro(uf + (R(k, ip2))), ro(uf + (R(k, ip))), ro(uf + c));
+            f_ip = up3q(rho_u_ip, st(TS_UF, 0, 2), st(TS_UF, 0, 1), st(TS_UF, 0, 0));
         else
-            f_ip = rho_u_ip * (ro(uf + c) + ro(uf + (R(k, ip)))) * T(0.5);
-        const T rho_u_im = T(0.5) * (ro(ru + (R(k, im))) + ro(ru + c));
+            f_ip = rho_u_ip * (st(TS_UF, 0, 0) + st(TS_UF, 0, 1)) * T(0.5);
+        const T rho_u_im = T(0.5) * (st(TS_RU, 0, -1) + st(TS_RU, 0, 0));
         T f_im;
         if (rho_u_im > EPS)
-            f_im = up3q(rho_u_im, ro(uf + (R(k, im2))), ro(uf + (R(k, im))), ro(uf + c));
+            f_im = up3q(rho_u_im, st(TS_UF, 0, -2), st(TS_UF, 0, -1), st(TS_UF, 0, 0));
         else if (rho_u_im < -EPS)
-            f_im = up3q(rho_u_im, ro(uf + (R(k, ip))), ro(uf + c), ro(uf + (R(k, im))));
+            f_im = up3q(rho_u_im, st(TS_UF, 0, 1), st(TS_UF, 0, 0), st(TS_UF, 0, -1));
         else
-            f_im = rho_u_im * (ro(uf + (R(k, im))) + ro(uf + c)) * T(0.5);
+            f_im = rho_u_im * (st(TS_UF, 0, -1) + st(TS_UF, 0, 0)) * T(0.5);
         const T druudx = Q(f_ip - f_im, dx, TR_DX);
         T f_kp;
         if (k == ke) {
             f_kp = T(0.0);
         } else {
-            const T rho_w_kp = T(0.5) * (ro(rw + c) + ro(rw + (R(k, ip))));
+            const T rho_w_kp = T(0.5) * (st(TS_RW, 0, 0) + st(TS_RW, 0, 1));
             if (rho_w_kp > EPS && k > 0)
-                f_kp = up3q(rho_w_kp, ro(uf + (c - P)), ro(uf + c), ro(uf + (c + P)));
+                f_kp = up3q(rho_w_kp, st(TS_UF, -1, 0), st(TS_UF, 0, 0), st(TS_UF, 1, 0));
             else if (rho_w_kp < -EPS && k < ke - 1)
-                f_kp = up3q(rho_w_kp, ro(uf + (c + 2 * P)), ro(uf + (c + P)), ro(uf + c));
+                f_kp = up3q(rho_w_kp, st(TS_UF, 2, 0), st(TS_UF, 1, 0), st(TS_UF, 0, 0));
             else
-                f_kp = rho_w_kp * f2h_kp(ro(uf + c), ro(uf + (c + P)), dz[k], dz[k + 1]);
+                f_kp = rho_w_kp * f2h_kp(st(TS_UF, 0, 0), st(TS_UF, 1, 0), dz[k], dz[k + 1]);
         }
         T f_km;
         if (k == 0) {
             f_km = T(0.0);
         } else {
-            const T rho_w_km = T(0.5) * (ro(rw + (c - P)) + ro(rw + (R(k - 1, ip))));
+            const T rho_w_km = T(0.5) * (st(TS_RW, -1, 0) + st(TS_RW, -1, 1));
             if (rho_w_km > EPS && k > 1)
-                f_km = up3q(rho_w_km, ro(uf + (c - 2 * P)), ro(uf + (c - P)), ro(uf + c));
+                f_km = up3q(rho_w_km, st(TS_UF, -2, 0), st(TS_UF, -1, 0), st(TS_UF, 0, 0));
             else if (rho_w_km < -EPS && k < ke)
-                f_km = up3q(rho_w_km, ro(uf + (c + P)), ro(uf + c), ro(uf + (c - P)));
+                f_km = up3q(rho_w_km, st(TS_UF, 1, 0), st(TS_UF, 0, 0), st(TS_UF, -1, 0));
             else
-                f_km = rho_w_km * f2h_km(ro(uf + (c - P)), ro(uf + c), dz[k - 1], dz[k]);
+                f_km = rho_w_km * f2h_km(st(TS_UF, -1, 0), st(TS_UF, 0, 0), dz[k - 1], dz[k]);
         }
         const T drwudz = Q(f_kp - f_km, dz[k], TR_DZ);
         const T advection = -druudx - drwudz;
-        const T u_ip = Q(ro(uf + (R(k, ip))) - ro(uf + c), dx, TR_DX);
-        const T u_im = Q(ro(uf + c) - ro(uf + (R(k, im))), dx, TR_DX);
-        const T u_xx = Q(u_ip * ro(rho + (R(k, ip))) - u_im * ro(rho + c), dx, TR_DX);
-        const T u_kp = k == ke ? T(0.0) : Q(ro(uf + (c + P)) - ro(uf + c), z[k + 1] - z[k], TR_ZD_KP);
-        const T u_km = k == 0 ? T(0.0) : Q(ro(uf + c) - ro(uf + (c - P)), z[k] - z[k - 1], TR_ZD_KM);
-        const T rho_kp = k == ke ? T(0.0) : T(0.25) * (ro(rho + c) + ro(rho + (c + P)) + ro(rho + (R(k, ip))) + ro(rho + (R(k + 1, ip))));
-        const T rho_km = k == 0 ? T(0.0) : T(0.25) * (ro(rho + (c - P)) + ro(rho + c) + ro(rho + (R(k - 1, ip))) + ro(rho + (R(k, ip))));
+        const T u_ip = Q(st(TS_UF, 0, 1) - st(TS_UF, 0, 0), dx, TR_DX);
+        const T u_im = Q(st(TS_UF, 0, 0) - st(TS_UF, 0, -1), dx, TR_DX);
+        const T u_xx = Q(u_ip * st(TS_RHO, 0, 1) - u_im * st(TS_RHO, 0, 0), dx, TR_DX);
+        const T u_kp = k == ke ? T(0.0) : Q(st(TS_UF, 1, 0) - st(TS_UF, 0, 0), z[k + 1] - z[k], TR_ZD_KP);
+        const T u_km = k == 0 ? T(0.0) : Q(st(TS_UF, 0, 0) - st(TS_UF, -1, 0), z[k] - z[k - 1], TR_ZD_KM);
+        const T rho_kp = k == ke ? T(0.0) : T(0.25) * (st(TS_RHO, 0, 0) + st(TS_RHO, 1, 0) + st(TS_RHO, 0, 1) + st(TS_RHO, 1, 1));
+        const T rho_km = k == 0 ? T(0.0) : T(0.25) * (st(TS_RHO, -1, 0) + st(TS_RHO, 0, 0) + st(TS_RHO, -1, 1) + st(TS_RHO, 0, 1));
         const T u_zz = Q(u_kp * rho_kp - u_km * rho_km, dz[k], TR_DZ);
         const T diffusion = p.nu * (u_xx + u_zz);
-        const T dpdx = Q(ro(a.pres + (R(k, ip))) - ro(a.pres + c), dx, TR_DX);
+        const T dpdx = Q(st(TS_PRES, 0, 1) - st(TS_PRES, 0, 0), dx, TR_DX);
         out[1] = advection - dpdx + diffusion + ro(a.ph.d_u + c);
     }
     // --- R_rho_w (1190-1278)
     if (k < ke) {
-        const T rho_u_ip = f2h_z(ro(ru + c), ro(ru + (c + P)), z[k], z[k + 1]);  // z weights, as written (1196)
+        const T rho_u_ip = f2h_z(st(TS_RU, 0, 0), st(TS_RU, 1, 0), z[k], z[k + 1]);  // z weights, as written (1196)
         T f_ip;
         if (rho_u_ip > EPS)
-            f_ip = up3q(rho_u_ip, ro(wf + (R(k, im))), ro(wf + c), ro(wf + (R(k, ip))));
+            f_ip = up3q(rho_u_ip, st(TS_WF, 0, -1), st(TS_WF, 0, 0), st(TS_WF, 0, 1));
         else if (rho_u_ip < -EPS)
-            f_ip = up3q(rho_u_ip, ro(wf + (R(k, ip2))), ro(wf + (R(k, ip))), ro(wf + c));
+            f_ip = up3q(rho_u_ip, st(TS_WF, 0, 2), st(TS_WF, 0, 1), st(TS_WF, 0, 0));
         else
-            f_ip = rho_u_ip * (ro(wf + c) + ro(wf + (R(k, ip)))) * T(0.5);
-        const T rho_u_im = f2h_kp(ro(ru + (R(k, im))), ro(ru + (R(k + 1, im))), dz[k], dz[k + 1]);
+            f_ip = rho_u_ip * (st(TS_WF, 0, 0) + st(TS_WF, 0, 1)) * T(0.5);
+        const T rho_u_im = f2h_kp(st(TS_RU, 0, -1), st(TS_RU, 1, -1), dz[k], dz[k + 1]);
         T f_im;
         if (rho_u_im > EPS)
-            f_im = up3q(rho_u_im, ro(wf + (R(k, im2))), ro(wf + (R(k, im))), ro(wf + c));
+            f_im = up3q(rho_u_im, st(TS_WF, 0, -2), st(TS_WF, 0, -1), st(TS_WF, 0, 0));
         else if (rho_u_im < -EPS)
-            f_im = up3q(rho_u_im, ro(wf + (R(k, ip))), ro(wf + c), ro(wf + (R(k, im))));
+            f_im = up3q(rho_u_im, st(TS_WF, 0, 1), st(TS_WF, 0, 0), st(TS_WF, 0, -1));
         else
-            f_im = rho_u_im * (ro(wf + (R(k, im))) + ro(wf + c)) * T(0.5);
+            f_im = rho_u_im * (st(TS_WF, 0, -1) + st(TS_WF, 0, 0)) * T(0.5);
         const T drwudx = Q(f_ip - f_im, dx, TR_DX);
         T f_kp;
         if (k == ke - 1) {
             f_kp = T(0.0);
         } else {
-            const T rho_w_kp = f2h_kp(ro(rw + c), ro(rw + (c + P)), dz[k], dz[k + 1]);
+            const T rho_w_kp = f2h_kp(st(TS_RW, 0, 0), st(TS_RW, 1, 0), dz[k], dz[k + 1]);
             if (rho_w_kp > EPS && k > 0)
-                f_kp = up3q(rho_w_kp, ro(wf + (c - P)), ro(wf + c), ro(wf + (c + P)));
+                f_kp = up3q(rho_w_kp, st(TS_WF, -1, 0), st(TS_WF, 0, 0), st(TS_WF, 1, 0));
             else if (rho_w_kp < -EPS && k < ke - 2)
-                f_kp = up3q(rho_w_kp, ro(wf + (c + 2 * P)), ro(wf + (c + P)), ro(wf + c));
+                f_kp = up3q(rho_w_kp, st(TS_WF, 2, 0), st(TS_WF, 1, 0), st(TS_WF, 0, 0));
             else
-                f_kp = rho_w_kp * f2h_kp(ro(wf + c), ro(wf + (c + P)), dz[k], dz[k + 1]);
+                f_kp = rho_w_kp * f2h_kp(st(TS_WF, 0, 0), st(TS_WF, 1, 0), dz[k], dz[k + 1]);
         }
         T f_km;
         if (k == 0) {
             f_km = T(0.0);
         } else {
-            const T rho_w_km = f2h_km(ro(rw + (c - P)), ro(rw + c), dz[k - 1], dz[k]);
+            const T rho_w_km = f2h_km(st(TS_RW, -1, 0), st(TS_RW, 0, 0), dz[k - 1], dz[k]);
             if (rho_w_km > EPS && k > 1)
-                f_km = up3q(rho_w_km, ro(wf + (c - 2 * P)), ro(wf + (c - P)), ro(wf + c));
+                f_km = up3q(rho_w_km, st(TS_WF, -2, 0), st(TS_WF, -1, 0), st(TS_WF, 0, 0));
             else if (rho_w_km < -EPS && k < ke - 1)
-                f_km = up3q(rho_w_km, ro(wf + (c + P)), ro(wf + c), ro(wf + (c - P)));
+                f_km = up3q(rho_w_km, st(TS_WF, 1, 0), st(TS_WF, 0, 0), st(TS_WF, -1, 0));
             else
-                f_km = rho_w_km * f2h_km(ro(wf + (c - P)), ro(wf + c), dz[k - 1], dz[k]);
+                f_km = rho_w_km * f2h_km(st(TS_WF, -1, 0), st(TS_WF, 0, 0), dz[k - 1], dz[k]);
         }
         const T drwwdz = Q(f_kp - f_km, z[k + 1] - z[k], TR_ZD_KP);
         const T advection = -drwudx - drwwdz;
-        const T w_ip = Q(ro(wf + (R(k, ip))) - ro(wf + c), dx, TR_DX);
-        const T w_im = Q(ro(wf + c) - ro(wf + (R(k, im))), dx, TR_DX);
-        const T rho_ip = T(0.25) * (ro(rho + c) + ro(rho + (c + P)) + ro(rho + (R(k, ip))) + ro(rho + (R(k + 1, ip))));
-        const T rho_im = T(0.25) * (ro(rho + (R(k, im))) + ro(rho + (R(k + 1, im))) + ro(rho + c) + ro(rho + (c + P)));
+        const T w_ip = Q(st(TS_WF, 0, 1) - st(TS_WF, 0, 0), dx, TR_DX);
+        const T w_im = Q(st(TS_WF, 0, 0) - st(TS_WF, 0, -1), dx, TR_DX);
+        const T rho_ip = T(0.25) * (st(TS_RHO, 0, 0) + st(TS_RHO, 1, 0) + st(TS_RHO, 0, 1) + st(TS_RHO, 1, 1));
+        const T rho_im = T(0.25) * (st(TS_RHO, 0, -1) + st(TS_RHO, 1, -1) + st(TS_RHO, 0, 0) + st(TS_RHO, 1, 0));
         const T w_xx = Q(w_ip * rho_ip - w_im * rho_im, dx, TR_DX);
-        const T w_kp = k == ke - 1 ? T(0.0) : Q(ro(wf + (c + P)) - ro(wf + c), dz[k + 1], TR_DZ_KP1);
-        const T w_km = k == 0 ? T(0.0) : Q(ro(wf + c) - ro(wf + (c - P)), dz[k], TR_DZ);
-        const T w_zz = Q(w_kp * ro(rho + (c + P)) - w_km * ro(rho + c), z[k + 1] - z[k], TR_ZD_KP);
+        const T w_kp = k == ke - 1 ? T(0.0) : Q(st(TS_WF, 1, 0) - st(TS_WF, 0, 0), dz[k + 1], TR_DZ_KP1);
+        const T w_km = k == 0 ? T(0.0) : Q(st(TS_WF, 0, 0) - st(TS_WF, -1, 0), dz[k], TR_DZ);
+        const T w_zz = Q(w_kp * st(TS_RHO, 1, 0) - w_km * st(TS_RHO, 0, 0), z[k + 1] - z[k], TR_ZD_KP);
         const T diffusion = p.nu * (w_xx + w_zz);
         T sigma = T(0.0);
         const T zfk = p.zf[k];
         if (zfk > (T(1.0) - p.zf_sponge) * p.H)
             sigma = (GRAV / T(30.0)) * ((zfk - (T(1.0) - p.zf_sponge) * p.H) / (p.zf_sponge * p.H));
-        const T sponge = -sigma * ro(rw + c);
-        const T dpdz = Q(ro(a.pres + (c + P)) - ro(a.pres + c), z[k + 1] - z[k], TR_ZD_KP);
-        const T buoyancy = -GRAV * (ro(rho + c) + ro(rho + (c + P))) * T(0.5);
+        const T sponge = -sigma * st(TS_RW, 0, 0);
+        const T dpdz = Q(st(TS_PRES, 1, 0) - st(TS_PRES, 0, 0), z[k + 1] - z[k], TR_ZD_KP);
+        const T buoyancy = -GRAV * (st(TS_RHO, 0, 0) + st(TS_RHO, 1, 0)) * T(0.5);
         out[2] = advection - dpdz + buoyancy + diffusion + sponge;
     }
     // --- R_rho_theta (1284-1331)
     {
-        const T ru_i = ro(ru + c), ru_m = ro(ru + (R(k, im)));
+        const T ru_i = st(TS_RU, 0, 0), ru_m = st(TS_RU, 0, -1);
         T f_ip, f_im, f_kp, f_km;
         if (ru_i > EPS)
-            f_ip = up3q(ru_i, ro(th + (R(k, im))), ro(th + c), ro(th + (R(k, ip))));
+            f_ip = up3q(ru_i, st(TS_TH, 0, -1), st(TS_TH, 0, 0), st(TS_TH, 0, 1));
         else if (ru_i < -EPS)
-            f_ip = up3q(ru_i, ro(th + (R(k, ip2))), ro(th + (R(k, ip))), ro(th + c));
+            f_ip = up3q(ru_i, st(TS_TH, 0, 2), st(TS_TH, 0, 1), st(TS_TH, 0, 0));
         else
-            f_ip = ru_i * (ro(th + c) + ro(th + (R(k, ip)))) * T(0.5);
+            f_ip = ru_i * (st(TS_TH, 0, 0) + st(TS_TH, 0, 1)) * T(0.5);
         if (ru_m > EPS)
-            f_im = up3q(ru_m, ro(th + (R(k, im2))), ro(th + (R(k, im))), ro(th + c));
+            f_im = up3q(ru_m, st(TS_TH, 0, -2), st(TS_TH, 0, -1), st(TS_TH, 0, 0));
         else if (ru_m < -EPS)
-            f_im = up3q(ru_m, ro(th + (R(k, ip))), ro(th + c), ro(th + (R(k, im))));
+            f_im = up3q(ru_m, st(TS_TH, 0, 1), st(TS_TH, 0, 0), st(TS_TH, 0, -1));
         else
-            f_im = ru_m * (ro(th + (R(k, im))) + ro(th + c)) * T(0.5);
+            f_im = ru_m * (st(TS_TH, 0, -1) + st(TS_TH, 0, 0)) * T(0.5);
         if (k == ke) {
             f_kp = T(0.0);
         } else {
-            const T w = ro(rw + c);
+            const T w = st(TS_RW, 0, 0);
             if (w > EPS && k > 0)
-                f_kp = up3q(w, ro(th + (c - P)), ro(th + c), ro(th + (c + P)));
+                f_kp = up3q(w, st(TS_TH, -1, 0), st(TS_TH, 0, 0), st(TS_TH, 1, 0));
             else if (w < -EPS && k < ke - 1)
-                f_kp = up3q(w, ro(th + (c + 2 * P)), ro(th + (c + P)), ro(th + c));
+                f_kp = up3q(w, st(TS_TH, 2, 0), st(TS_TH, 1, 0), st(TS_TH, 0, 0));
             else
-                f_kp = w * f2h_kp(ro(th + c), ro(th + (c + P)), dz[k], dz[k + 1]);
+                f_kp = w * f2h_kp(st(TS_TH, 0, 0), st(TS_TH, 1, 0), dz[k], dz[k + 1]);
         }
         if (k == 0) {
             f_km = T(0.0);
         } else {
-            const T w = ro(rw + (c - P));
+            const T w = st(TS_RW, -1, 0);
             if (w > EPS && k > 1)
-                f_km = up3q(w, ro(th + (c - 2 * P)), ro(th + (c - P)), ro(th + c));
+                f_km = up3q(w, st(TS_TH, -2, 0), st(TS_TH, -1, 0), st(TS_TH, 0, 0));
             else if (w < -EPS && k < ke)
-                f_km = up3q(w, ro(th + (c + P)), ro(th + c), ro(th + (c - P)));
+                f_km = up3q(w, st(TS_TH, 1, 0), st(TS_TH, 0, 0), st(TS_TH, -1, 0));
             else
-                f_km = w * f2h_km(ro(th + (c - P)), ro(th + c), dz[k - 1], dz[k]);
+                f_km = w * f2h_km(st(TS_TH, -1, 0), st(TS_TH, 0, 0), dz[k - 1], dz[k]);
         }
         const T advection = -(Q(f_ip - f_im, dx, TR_DX) + Q(f_kp - f_km, dz[k], TR_DZ));
         out[3] = advection + ro(a.ph.d_th + c);
@@ -467,14 +465,49 @@ struct TendDiv64 {
     }
 };
 
+// The stencil fields of a (TEND_TY x TEND_TX) block of cells with a two-cell halo, staged in
+// shared memory: every block issues all its loads at once (coalesced rows, x periodic) and the
+// cells then read their 45 stencil values from the tile.
+template <class T>
+struct TendTile {
+    T f[TS_NF][TEND_TY + 2 * TEND_H][TEND_TX + 2 * TEND_H];
+};
+template <class T>
+struct TendStaged {
+    const TendTile<T>& t;
+    int tx, ty;
+    __device__ __forceinline__ T operator()(int f, int dk, int di) const {
+        return t.f[f][ty + TEND_H + dk][tx + TEND_H + di];
+    }
+};
+
 // slow tendencies (moist.jl:1079-1332), perturbation initialisation and the saved momentum
-// fluxes (1339-1348) of one cell
+// fluxes (1339-1348) of one block of TEND_TY x TEND_TX cells (blockDim = (TEND_TX, TEND_TY))
 template <class T>
 __device__ __forceinline__ void b_tend(DevParams<T> p, TendArgs<T> a, const int* err, int bx, int by) {
-    const int i = bx * blockDim.x + threadIdx.x;
-    const int k = by * blockDim.y + threadIdx.y;
+    __shared__ TendTile<T> tile;
+    if (halted(err)) return;  // the same for every thread of the launch
     const int nx = p.nx, nz = p.nz, P = p.P;
-    if (i >= nx || k >= nz || halted(err)) return;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int i0 = bx * TEND_TX, k0 = by * TEND_TY;
+    {
+        const T* src[TS_NF] = {a.s.ru, a.s.rw, a.u_face, a.w_face, a.theta, a.s.rho, a.pres};
+        constexpr int W = TEND_TX + 2 * TEND_H, H = TEND_TY + 2 * TEND_H;
+        for (int j = ty * TEND_TX + tx; j < W * H; j += TEND_TX * TEND_TY) {
+            const int rr = j / W, cc = j % W;
+            const int kk = k0 - TEND_H + rr;
+            int ii = (i0 - TEND_H + cc) % nx;
+            if (ii < 0) ii += nx;
+            const bool ok = kk >= 0 && kk < nz;  // rows outside the column are never read
+            const size_t off = ok ? MOIST_IDX(kk, ii) : 0;
+#pragma unroll
+            for (int f = 0; f < TS_NF; f++) tile.f[f][rr][cc] = ok ? ro(src[f] + off) : T(0);
+        }
+    }
+    __syncthreads();
+    const int i = i0 + tx, k = k0 + ty;
+    if (i >= nx || k >= nz) return;
+    const TendStaged<T> st{tile, tx, ty};
     const size_t c = MOIST_IDX(k, i);
     if (k == 0 && i == 0) {
         *a.ru_left = ro(a.s.ru + MOIST_IDX(0, nx - 1));
@@ -483,14 +516,14 @@ __device__ __forceinline__ void b_tend(DevParams<T> p, TendArgs<T> a, const int*
     T out[4];
     if constexpr (sizeof(T) == 4) {
         TendDiv64 dv;
-        tend_cell(p, a, i, k, dv, out);
+        tend_cell(p, a, st, i, k, dv, out);
         if (guard_hit(dv.g)) {  // rare: recompute the cell with IEEE division
             TendDivIEEE<T> di;
-            tend_cell(p, a, i, k, di, out);
+            tend_cell(p, a, st, i, k, di, out);
         }
     } else {
         TendDivIEEE<T> di;
-        tend_cell(p, a, i, k, di, out);
+        tend_cell(p, a, st, i, k, di, out);
     }
     a.R_rho[c] = out[0];
     a.R_ru[c] = out[1];

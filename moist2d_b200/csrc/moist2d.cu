@@ -1757,7 +1757,8 @@ struct BatchImpl : BatchBase {
     std::vector<void*> allocs;
     int col_threads = BATCH_COL_THREADS;  // threads per block of the per-column kernels
     bool sub_strips = false;               // factorisation and substep over column strips instead
-    int stream_minb = 1;                   // register bound of the streaming tracer sweep (1 or 2)
+    int stream_minb = 1;                   // register bound of the streaming tracer sweep: 1 or 2 blocks of
+                                           // 256 threads per SM, or 3 blocks of 128 (rows <= 128)
     // per-column substep body: 0 b_substep_col (64 registers), 1 and 2 b_substep_col_pf (loads one
     // level ahead; 128 and 85 registers)
     int sub_form = 1;
@@ -1858,7 +1859,7 @@ struct BatchImpl : BatchBase {
             BATCH_LAUNCH(BK_RD, BRd<T>, FRd<T>, 1)
             BATCH_LAUNCH(BK_PHYS, BPhys<T>, FPhys<T>, 3)
             BATCH_LAUNCH(BK_DIAG, BDiag<T>, FDiag<T>, 4)
-            BATCH_LAUNCH(BK_TEND, BTend<T>, FTend<T>, 3)
+            BATCH_LAUNCH(BK_TEND, BTend<T>, FTend<T>, 4)
             case BK_THOMAS:
                 if (sub_strips)
                     k_batched<BThomas<T, TT>, FThomasStrip<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
@@ -1885,6 +1886,9 @@ struct BatchImpl : BatchBase {
             case BK_STREAM:
                 if (stream_minb == 2)  // registers bounded so that twice the blocks fit on an SM
                     k_batched<BStream<T>, FStream<T>, 2><<<s.nitems, s.block, s.smem, st>>>(
+                        s.items, (const BStream<T>*)s.args, FStream<T>{});
+                else if (stream_minb == 3)  // blocks of at most 128 threads, three of them per SM
+                    k_batched_b<BStream<T>, FStream<T>, 128, 3><<<s.nitems, s.block, s.smem, st>>>(
                         s.items, (const BStream<T>*)s.args, FStream<T>{});
                 else
                     k_batched<BStream<T>, FStream<T>, 1><<<s.nitems, s.block, s.smem, st>>>(
@@ -2160,7 +2164,8 @@ struct BatchImpl : BatchBase {
         // then, with that form, the register bound of the streaming tracer sweep
         int bmb = stream_minb;
         float best_mb = 1e30f;
-        for (int mb : {1, 2}) {
+        for (int mb : {1, 2, 3}) {
+            if (mb == 3 && max_rows > 128) continue;  // the 128-thread bound needs rows <= 128
             stream_minb = mb;
             if (int r = set_col_threads(bct)) return r;  // recaptures the graphs
             if (int r = copy_all(false)) return r;
