@@ -187,6 +187,12 @@ struct FSubPf {
         b_substep_col_pf<T, TT>(a.p, a.a, a.dt_s, a.ns_T, a.fact_tp64, a.err, bx);
     }
 };
+template <class T, class TT>
+struct FSubAsync {
+    __device__ void operator()(const BSub<T, TT>& a, int bx, int) const {
+        b_substep_col_async<T, TT>(a.p, a.a, a.dt_s, a.ns_T, a.fact_tp64, a.err, bx);
+    }
+};
 // the same two kernels over column strips (for ensembles too small to fill the GPU with columns)
 template <class T, class TT>
 struct FThomasStrip {

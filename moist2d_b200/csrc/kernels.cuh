@@ -932,6 +932,247 @@ __device__ __forceinline__ void b_substep_col_pf(DevParams<T> p, SubArgs<T, TT> 
 }
 
 
+// Asynchronous copies global -> shared (cp.async, sm_80 and later): the copy proceeds while the
+// thread computes; cp_async_wait<N>() waits until at most N of its committed groups are pending.
+template <class X>
+__device__ __forceinline__ void cp_async(X* s, const X* g) {
+    static_assert(sizeof(X) == 4 || sizeof(X) == 8, "4- or 8-byte elements");
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+    if constexpr (sizeof(X) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(g) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// the per-level inputs of the upward pass that b_substep_col_async stages in shared memory
+enum {
+    SU_RT_M = 0, SU_RT_C, SU_RT_P, SU_RO_M, SU_RO_C, SU_RO_P, SU_R2_M, SU_R2_C, SU_R2_P, SU_RU_M, SU_RU_C,
+    SU_RRU_M, SU_RRU_C, SU_MFX, SU_RRHO, SU_RHOP, SU_TH_C, SU_TH_P, SU_TH_M, SU_RRT, SU_RRW, SU_RWP, SU_TA,
+    SU_TB, SU_TC, SU_NV
+};
+// shared memory of b_substep_col_async per thread: two levels of the SU_NV inputs and the pivot
+template <class T, class TT>
+__host__ __device__ constexpr size_t sub_async_bytes_per_thread() {
+    return 2 * (SU_NV * sizeof(T) + sizeof(TT));
+}
+
+// b_substep_col_pf with the next level's inputs brought in by asynchronous copies into this
+// thread's slots of shared memory instead of registers: the copies of level k + 1 run during
+// level k's arithmetic, and the registers they would hold are free, so more warps fit on an
+// SM. Same arithmetic, operation for operation; the downward pass is b_substep_col_pf's.
+template <class T, class TT>
+__device__ __forceinline__ void b_substep_col_async(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T,
+                                                    double fact_tp64, const int* err, int bx) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nt = blockDim.x, tid = threadIdx.x;
+    const int i = bx * nt + tid;
+    const int nx = p.nx, nz = p.nz, P = p.P;
+    if (i >= nx || halted(err)) return;
+    const T dx = p.dx, EPS = p.EPS;
+    const T* dz = p.dz;
+    const T* z = p.z;
+    const int im = wrapx(i - 1, nx), ip = wrapx(i + 1, nx);
+    const int ke = nz - 1, n = nz - 1;
+    const T fact_tpT = T(0.5) * (T(1.0) + p.beta);
+    const T fact_tmT = T(0.5) * (T(1.0) - p.beta);
+    const T fact = fact_tmT / fact_tpT;
+    T* fs = reinterpret_cast<T*>(smem_raw);                                          // [2][SU_NV][nt]
+    TT* ps = reinterpret_cast<TT*>(smem_raw + (size_t)2 * SU_NV * nt * sizeof(T));  // [2][nt]
+    auto slot = [&](int b, int f) { return fs + ((size_t)(b * SU_NV + f) * nt + tid); };
+    auto issue = [&](int k, int b) {
+        const size_t c = MOIST_IDX(k, i), cm = MOIST_IDX(k, im), cp = MOIST_IDX(k, ip);
+        cp_async(slot(b, SU_RT_M), a.rt_in + cm);
+        cp_async(slot(b, SU_RT_C), a.rt_in + c);
+        cp_async(slot(b, SU_RT_P), a.rt_in + cp);
+        cp_async(slot(b, SU_RO_M), a.rt_old + cm);
+        cp_async(slot(b, SU_RO_C), a.rt_old + c);
+        cp_async(slot(b, SU_RO_P), a.rt_old + cp);
+        cp_async(slot(b, SU_R2_M), a.rt2pres + cm);
+        cp_async(slot(b, SU_R2_C), a.rt2pres + c);
+        cp_async(slot(b, SU_R2_P), a.rt2pres + cp);
+        cp_async(slot(b, SU_RU_M), a.ru_in + cm);
+        cp_async(slot(b, SU_RU_C), a.ru_in + c);
+        cp_async(slot(b, SU_RRU_M), a.R_ru + cm);
+        cp_async(slot(b, SU_RRU_C), a.R_ru + c);
+        cp_async(slot(b, SU_MFX), (const T*)a.mfx + c);
+        cp_async(slot(b, SU_RRHO), a.R_rho + c);
+        cp_async(slot(b, SU_RHOP), (const T*)a.rho_p + c);
+        cp_async(slot(b, SU_TH_C), a.theta + c);
+        cp_async(slot(b, SU_TH_P), a.theta + cp);
+        cp_async(slot(b, SU_TH_M), a.theta + cm);
+        cp_async(slot(b, SU_RRT), a.R_rt + c);
+        cp_async(slot(b, SU_RRW), a.R_rw + c);
+        cp_async(slot(b, SU_RWP), (const T*)a.rw_p + c);
+        cp_async(slot(b, SU_TA), a.ta + c);
+        cp_async(slot(b, SU_TB), a.tb + c);
+        cp_async(slot(b, SU_TC), a.tc + c);
+        cp_async(ps + (size_t)b * nt + tid, a.tpiv + c);
+        cp_async_commit();
+    };
+    issue(0, 0);
+    // face k - 1 values the next level uses: R_rho_w, rho_w_p, the factors, the pivot, rt2pres
+    T pv_r2c = T(0), pv_Rrw = T(0), pv_rwp = T(0), pv_ta = T(0), pv_tb = T(0), pv_tc = T(0);
+    TT pv_piv = TT(1);
+    T rho_tp_prev = T(0), rt_tp_prev = T(0);
+    TT dprev = TT(0);
+    for (int k = 0; k < nz; k++) {
+        if (k + 1 < nz)
+            issue(k + 1, (k + 1) & 1);
+        else
+            cp_async_commit();  // an empty group keeps the count of pending groups uniform
+        cp_async_wait<1>();     // level k's copies have landed
+        const int bb = k & 1;
+        auto V = [&](int f) { return *slot(bb, f); };
+        const size_t c = MOIST_IDX(k, i);
+        const T r2_c = V(SU_R2_C), rt_c = V(SU_RT_C), rwp = V(SU_RWP);
+        T grad_m = (rt_c - V(SU_RT_M)) / dx;
+        const T grad_m_old = (V(SU_RO_C) - V(SU_RO_M)) / dx;
+        grad_m = grad_m + p.gamma_d * (grad_m - grad_m_old);
+        const T rh_m = (V(SU_R2_M) + r2_c) * T(0.5);
+        const T u_m = V(SU_RU_M) + dt_s * (V(SU_RRU_M) - rh_m * grad_m);
+        T grad_p = (V(SU_RT_P) - rt_c) / dx;
+        const T grad_p_old = (V(SU_RO_P) - V(SU_RO_C)) / dx;
+        grad_p = grad_p + p.gamma_d * (grad_p - grad_p_old);
+        const T rh_p = (r2_c + V(SU_R2_P)) * T(0.5);
+        const T u_p = V(SU_RU_C) + dt_s * (V(SU_RRU_C) - rh_p * grad_p);
+        a.ru_out[c] = u_p;
+        a.mfx[c] = V(SU_MFX) + u_p / ns_T;
+        T advection = -(u_p - u_m) / dx;
+        T inc = dt_s * (V(SU_RRHO) + advection);
+        const T rhop = V(SU_RHOP);
+        const T rho_tp = (T)((double)rhop + fact_tp64 * (double)inc);
+        a.rho_p[c] = rhop + inc;
+        const T th_c = V(SU_TH_C);
+        const T flux_ip = (V(SU_TH_P) + th_c) * T(0.5) * u_p;
+        const T flux_im = (th_c + V(SU_TH_M)) * T(0.5) * u_m;
+        advection = -(flux_ip - flux_im) / dx;
+        inc = dt_s * (V(SU_RRT) + advection);
+        const T rt_tp = (T)((double)rt_c + fact_tp64 * (double)inc);
+        a.rt_out[c] = rt_c + inc;
+        if (k >= 1) {
+            const int j = k - 1;
+            const size_t cj = c - P;
+            const T buoyancy = (rt_tp - rt_tp_prev) / (ro(z + k) - ro(z + j));
+            const T grav = -p.GRAV * T(0.5) * (rho_tp + rho_tp_prev);
+            const T rt2pres_h = (pv_r2c + r2_c) * T(0.5);
+            const T drho_w = dt_s * (pv_Rrw - rt2pres_h * buoyancy + grav);
+            const T w_j = pv_rwp;
+            const T aj = pv_ta;
+            T d = w_j + drho_w;
+            if (j > 0) d -= aj * fact * w_j;
+            d -= pv_tb * fact * w_j;
+            if (j < n - 1) d -= pv_tc * fact * rwp;
+            TT dp;
+            if (j == 0)
+                dp = (TT)d / pv_piv;
+            else
+                dp = ((TT)d - (TT)aj * dprev) / pv_piv;
+            a.dprime[cj] = dp;
+            dprev = dp;
+        }
+        rho_tp_prev = rho_tp;
+        rt_tp_prev = rt_tp;
+        pv_r2c = r2_c;
+        pv_Rrw = V(SU_RRW);
+        pv_rwp = rwp;
+        pv_ta = V(SU_TA);
+        pv_tb = V(SU_TB);
+        pv_tc = V(SU_TC);
+        pv_piv = ps[(size_t)bb * nt + tid];
+    }
+    cp_async_wait<0>();
+    // Back substitution going down fused with the vertical updates of cell k (moist.jl:
+    // 968-970, 1412-1446, 1452-1458), as in b_substep_col: at level k the faces k (w_k, known
+    // from level k + 1) and k - 1 (x_{k-1} = d'_{k-1} - c'_{k-1} x_k, computed here).
+    const T* th = a.theta;
+    // theta at k-2 .. k+2 and s.rho_w at k-1, k, kept in registers as k falls
+    T t_m2 = ke >= 2 ? ro(th + MOIST_IDX(ke - 2, i)) : T(0);
+    T t_m1 = ke >= 1 ? ro(th + MOIST_IDX(ke - 1, i)) : T(0);
+    T t_0 = ro(th + MOIST_IDX(ke, i)), t_p1 = T(0), t_p2 = T(0);
+    T sw_0 = ro(a.s_rw + MOIST_IDX(ke, i)), sw_m1 = ro(a.s_rw + MOIST_IDX(ke - 1, i));
+    T v_rho = a.rho_p[MOIST_IDX(ke, i)], v_rt = a.rt_out[MOIST_IDX(ke, i)], v_mfz = a.mfz[MOIST_IDX(ke, i)];
+    TT v_dp = dprev, v_cp = TT(0);  // d' and c' of face k - 1 (x_{ke-1} = d'_{ke-1} itself)
+    TT x = TT(0);
+    T w_k = T(0);
+    for (int k = ke; k >= 0; k--) {
+        // next level's inputs: cell k - 1 and face k - 2
+        T n_rho = T(0), n_rt = T(0), n_mfz = T(0), n_t = T(0), n_sw = T(0);
+        TT n_dp = TT(0), n_cp = TT(0);
+        if (k >= 1) {
+            const size_t cn = MOIST_IDX(k - 1, i);
+            n_rho = a.rho_p[cn];
+            n_rt = a.rt_out[cn];
+            n_mfz = a.mfz[cn];
+            if (k >= 3) n_t = ro(th + MOIST_IDX(k - 3, i));
+            if (k >= 2) {
+                n_sw = ro(a.s_rw + MOIST_IDX(k - 2, i));
+                n_dp = a.dprime[MOIST_IDX(k - 2, i)];
+                n_cp = ro(a.tcp + MOIST_IDX(k - 2, i));
+            }
+        }
+        T w_km = T(0);
+        if (k >= 1) {
+            x = (k == ke) ? v_dp : v_dp - v_cp * x;
+            w_km = (T)x;
+            a.rw_p[MOIST_IDX(k - 1, i)] = w_km;
+        }
+        const size_t c = MOIST_IDX(k, i);
+        {
+            const T flux_kp = k == ke ? T(0.0) : w_k;
+            const T flux_km = k == 0 ? T(0.0) : w_km;
+            const T adv = -(flux_kp - flux_km) / ro(dz + k);
+            a.rho_p[c] = v_rho + dt_s * adv;
+        }
+        T flux_kp, flux_km;
+        if (k == ke) {
+            flux_kp = T(0.0);
+        } else {
+            const T wp = w_k;
+            if (wp > EPS && k > 0)
+                flux_kp = up3(wp, t_m1, t_0, t_p1);
+            else if (sw_0 < -EPS && k < ke - 1)  // selector on s.rho_w, as written (1426)
+                flux_kp = up3(wp, t_p2, t_p1, t_0);
+            else
+                flux_kp = wp * f2h(t_0, t_p1, ro(dz + k), ro(dz + k + 1));
+        }
+        if (k == 0) {
+            flux_km = T(0.0);
+        } else {
+            const T wp = w_km;
+            const T sw = sw_m1;
+            if (sw > EPS && k > 1)
+                flux_km = up3(wp, t_m2, t_m1, t_0);
+            else if (sw < -EPS && k < ke)
+                flux_km = up3(wp, t_p1, t_0, t_m1);
+            else
+                flux_km = wp * f2h(t_m1, t_0, ro(dz + k - 1), ro(dz + k));
+        }
+        const T adv = -(flux_kp - flux_km) / ro(dz + k);
+        a.rt_out[c] = v_rt + dt_s * adv;
+        if (k < ke) a.mfz[c] = v_mfz + w_k / ns_T;
+        // slide the windows down one level
+        w_k = w_km;
+        t_p2 = t_p1;
+        t_p1 = t_0;
+        t_0 = t_m1;
+        t_m1 = t_m2;
+        t_m2 = n_t;
+        sw_0 = sw_m1;
+        sw_m1 = n_sw;
+        v_rho = n_rho;
+        v_rt = n_rt;
+        v_mfz = n_mfz;
+        v_dp = n_dp;
+        v_cp = n_cp;
+    }
+}
+
+
 // ----------------------------------------------------------------------------- column strips
 //
 // Strip form of the per-stage factorisation and of the acoustic substep. A block of

@@ -1758,9 +1758,10 @@ struct BatchImpl : BatchBase {
     int col_threads = BATCH_COL_THREADS;  // threads per block of the per-column kernels
     bool sub_strips = false;               // factorisation and substep over column strips instead
     int stream_minb = 1;                   // register bound of the streaming tracer sweep: 1 or 2 blocks of
-                                           // 256 threads per SM, or 3 blocks of 128 (rows <= 128)
+                                           // 256 threads per SM, or 3 or 4 blocks of 128 (rows <= 128)
     // per-column substep body: 0 b_substep_col (64 registers), 1 and 2 b_substep_col_pf (loads one
-    // level ahead; 128 and 85 registers)
+    // level ahead; 128 and 85 registers), 3 and 4 b_substep_col_async (the next level copied into
+    // shared memory; 85 and 128 registers)
     int sub_form = 1;
     std::vector<std::array<T*, 8>> tune_save;  // the members' States saved by autotune
     std::vector<T*> tune_halo;
@@ -1826,6 +1827,8 @@ struct BatchImpl : BatchBase {
                         for (unsigned bx = 0; bx < cdiv(m[i]->nx, m[i]->strip_wc); bx++) it.push_back({i, (int)bx, 0});
                 } else {
                     block = dim3(col_threads);
+                    if (kind == BK_SUB && (sub_form == 3 || sub_form == 4))
+                        smem = (size_t)col_threads * sub_async_bytes_per_thread<T, TT>();
                     for (int i = 0; i < n; i++)
                         for (unsigned bx = 0; bx < cdiv(m[i]->nx, col_threads); bx++) it.push_back({i, (int)bx, 0});
                 }
@@ -1878,6 +1881,12 @@ struct BatchImpl : BatchBase {
                 else if (sub_form == 2)
                     k_batched<BSub<T, TT>, FSubPf<T, TT>, 3><<<s.nitems, s.block, s.smem, st>>>(
                         s.items, (const BSub<T, TT>*)s.args, FSubPf<T, TT>{});
+                else if (sub_form == 3)
+                    k_batched<BSub<T, TT>, FSubAsync<T, TT>, 3><<<s.nitems, s.block, s.smem, st>>>(
+                        s.items, (const BSub<T, TT>*)s.args, FSubAsync<T, TT>{});
+                else if (sub_form == 4)
+                    k_batched<BSub<T, TT>, FSubAsync<T, TT>, 2><<<s.nitems, s.block, s.smem, st>>>(
+                        s.items, (const BSub<T, TT>*)s.args, FSubAsync<T, TT>{});
                 else
                     k_batched<BSub<T, TT>, FSub<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
                         s.items, (const BSub<T, TT>*)s.args, FSub<T, TT>{});
@@ -1889,6 +1898,9 @@ struct BatchImpl : BatchBase {
                         s.items, (const BStream<T>*)s.args, FStream<T>{});
                 else if (stream_minb == 3)  // blocks of at most 128 threads, three of them per SM
                     k_batched_b<BStream<T>, FStream<T>, 128, 3><<<s.nitems, s.block, s.smem, st>>>(
+                        s.items, (const BStream<T>*)s.args, FStream<T>{});
+                else if (stream_minb == 4)  // blocks of at most 128 threads, four of them per SM
+                    k_batched_b<BStream<T>, FStream<T>, 128, 4><<<s.nitems, s.block, s.smem, st>>>(
                         s.items, (const BStream<T>*)s.args, FStream<T>{});
                 else
                     k_batched<BStream<T>, FStream<T>, 1><<<s.nitems, s.block, s.smem, st>>>(
@@ -1987,6 +1999,10 @@ struct BatchImpl : BatchBase {
             BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BThomas<T, TT>), SINGLE_ARG(FThomasStrip<T, TT>), 4>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
             BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSubStrip<T, TT>), 4>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSubAsync<T, TT>), 3>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSubAsync<T, TT>), 2>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
         }
         for (int q = 0; q < 2; q++) {
@@ -2120,7 +2136,7 @@ struct BatchImpl : BatchBase {
             int ct, form;
         };
         std::vector<SubCand> sub_cands{{0, 0}};
-        for (int form : {1, 2, 0})
+        for (int form : {1, 3, 4, 2, 0})
             for (int ct : {32, 64, 128, 256}) sub_cands.push_back({ct, form});
         for (const SubCand& sc : sub_cands) {
             const int ct = sc.ct;
@@ -2164,8 +2180,8 @@ struct BatchImpl : BatchBase {
         // then, with that form, the register bound of the streaming tracer sweep
         int bmb = stream_minb;
         float best_mb = 1e30f;
-        for (int mb : {1, 2, 3}) {
-            if (mb == 3 && max_rows > 128) continue;  // the 128-thread bound needs rows <= 128
+        for (int mb : {1, 2, 3, 4}) {
+            if (mb >= 3 && max_rows > 128) continue;  // the 128-thread bounds need rows <= 128
             stream_minb = mb;
             if (int r = set_col_threads(bct)) return r;  // recaptures the graphs
             if (int r = copy_all(false)) return r;
