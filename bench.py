@@ -212,12 +212,21 @@ def measure_ensemble(nmem, steps, warmup, peak, plain_value):
         ms = e.time_steps(steps) / steps
         tot, g = e.profile(2)
     value = cells / (ms / 1e3)
+    # each group's algorithmic bytes per step (WORDS per cell and launch x launches per step)
+    # over its device time, against the measured HBM copy bandwidth
+    inst = group_instances(mem[0][0].ns)
+    group_frac = {}
+    for k, x in zip(GROUPS, g):
+        gms = float(x) / 2
+        if WORDS[k] and gms > 0:
+            group_frac[k] = WORDS[k] * 4 * cells * inst[k] / (gms / 1e3) / 1e9 / peak
     one = one_domain_per_launch(mem)
     return {"members": nmem, "cells": cells, "steps": steps, "warmup": warmup, "ms_per_step": ms,
             "value": value, "unit": "cell-steps/s", "vs_plain": value / plain_value,
             "one_domain_per_launch": one, "vs_one_domain_per_launch": one["ms_per_step"] / ms,
             "hbm_frac": cells * words * 4 / (ms / 1e3) / 1e9 / peak,
             "group_ms_per_step": {k: float(x) / 2 for k, x in zip(GROUPS, g)},
+            "group_hbm_frac": group_frac,
             "setup_s": setup_s, "autotune": tune,
             "workload": "%d members, nx in {256,...,2048}, nz in {64,96,128}, dx=250 m, dz=125 m, "
                         "dt=2 s, ns=8, one seeded bubble each on the analytic sounding, Float32 "

@@ -1758,7 +1758,7 @@ struct BatchImpl : BatchBase {
     int col_threads = BATCH_COL_THREADS;  // threads per block of the per-column kernels
     bool sub_strips = false;               // factorisation and substep over column strips instead
     int stream_minb = 1;                   // register bound of the streaming tracer sweep: 1 or 2 blocks of
-                                           // 256 threads per SM, or 3 or 4 blocks of 128 (rows <= 128)
+                                           // 256 threads per SM, or 3 blocks of 128 (rows <= 128)
     // per-column substep body: 0 b_substep_col (64 registers), 1 and 2 b_substep_col_pf (loads one
     // level ahead; 128 and 85 registers), 3 and 4 b_substep_col_async (the next level copied into
     // shared memory; 85 and 128 registers)
@@ -1898,9 +1898,6 @@ struct BatchImpl : BatchBase {
                         s.items, (const BStream<T>*)s.args, FStream<T>{});
                 else if (stream_minb == 3)  // blocks of at most 128 threads, three of them per SM
                     k_batched_b<BStream<T>, FStream<T>, 128, 3><<<s.nitems, s.block, s.smem, st>>>(
-                        s.items, (const BStream<T>*)s.args, FStream<T>{});
-                else if (stream_minb == 4)  // blocks of at most 128 threads, four of them per SM
-                    k_batched_b<BStream<T>, FStream<T>, 128, 4><<<s.nitems, s.block, s.smem, st>>>(
                         s.items, (const BStream<T>*)s.args, FStream<T>{});
                 else
                     k_batched<BStream<T>, FStream<T>, 1><<<s.nitems, s.block, s.smem, st>>>(
@@ -2180,8 +2177,8 @@ struct BatchImpl : BatchBase {
         // then, with that form, the register bound of the streaming tracer sweep
         int bmb = stream_minb;
         float best_mb = 1e30f;
-        for (int mb : {1, 2, 3, 4}) {
-            if (mb >= 3 && max_rows > 128) continue;  // the 128-thread bounds need rows <= 128
+        for (int mb : {1, 2, 3}) {
+            if (mb == 3 && max_rows > 128) continue;  // the 128-thread bound needs rows <= 128
             stream_minb = mb;
             if (int r = set_col_threads(bct)) return r;  // recaptures the graphs
             if (int r = copy_all(false)) return r;

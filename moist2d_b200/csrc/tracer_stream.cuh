@@ -34,15 +34,6 @@ struct StreamArgs {
     const double* rrho;  // 1 / rho in double precision, [nz][P] (Float32 fast cell)
 };
 
-// the per-row constants of the sweep
-template <class T>
-struct StreamRowC {
-    FastRow<double> fw;  // the Float32 fast cell's row (fastdiv.cuh)
-    RowRcp<T> rr;        // reciprocals of the IEEE cell
-    T dz_k, dz_kp1, dz_km1, z_k, z_kp1, z_km1;
-    T lin_km1, lin_k, lin_kp1;  // column 1 of the reference array (the linear-index clamp, moist.jl:917)
-};
-
 __device__ __forceinline__ int pmod(int c, int n) {
     const int r = c % n;
     return r < 0 ? r + n : r;
@@ -70,8 +61,7 @@ __global__ void k_stream_prep(DevParams<T> p, TracerArgs<T> a, T* s0, T* s1, T* 
 
 // one tracer t of one domain; blockDim.x = 32 * ceil(nz / 32); ring: [nwarps][2][STREAM_RING]
 template <class T>
-__device__ __forceinline__ void stream_sweep(const DevParams<T>& p, const StreamArgs<T>& a, int t, T* ring,
-                                             StreamRowC<T>* rows) {
+__device__ __forceinline__ void stream_sweep(const DevParams<T>& p, const StreamArgs<T>& a, int t, T* ring) {
     const int nx = p.nx, nz = p.nz, P = p.P, ke = nz - 1;
     const int k = threadIdx.x, lane = k & 31, w = k >> 5;
     const bool row_ok = k < nz;
@@ -92,36 +82,33 @@ __device__ __forceinline__ void stream_sweep(const DevParams<T>& p, const Stream
         return (kk >= 0 && kk < nz && c >= 0 && c < nx) ? mfz[MOIST_IDX(kk, c)] : T(0);
     };
 
-    // row constants (as the tiled sweep forms them). Float32 keeps them in shared memory (the
-    // row's own entry of `rows`), which leaves the registers to the window and the cell: the
-    // sweep then fits the register bound that lets four blocks share an SM.
-    StreamRowC<T> rcl;
-    rcl.dz_k = row_ok ? p.dz[k] : T(1);
-    rcl.dz_kp1 = (row_ok && k < ke) ? p.dz[k + 1] : T(1);
-    rcl.dz_km1 = (row_ok && k > 0) ? p.dz[k - 1] : T(1);
-    rcl.z_k = row_ok ? p.z[k] : T(0);
-    rcl.z_kp1 = (row_ok && k < ke) ? p.z[k + 1] : T(1);
-    rcl.z_km1 = (row_ok && k > 0) ? p.z[k - 1] : T(-1);
-    rcl.rr.dx = T(1) / p.dx;
-    rcl.rr.dz_k = T(1) / rcl.dz_k;
-    rcl.rr.sum_kp = T(1) / (rcl.dz_k + rcl.dz_kp1);
-    rcl.rr.sum_km = T(1) / (rcl.dz_km1 + rcl.dz_k);
-    rcl.rr.zd_kp = T(1) / (rcl.z_kp1 - rcl.z_k);
-    rcl.rr.zd_km = T(1) / (rcl.z_k - rcl.z_km1);
-    rcl.lin_km1 = (k - 1 >= 0 && k - 1 < nz) ? qo[MOIST_IDX(k - 1, nx - 2)] : T(0);
-    rcl.lin_k = row_ok ? qo[MOIST_IDX(k, nx - 2)] : T(0);
-    rcl.lin_kp1 = (k + 1 < nz) ? qo[MOIST_IDX(k + 1, nx - 2)] : T(0);
-    rcl.fw = FastRow<double>{};
+    // row constants (as the tiled sweep forms them)
+    const T dz_k = row_ok ? p.dz[k] : T(1);
+    const T dz_kp1 = (row_ok && k < ke) ? p.dz[k + 1] : T(1);
+    const T dz_km1 = (row_ok && k > 0) ? p.dz[k - 1] : T(1);
+    const T z_k = row_ok ? p.z[k] : T(0);
+    const T z_kp1 = (row_ok && k < ke) ? p.z[k + 1] : T(1);
+    const T z_km1 = (row_ok && k > 0) ? p.z[k - 1] : T(-1);
+    RowRcp<T> rr;
+    rr.dx = T(1) / p.dx;
+    rr.dz_k = T(1) / dz_k;
+    rr.sum_kp = T(1) / (dz_k + dz_kp1);
+    rr.sum_km = T(1) / (dz_km1 + dz_k);
+    rr.zd_kp = T(1) / (z_kp1 - z_k);
+    rr.zd_km = T(1) / (z_k - z_km1);
+    const T lin_km1 = (k - 1 >= 0 && k - 1 < nz) ? qo[MOIST_IDX(k - 1, nx - 2)] : T(0);
+    const T lin_k = row_ok ? qo[MOIST_IDX(k, nx - 2)] : T(0);
+    const T lin_kp1 = (k + 1 < nz) ? qo[MOIST_IDX(k + 1, nx - 2)] : T(0);
+    FastRow<double> fw{};
     if constexpr (sizeof(T) == 4) {
-        FastRow<double>& fw = rcl.fw;
         fw.dx = p.dx;
-        fw.dz_k = rcl.dz_k;
-        fw.dz_kp1 = rcl.dz_kp1;
-        fw.dz_km1 = rcl.dz_km1;
-        fw.sum_kp = rcl.dz_k + rcl.dz_kp1;
-        fw.sum_km = rcl.dz_km1 + rcl.dz_k;
-        fw.zd_kp = rcl.z_kp1 - rcl.z_k;
-        fw.zd_km = rcl.z_k - rcl.z_km1;
+        fw.dz_k = dz_k;
+        fw.dz_kp1 = dz_kp1;
+        fw.dz_km1 = dz_km1;
+        fw.sum_kp = dz_k + dz_kp1;
+        fw.sum_km = dz_km1 + dz_k;
+        fw.zd_kp = z_kp1 - z_k;
+        fw.zd_km = z_k - z_km1;
         fw.rdx = Div64::rcp(fw.dx);
         fw.rdz_k = Div64::rcp(fw.dz_k);
         fw.rsum_kp = Div64::rcp(fw.sum_kp);
@@ -137,11 +124,7 @@ __device__ __forceinline__ void stream_sweep(const DevParams<T>& p, const Stream
         fw.kp_atnm2 = k == nz - 2;
         fw.km_at0 = k - 1 == 0;
         fw.km_atnm2 = k - 1 == nz - 2;
-        rows[k] = rcl;
     }
-    const StreamRowC<T>& rc = (sizeof(T) == 4) ? rows[k] : rcl;
-    const FastRow<double>& fw = rc.fw;
-    const RowRcp<T>& rr = rc.rr;
     const bool clamp_kp_row = row_ok && (k == 0 || k == nz - 2) && k < ke;
     const bool clamp_km_row = row_ok && (k == 1 || k == nz - 1) && k >= 1;
 
@@ -226,12 +209,12 @@ __device__ __forceinline__ void stream_sweep(const DevParams<T>& p, const Stream
             const T q0_c = q0c, dph_c = dphc;
             // the clamp quotients of limited_flux_z, on the four rows that can use them
             T cl_kp = T(0), cl_km = T(0);
-            if (clamp_kp_row) cl_kp = z0 > p.EPS ? rc.lin_k / (z0 * p.dt) : rc.lin_kp1 / (-z0 * p.dt);
-            if (clamp_km_row) cl_km = mfz_km > p.EPS ? rc.lin_km1 / (mfz_km * p.dt) : rc.lin_k / (-mfz_km * p.dt);
+            if (clamp_kp_row) cl_kp = z0 > p.EPS ? lin_k / (z0 * p.dt) : lin_kp1 / (-z0 * p.dt);
+            if (clamp_km_row) cl_km = mfz_km > p.EPS ? lin_km1 / (mfz_km * p.dt) : lin_k / (-mfz_km * p.dt);
 #define MOIST_STREAM_IEEE_CELL                                                                            \
-    tracer_cell_t<DivIEEE<T>>(p, k, a.tr.dt, s0, s1, s2, s_kp1, s_kp2, prev1, prev2, s_km1, s_km2, rc.lin_km1, \
-                              rc.lin_k, rc.lin_kp1, x0, xm, z0, mfz_km, r0, r1, rm, rho_kp, rho_km, rc.dz_k,      \
-                              rc.dz_kp1, rc.dz_km1, rc.z_k, rc.z_kp1, rc.z_km1, q0_c, dph_c, rr, unused)
+    tracer_cell_t<DivIEEE<T>>(p, k, a.tr.dt, s0, s1, s2, s_kp1, s_kp2, prev1, prev2, s_km1, s_km2, lin_km1,     \
+                              lin_k, lin_kp1, x0, xm, z0, mfz_km, r0, r1, rm, rho_kp, rho_km, dz_k, dz_kp1,       \
+                              dz_km1, z_k, z_kp1, z_km1, q0_c, dph_c, rr, unused)
             if constexpr (sizeof(T) == 4) {
                 bool bad;
                 unsigned g = ~0u;
@@ -297,12 +280,7 @@ template <class T>
 __device__ __forceinline__ void b_tracer_stream(const DevParams<T>& p, const StreamArgs<T>& a, const int* err, int t) {
     __shared__ T ring[2 * (STREAM_MAX_ROWS / 32) * STREAM_RING];
     if (halted(err)) return;
-    if constexpr (sizeof(T) == 4) {
-        __shared__ StreamRowC<T> rows[STREAM_MAX_ROWS];
-        stream_sweep(p, a, t, ring, rows);
-    } else {
-        stream_sweep(p, a, t, ring, (StreamRowC<T>*)nullptr);
-    }
+    stream_sweep(p, a, t, ring);
 }
 
 // single domain: block t sweeps tracer t
