@@ -187,10 +187,10 @@ struct FSubPf {
         b_substep_col_pf<T, TT>(a.p, a.a, a.dt_s, a.ns_T, a.fact_tp64, a.err, bx);
     }
 };
-template <class T, class TT>
+template <class T, class TT, int NBUF>
 struct FSubAsync {
     __device__ void operator()(const BSub<T, TT>& a, int bx, int) const {
-        b_substep_col_async<T, TT>(a.p, a.a, a.dt_s, a.ns_T, a.fact_tp64, a.err, bx);
+        b_substep_col_async<T, TT, NBUF>(a.p, a.a, a.dt_s, a.ns_T, a.fact_tp64, a.err, bx);
     }
 };
 // the same two kernels over column strips (for ensembles too small to fill the GPU with columns)

@@ -955,17 +955,17 @@ enum {
     SU_RRU_M, SU_RRU_C, SU_MFX, SU_RRHO, SU_RHOP, SU_TH_C, SU_TH_P, SU_TH_M, SU_RRT, SU_RRW, SU_RWP, SU_TA,
     SU_TB, SU_TC, SU_NV
 };
-// shared memory of b_substep_col_async per thread: two levels of the SU_NV inputs and the pivot
+// shared memory of b_substep_col_async per thread: nbuf levels of the SU_NV inputs and the pivot
 template <class T, class TT>
-__host__ __device__ constexpr size_t sub_async_bytes_per_thread() {
-    return 2 * (SU_NV * sizeof(T) + sizeof(TT));
+__host__ __device__ constexpr size_t sub_async_bytes_per_thread(int nbuf) {
+    return (size_t)nbuf * (SU_NV * sizeof(T) + sizeof(TT));
 }
 
-// b_substep_col_pf with the next level's inputs brought in by asynchronous copies into this
-// thread's slots of shared memory instead of registers: the copies of level k + 1 run during
-// level k's arithmetic, and the registers they would hold are free, so more warps fit on an
-// SM. Same arithmetic, operation for operation; the downward pass is b_substep_col_pf's.
-template <class T, class TT>
+// b_substep_col_pf with the next levels' inputs brought in by asynchronous copies into this
+// thread's slots of shared memory instead of registers: the copies of levels k + 1 .. k + NBUF - 1
+// run during level k's arithmetic, and the registers they would hold are free, so more warps fit
+// on an SM. Same arithmetic, operation for operation; the downward pass is b_substep_col_pf's.
+template <class T, class TT, int NBUF>
 __device__ __forceinline__ void b_substep_col_async(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T,
                                                     double fact_tp64, const int* err, int bx) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -981,8 +981,8 @@ __device__ __forceinline__ void b_substep_col_async(DevParams<T> p, SubArgs<T, T
     const T fact_tpT = T(0.5) * (T(1.0) + p.beta);
     const T fact_tmT = T(0.5) * (T(1.0) - p.beta);
     const T fact = fact_tmT / fact_tpT;
-    T* fs = reinterpret_cast<T*>(smem_raw);                                          // [2][SU_NV][nt]
-    TT* ps = reinterpret_cast<TT*>(smem_raw + (size_t)2 * SU_NV * nt * sizeof(T));  // [2][nt]
+    T* fs = reinterpret_cast<T*>(smem_raw);                                             // [NBUF][SU_NV][nt]
+    TT* ps = reinterpret_cast<TT*>(smem_raw + (size_t)NBUF * SU_NV * nt * sizeof(T));  // [NBUF][nt]
     auto slot = [&](int b, int f) { return fs + ((size_t)(b * SU_NV + f) * nt + tid); };
     auto issue = [&](int k, int b) {
         const size_t c = MOIST_IDX(k, i), cm = MOIST_IDX(k, im), cp = MOIST_IDX(k, ip);
@@ -1014,19 +1014,24 @@ __device__ __forceinline__ void b_substep_col_async(DevParams<T> p, SubArgs<T, T
         cp_async(ps + (size_t)b * nt + tid, a.tpiv + c);
         cp_async_commit();
     };
-    issue(0, 0);
+    for (int q = 0; q < NBUF - 1; q++) {  // levels 0 .. NBUF - 2 in flight before the walk starts
+        if (q < nz)
+            issue(q, q);
+        else
+            cp_async_commit();
+    }
     // face k - 1 values the next level uses: R_rho_w, rho_w_p, the factors, the pivot, rt2pres
     T pv_r2c = T(0), pv_Rrw = T(0), pv_rwp = T(0), pv_ta = T(0), pv_tb = T(0), pv_tc = T(0);
     TT pv_piv = TT(1);
     T rho_tp_prev = T(0), rt_tp_prev = T(0);
     TT dprev = TT(0);
     for (int k = 0; k < nz; k++) {
-        if (k + 1 < nz)
-            issue(k + 1, (k + 1) & 1);
+        if (k + NBUF - 1 < nz)
+            issue(k + NBUF - 1, (k + NBUF - 1) % NBUF);
         else
-            cp_async_commit();  // an empty group keeps the count of pending groups uniform
-        cp_async_wait<1>();     // level k's copies have landed
-        const int bb = k & 1;
+            cp_async_commit();     // an empty group keeps the count of pending groups uniform
+        cp_async_wait<NBUF - 1>();  // level k's copies have landed
+        const int bb = k % NBUF;
         auto V = [&](int f) { return *slot(bb, f); };
         const size_t c = MOIST_IDX(k, i);
         const T r2_c = V(SU_R2_C), rt_c = V(SU_RT_C), rwp = V(SU_RWP);

@@ -1752,8 +1752,23 @@ struct BatchImpl : BatchBase {
         size_t smem;
         const BItem* items;
         const void* args;
+        int group;
     };
+    // the packed launches of the even and odd step: kind and the members' argument structs
+    struct Launch {
+        int kind;
+        const void* args;
+    };
+    std::vector<Launch> launches[2];
+    // per parity: the launches of member group 0, then of group 1, ...; the groups' chains are
+    // parallel branches of the step graph, so one group's kernels fill the SMs that another
+    // group's long members leave idle at the end of a launch
     std::vector<Slot> slots[2];
+    static constexpr int MAX_GROUPS = 4;
+    int ngroups = 1;
+    std::vector<int> grp;  // group of each member
+    cudaStream_t gstream[MAX_GROUPS] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t gfork = nullptr, gjoin[MAX_GROUPS] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<void*> allocs;
     int col_threads = BATCH_COL_THREADS;  // threads per block of the per-column kernels
     bool sub_strips = false;               // factorisation and substep over column strips instead
@@ -1761,8 +1776,8 @@ struct BatchImpl : BatchBase {
                                            // 256 threads per SM, or 3 blocks of 128 (rows <= 128)
     // per-column substep body: 0 b_substep_col (64 registers), 1 and 2 b_substep_col_pf (loads one
     // level ahead; 128 and 85 registers), 3 and 4 b_substep_col_async (the next level copied into
-    // shared memory; 85 and 128 registers)
-    int sub_form = 1;
+    // shared memory; 85 and 128 registers), 5 the same two levels ahead (128 registers)
+    int sub_form = 4;
     std::vector<std::array<T*, 8>> tune_save;  // the members' States saved by autotune
     std::vector<T*> tune_halo;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
@@ -1777,6 +1792,12 @@ struct BatchImpl : BatchBase {
         if (st) cudaStreamSynchronize(st);
         for (auto& e : exec)
             if (e) cudaGraphExecDestroy(e);
+        for (int g = 1; g < MAX_GROUPS; g++) {
+            if (gstream[g]) cudaStreamDestroy(gstream[g]);
+            if (gjoin[g]) cudaEventDestroy(gjoin[g]);
+        }
+        if (gfork) cudaEventDestroy(gfork);
+        for (void* a : item_allocs) cudaFree(a);
         for (void* a : allocs) cudaFree(a);
     }
 
@@ -1791,9 +1812,10 @@ struct BatchImpl : BatchBase {
     }
 
     // (member, block) items of one launch kind
-    void items_of(int kind, std::vector<BItem>& it, dim3& block, size_t& smem) {
+    void items_of(int kind, std::vector<BItem>& it, dim3& block, size_t& smem, int group) {
         const int n = (int)m.size();
         smem = 0;
+        auto in_group = [&](int i) { return grp[i] == group; };
         auto cells = [&](int i) {
             for (unsigned by = 0; by < cdiv(m[i]->nz, 8); by++)
                 for (unsigned bx = 0; bx < cdiv(m[i]->nx, 32); bx++) it.push_back({i, (int)bx, (int)by});
@@ -1801,14 +1823,16 @@ struct BatchImpl : BatchBase {
         switch (kind) {
             case BK_MEMSET:
                 block = dim3(256);
-                for (int i = 0; i < n; i++) it.push_back({i, 0, 0});
+                for (int i = 0; i < n; i++)
+                    if (in_group(i)) it.push_back({i, 0, 0});
                 break;
             case BK_SF:
             case BK_RD:
             case BK_PREC:
                 block = dim3(128);
                 for (int i = 0; i < n; i++)
-                    for (unsigned bx = 0; bx < cdiv(m[i]->nx, 128); bx++) it.push_back({i, (int)bx, 0});
+                    if (in_group(i))
+                        for (unsigned bx = 0; bx < cdiv(m[i]->nx, 128); bx++) it.push_back({i, (int)bx, 0});
                 break;
             case BK_PHYS:
             case BK_DIAG:
@@ -1816,7 +1840,8 @@ struct BatchImpl : BatchBase {
             case BK_UPD:
             case BK_PREP:
                 block = dim3(32, 8);
-                for (int i = 0; i < n; i++) cells(i);
+                for (int i = 0; i < n; i++)
+                    if (in_group(i)) cells(i);
                 break;
             case BK_THOMAS:
             case BK_SUB:
@@ -1824,13 +1849,15 @@ struct BatchImpl : BatchBase {
                     block = dim3(STRIP_THREADS);
                     smem = max_strip_smem;
                     for (int i = 0; i < n; i++)
-                        for (unsigned bx = 0; bx < cdiv(m[i]->nx, m[i]->strip_wc); bx++) it.push_back({i, (int)bx, 0});
+                        if (in_group(i))
+                            for (unsigned bx = 0; bx < cdiv(m[i]->nx, m[i]->strip_wc); bx++) it.push_back({i, (int)bx, 0});
                 } else {
                     block = dim3(col_threads);
-                    if (kind == BK_SUB && (sub_form == 3 || sub_form == 4))
-                        smem = (size_t)col_threads * sub_async_bytes_per_thread<T, TT>();
+                    if (kind == BK_SUB && sub_form >= 3)
+                        smem = (size_t)col_threads * sub_async_bytes_per_thread<T, TT>(sub_form == 5 ? 3 : 2);
                     for (int i = 0; i < n; i++)
-                        for (unsigned bx = 0; bx < cdiv(m[i]->nx, col_threads); bx++) it.push_back({i, (int)bx, 0});
+                        if (in_group(i))
+                            for (unsigned bx = 0; bx < cdiv(m[i]->nx, col_threads); bx++) it.push_back({i, (int)bx, 0});
                 }
                 break;
             case BK_STREAM: {
@@ -1838,6 +1865,7 @@ struct BatchImpl : BatchBase {
                 block = dim3(max_rows);
                 std::vector<int> order(n);
                 for (int i = 0; i < n; i++) order[i] = i;
+                order.erase(std::remove_if(order.begin(), order.end(), [&](int i) { return !in_group(i); }), order.end());
                 std::stable_sort(order.begin(), order.end(),
                                  [&](int a, int b) { return m[a]->nx + m[a]->nz > m[b]->nx + m[b]->nz; });
                 for (int i : order)
@@ -1846,16 +1874,17 @@ struct BatchImpl : BatchBase {
             }
             case BK_STAGE_END:
                 block = dim3(32);
-                for (int i = 0; i < n; i++) it.push_back({i, 0, 0});
+                for (int i = 0; i < n; i++)
+                    if (in_group(i)) it.push_back({i, 0, 0});
                 break;
         }
     }
 
 #define BATCH_LAUNCH(KIND, A, F, MINB)                                                                 \
     case KIND:                                                                                         \
-        k_batched<A, F, MINB><<<s.nitems, s.block, s.smem, st>>>(s.items, (const A*)s.args, F{});     \
+        k_batched<A, F, MINB><<<s.nitems, s.block, s.smem, ls>>>(s.items, (const A*)s.args, F{});     \
         break;
-    int launch(const Slot& s) {
+    int launch(const Slot& s, cudaStream_t ls) {
         switch (s.kind) {
             BATCH_LAUNCH(BK_MEMSET, BMemset, FMemset, 1)
             BATCH_LAUNCH(BK_SF, BSf<T>, FSf<T>, 1)
@@ -1865,42 +1894,45 @@ struct BatchImpl : BatchBase {
             BATCH_LAUNCH(BK_TEND, BTend<T>, FTend<T>, 4)
             case BK_THOMAS:
                 if (sub_strips)
-                    k_batched<BThomas<T, TT>, FThomasStrip<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
+                    k_batched<BThomas<T, TT>, FThomasStrip<T, TT>, 4><<<s.nitems, s.block, s.smem, ls>>>(
                         s.items, (const BThomas<T, TT>*)s.args, FThomasStrip<T, TT>{});
                 else
-                    k_batched<BThomas<T, TT>, FThomas<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
+                    k_batched<BThomas<T, TT>, FThomas<T, TT>, 4><<<s.nitems, s.block, s.smem, ls>>>(
                         s.items, (const BThomas<T, TT>*)s.args, FThomas<T, TT>{});
                 break;
             case BK_SUB:
                 if (sub_strips)
-                    k_batched<BSub<T, TT>, FSubStrip<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
+                    k_batched<BSub<T, TT>, FSubStrip<T, TT>, 4><<<s.nitems, s.block, s.smem, ls>>>(
                         s.items, (const BSub<T, TT>*)s.args, FSubStrip<T, TT>{});
                 else if (sub_form == 1)
-                    k_batched<BSub<T, TT>, FSubPf<T, TT>, 2><<<s.nitems, s.block, s.smem, st>>>(
+                    k_batched<BSub<T, TT>, FSubPf<T, TT>, 2><<<s.nitems, s.block, s.smem, ls>>>(
                         s.items, (const BSub<T, TT>*)s.args, FSubPf<T, TT>{});
                 else if (sub_form == 2)
-                    k_batched<BSub<T, TT>, FSubPf<T, TT>, 3><<<s.nitems, s.block, s.smem, st>>>(
+                    k_batched<BSub<T, TT>, FSubPf<T, TT>, 3><<<s.nitems, s.block, s.smem, ls>>>(
                         s.items, (const BSub<T, TT>*)s.args, FSubPf<T, TT>{});
                 else if (sub_form == 3)
-                    k_batched<BSub<T, TT>, FSubAsync<T, TT>, 3><<<s.nitems, s.block, s.smem, st>>>(
-                        s.items, (const BSub<T, TT>*)s.args, FSubAsync<T, TT>{});
+                    k_batched<BSub<T, TT>, SINGLE_ARG(FSubAsync<T, TT, 2>), 3><<<s.nitems, s.block, s.smem, ls>>>(
+                        s.items, (const BSub<T, TT>*)s.args, FSubAsync<T, TT, 2>{});
                 else if (sub_form == 4)
-                    k_batched<BSub<T, TT>, FSubAsync<T, TT>, 2><<<s.nitems, s.block, s.smem, st>>>(
-                        s.items, (const BSub<T, TT>*)s.args, FSubAsync<T, TT>{});
+                    k_batched<BSub<T, TT>, SINGLE_ARG(FSubAsync<T, TT, 2>), 2><<<s.nitems, s.block, s.smem, ls>>>(
+                        s.items, (const BSub<T, TT>*)s.args, FSubAsync<T, TT, 2>{});
+                else if (sub_form == 5)
+                    k_batched<BSub<T, TT>, SINGLE_ARG(FSubAsync<T, TT, 3>), 2><<<s.nitems, s.block, s.smem, ls>>>(
+                        s.items, (const BSub<T, TT>*)s.args, FSubAsync<T, TT, 3>{});
                 else
-                    k_batched<BSub<T, TT>, FSub<T, TT>, 4><<<s.nitems, s.block, s.smem, st>>>(
+                    k_batched<BSub<T, TT>, FSub<T, TT>, 4><<<s.nitems, s.block, s.smem, ls>>>(
                         s.items, (const BSub<T, TT>*)s.args, FSub<T, TT>{});
                 break;
             BATCH_LAUNCH(BK_PREP, BPrep<T>, FPrep<T>, 4)
             case BK_STREAM:
                 if (stream_minb == 2)  // registers bounded so that twice the blocks fit on an SM
-                    k_batched<BStream<T>, FStream<T>, 2><<<s.nitems, s.block, s.smem, st>>>(
+                    k_batched<BStream<T>, FStream<T>, 2><<<s.nitems, s.block, s.smem, ls>>>(
                         s.items, (const BStream<T>*)s.args, FStream<T>{});
                 else if (stream_minb == 3)  // blocks of at most 128 threads, three of them per SM
-                    k_batched_b<BStream<T>, FStream<T>, 128, 3><<<s.nitems, s.block, s.smem, st>>>(
+                    k_batched_b<BStream<T>, FStream<T>, 128, 3><<<s.nitems, s.block, s.smem, ls>>>(
                         s.items, (const BStream<T>*)s.args, FStream<T>{});
                 else
-                    k_batched<BStream<T>, FStream<T>, 1><<<s.nitems, s.block, s.smem, st>>>(
+                    k_batched<BStream<T>, FStream<T>, 1><<<s.nitems, s.block, s.smem, ls>>>(
                         s.items, (const BStream<T>*)s.args, FStream<T>{});
                 break;
             BATCH_LAUNCH(BK_UPD, BUpd<T>, FUpd<T>, 4)
@@ -1997,9 +2029,11 @@ struct BatchImpl : BatchBase {
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
             BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSubStrip<T, TT>), 4>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-            BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSubAsync<T, TT>), 3>,
+            BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSubAsync<T, TT, 2>), 3>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
-            BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSubAsync<T, TT>), 2>,
+            BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSubAsync<T, TT, 2>), 2>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSubAsync<T, TT, 3>), 2>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
         }
         for (int q = 0; q < 2; q++) {
@@ -2016,30 +2050,69 @@ struct BatchImpl : BatchBase {
                     return set_berr(owner, MOIST_ERR_ARG,
                                     "member %d takes other launches than member 0 (ns, do_sf and do_rd must agree)", i);
             for (size_t j = 0; j < rec[0].kind.size(); j++) {
-                Slot sl{};
-                sl.kind = rec[0].kind[j];
                 const size_t sz = rec[0].args[j].size();
                 std::vector<unsigned char> packed(sz * n);
                 for (int i = 0; i < n; i++) std::memcpy(packed.data() + sz * i, rec[i].args[j].data(), sz);
-                std::vector<BItem> it;
-                items_of(sl.kind, it, sl.block, sl.smem);
-                sl.nitems = (unsigned)it.size();
                 unsigned char* dargs;
-                BItem* ditems;
                 if (int r = dalloc(&dargs, packed.size())) return r;
-                if (int r = dalloc(&ditems, it.size())) return r;
                 BCK(cudaMemcpy(dargs, packed.data(), packed.size(), cudaMemcpyHostToDevice));
-                BCK(cudaMemcpy(ditems, it.data(), it.size() * sizeof(BItem), cudaMemcpyHostToDevice));
-                sl.items = ditems;
-                sl.args = dargs;
-                slots[q].push_back(sl);
+                launches[q].push_back(Launch{rec[0].kind[j], dargs});
             }
         }
+        for (int g = 1; g < MAX_GROUPS; g++) {
+            BCK(cudaStreamCreateWithFlags(&gstream[g], cudaStreamNonBlocking));
+            BCK(cudaEventCreateWithFlags(&gjoin[g], cudaEventDisableTiming));
+        }
+        BCK(cudaEventCreateWithFlags(&gfork, cudaEventDisableTiming));
+        assign_groups(1);
         std::vector<int*> ev(n);
         for (int i = 0; i < n; i++) ev[i] = m[i]->err;
         if (int r = dalloc(&errs, n)) return r;
         if (int r = dalloc(&err_all, 4 * n)) return r;
         BCK(cudaMemcpy(errs, ev.data(), n * sizeof(int*), cudaMemcpyHostToDevice));
+        return rebuild_slots();
+    }
+
+    // G groups of members, dealt in turn from the longest sweeps (nx + nz) down, so that every
+    // group holds long and short members
+    void assign_groups(int G) {
+        const int n = (int)m.size();
+        ngroups = std::max(1, std::min(G, n));
+        std::vector<int> order(n);
+        for (int i = 0; i < n; i++) order[i] = i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return m[a]->nx + m[a]->nz > m[b]->nx + m[b]->nz; });
+        grp.assign(n, 0);
+        for (int r = 0; r < n; r++) grp[order[r]] = r % ngroups;
+    }
+
+    // the work lists of every launch for the current groups, forms and block sizes, and new graphs
+    std::vector<void*> item_allocs;
+    int rebuild_slots() {
+        BCK(cudaStreamSynchronize(st));  // no graph that reads the old work lists is in flight
+        for (void* a : item_allocs) cudaFree(a);
+        item_allocs.clear();
+        for (int q = 0; q < 2; q++) {
+            slots[q].clear();
+            for (int g = 0; g < ngroups; g++)
+                for (const Launch& L : launches[q]) {
+                    Slot sl{};
+                    sl.kind = L.kind;
+                    sl.args = L.args;
+                    sl.group = g;
+                    std::vector<BItem> it;
+                    items_of(sl.kind, it, sl.block, sl.smem, g);
+                    if (it.empty()) continue;
+                    void* d = nullptr;
+                    cudaError_t e = cudaMalloc(&d, it.size() * sizeof(BItem));
+                    if (e != cudaSuccess) return set_berr(owner, MOIST_ERR_NOMEM, "cudaMalloc of a work list failed");
+                    item_allocs.push_back(d);
+                    BCK(cudaMemcpy(d, it.data(), it.size() * sizeof(BItem), cudaMemcpyHostToDevice));
+                    sl.items = (const BItem*)d;
+                    sl.nitems = (unsigned)it.size();
+                    slots[q].push_back(sl);
+                }
+        }
         return capture();
     }
 
@@ -2053,9 +2126,21 @@ struct BatchImpl : BatchBase {
             cudaGraph_t g;
             BCK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             int r = MOIST_OK;
-            for (const Slot& sl : slots[q])
-                if ((r = launch(sl)) != MOIST_OK) break;
+            cudaError_t ef = cudaSuccess;
+            if (ngroups > 1) {  // fork: the groups' chains become parallel branches of the graph
+                ef = cudaEventRecord(gfork, st);
+                for (int g2 = 1; g2 < ngroups && ef == cudaSuccess; g2++) ef = cudaStreamWaitEvent(gstream[g2], gfork, 0);
+            }
+            for (const Slot& sl : slots[q]) {
+                if (ef != cudaSuccess) break;
+                if ((r = launch(sl, sl.group == 0 ? st : gstream[sl.group])) != MOIST_OK) break;
+            }
+            for (int g2 = 1; g2 < ngroups; g2++) {  // join every branch back before the capture ends
+                cudaEventRecord(gjoin[g2], gstream[g2]);
+                cudaStreamWaitEvent(st, gjoin[g2], 0);
+            }
             cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (ef != cudaSuccess && e == cudaSuccess) e = ef;
             if (r != MOIST_OK) return r;
             if (e != cudaSuccess) return set_berr(owner, MOIST_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
             e = cudaGraphInstantiate(&exec[q], g, 0);
@@ -2070,18 +2155,7 @@ struct BatchImpl : BatchBase {
     int set_col_threads(int ct) {
         sub_strips = ct == 0;
         if (ct > 0) col_threads = ct;
-        for (int q = 0; q < 2; q++)
-            for (Slot& sl : slots[q]) {
-                if (sl.kind != BK_SUB && sl.kind != BK_THOMAS) continue;
-                std::vector<BItem> it;
-                items_of(sl.kind, it, sl.block, sl.smem);
-                BItem* ditems;
-                if (int r = dalloc(&ditems, it.size())) return r;
-                BCK(cudaMemcpy(ditems, it.data(), it.size() * sizeof(BItem), cudaMemcpyHostToDevice));
-                sl.items = ditems;
-                sl.nitems = (unsigned)it.size();
-            }
-        return capture();
+        return rebuild_slots();
     }
 
     // Times nsteps batch steps for the factorisation and acoustic substep over column strips and
@@ -2133,7 +2207,7 @@ struct BatchImpl : BatchBase {
             int ct, form;
         };
         std::vector<SubCand> sub_cands{{0, 0}};
-        for (int form : {1, 3, 4, 2, 0})
+        for (int form : {4, 5, 3, 1, 2, 0})
             for (int ct : {32, 64, 128, 256}) sub_cands.push_back({ct, form});
         for (const SubCand& sc : sub_cands) {
             const int ct = sc.ct;
@@ -2206,14 +2280,46 @@ struct BatchImpl : BatchBase {
         }
         best = best_mb;
         stream_minb = bmb;
+        // then the number of member groups whose chains run as parallel branches of the graph
+        int bg = 1;
+        float best_g = best;
+        for (int G : {2, 4}) {
+            if (G > (int)m.size()) continue;
+            assign_groups(G);
+            if (int r = set_col_threads(bct)) return r;  // new work lists and graphs
+            if (int r = copy_all(false)) return r;
+            float ms = 0.f;
+            if (int r = launch_steps(1)) return r;
+            if (int r = time_steps(nsteps, &ms)) return r;
+            BCK(cudaMemsetAsync(hb, 0, sizeof(unsigned long long), st));
+            for (int i = 0; i < n; i++) {
+                const auto cf = m[i]->cur_fields();
+                for (int f = 0; f < 7; f++) k_hash<T><<<64, 256, 0, st>>>(cf[f], m[i]->fsz, hb);
+                k_hash<T><<<1, 256, 0, st>>>(m[i]->prec, (size_t)m[i]->P, hb);
+            }
+            unsigned long long h = 0;
+            BCK(cudaMemcpyAsync(&h, hb, sizeof h, cudaMemcpyDeviceToHost, st));
+            BCK(cudaStreamSynchronize(st));
+            if (h != h0) return set_berr(owner, MOIST_ERR_CUDA, "autotune: %d member groups give other States", G);
+            ms /= nsteps;
+            snprintf(buf, sizeof buf, "; %d groups: %.2f ms", G, ms);
+            report += buf;
+            if (ms < best_g) {
+                best_g = ms;
+                bg = G;
+            }
+        }
+        best = best_g;
+        assign_groups(bg);
         if (int r = set_col_threads(bct)) return r;
         if (int r = copy_all(false)) return r;
         BCK(cudaStreamSynchronize(st));
         if (bct == 0)
-            snprintf(buf, sizeof buf, " -> column strips, tracer bound %d (%.2f ms per step)", bmb, best);
+            snprintf(buf, sizeof buf, " -> column strips, tracer bound %d, %d groups (%.2f ms per step)", bmb, ngroups,
+                     best);
         else
-            snprintf(buf, sizeof buf, " -> column block %d form %d, tracer bound %d (%.2f ms per step)", bct, sub_form,
-                     bmb, best);
+            snprintf(buf, sizeof buf, " -> column block %d form %d, tracer bound %d, %d groups (%.2f ms per step)", bct,
+                     sub_form, bmb, ngroups, best);
         report += buf;
         return MOIST_OK;
     }
@@ -2271,7 +2377,7 @@ struct BatchImpl : BatchBase {
         BCK(cudaEventRecord(ev[j++], st));
         for (int n = 0; n < nsteps; n++) {
             for (const Slot& sl : slots[parity]) {
-                if (int r = launch(sl)) return r;
+                if (int r = launch(sl, st)) return r;
                 kinds.push_back(sl.kind);
                 BCK(cudaEventRecord(ev[j++], st));
             }
