@@ -552,20 +552,28 @@ __device__ __forceinline__ void b_thomas_col(DevParams<T> p, const T* theta, con
     const int i = bx * blockDim.x + threadIdx.x;
     const int nx = p.nx, nz = p.nz, P = p.P;
     if (i >= nx || halted(err)) return;
-    const T* dz = p.dz;
-    const T* z = p.z;
     const int ke = nz - 1, n = nz - 1;
     const T fact_tp = T(0.5) * (T(1.0) + p.beta);
     const T dt_tp2 = (dt_s * fact_tp) * (dt_s * fact_tp);
-    T th_prev = T(0), th_cur = f2h(ro(theta + MOIST_IDX(0, i)), ro(theta + MOIST_IDX(1, i)), dz[0], dz[1]);
+    // the walk keeps theta, rt2pres, dz and z of the levels it needs in registers and reads the
+    // next level's new values one level ahead, so that no level waits for its loads
+    auto TH = [&](int kk) { return kk <= ke ? ro(theta + MOIST_IDX(kk, i)) : T(0); };
+    auto R2 = [&](int kk) { return kk <= ke ? ro(rt2pres + MOIST_IDX(kk, i)) : T(0); };
+    auto DZ = [&](int kk) { return kk <= ke ? ro(p.dz + kk) : T(1); };
+    auto ZZ = [&](int kk) { return kk <= ke ? ro(p.z + kk) : T(0); };
+    T t1 = TH(1), t2 = TH(2);          // theta at k+1, k+2
+    T rk = R2(0), rkp = R2(1);         // rt2pres at k, k+1
+    T d0 = DZ(0), d1 = DZ(1), d2 = DZ(2);  // dz at k, k+1, k+2
+    T z0 = ZZ(0), z1 = ZZ(1);          // z at k, k+1
+    T th_prev = T(0), th_cur = f2h(TH(0), t1, d0, d1);
     TT cp_prev = TT(0);
     for (int j = 0; j < n; j++) {
         const int k = j;
-        const T th_next = (k + 1 <= ke - 1) ? f2h(ro(theta + MOIST_IDX(k + 1, i)), ro(theta + MOIST_IDX(k + 2, i)), dz[k + 1], dz[k + 2]) : T(0);
-        const T r_k = ro(rt2pres + MOIST_IDX(k, i)), r_kp = ro(rt2pres + MOIST_IDX(k + 1, i));
-        const T b = dt_tp2 * (r_k / dz[k] + r_kp / dz[k + 1]) * th_cur / (z[k + 1] - z[k]);
-        const T a = (k > 0) ? -dt_tp2 * (r_k * th_prev / ((z[k + 1] - z[k]) * dz[k]) - p.GRAV / (dz[k] + dz[k + 1])) : T(0);
-        const T c = (k < ke - 1) ? -dt_tp2 * (r_kp * th_next / ((z[k + 1] - z[k]) * dz[k + 1]) + p.GRAV / (dz[k] + dz[k + 1])) : T(0);
+        const T n_t = TH(k + 3), n_r = R2(k + 2), n_d = DZ(k + 3), n_z = ZZ(k + 2);
+        const T th_next = (k + 1 <= ke - 1) ? f2h(t1, t2, d1, d2) : T(0);
+        const T b = dt_tp2 * (rk / d0 + rkp / d1) * th_cur / (z1 - z0);
+        const T a = (k > 0) ? -dt_tp2 * (rk * th_prev / ((z1 - z0) * d0) - p.GRAV / (d0 + d1)) : T(0);
+        const T c = (k < ke - 1) ? -dt_tp2 * (rkp * th_next / ((z1 - z0) * d1) + p.GRAV / (d0 + d1)) : T(0);
         ta[MOIST_IDX(j, i)] = a;
         tb[MOIST_IDX(j, i)] = b;
         tc[MOIST_IDX(j, i)] = c;
@@ -583,6 +591,15 @@ __device__ __forceinline__ void b_thomas_col(DevParams<T> p, const T* theta, con
         cp_prev = cpj;
         th_prev = th_cur;
         th_cur = th_next;
+        t1 = t2;
+        t2 = n_t;
+        rk = rkp;
+        rkp = n_r;
+        d0 = d1;
+        d1 = d2;
+        d2 = n_d;
+        z0 = z1;
+        z1 = n_z;
     }
 }
 
