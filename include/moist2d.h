@@ -81,7 +81,11 @@ enum {
     MOIST_FLAG_TRACER_WAVEFRONT = 2,
     /* Run the tracer transport as one exact row-streaming wavefront per tracer (one thread per
      * row; no repair passes; same results bit for bit). Needs nz <= 256. */
-    MOIST_FLAG_TRACER_STREAM = 4
+    MOIST_FLAG_TRACER_STREAM = 4,
+    /* Run the tiled tracer sweep without grid-wide passes: each tile publishes numbered versions
+     * of its boundary strips and recomputes as soon as its left or lower neighbour publishes a
+     * new one (same results bit for bit). */
+    MOIST_FLAG_TRACER_DATAFLOW = 8
 };
 
 /*
@@ -464,7 +468,8 @@ int moist_tracer_pass_counts(moist_ctx* ctx, int* counts, int n);
 
 /* Bound of the device-side waits of the context's kernels (no counterpart in the reference,
  * whose threads never wait on one another). The tiled tracer sweep's blocks wait for each
- * other between repair passes; every such wait gives up after `cycles` SM clock cycles
+ * other between repair passes, or in its dataflow form (MOIST_FLAG_TRACER_DATAFLOW) for their
+ * left and lower neighbours' new strips; every such wait gives up after `cycles` SM clock cycles
  * (cycles <= 0 restores the default, about two seconds), and the step then returns
  * MOIST_ERR_TIMEOUT, leaving the context's State undefined (upload a State before stepping
  * again). Meant for tests of that path. MOIST_ERR_UNSUPPORTED when the context's tracer sweep
@@ -476,7 +481,10 @@ int moist_set_wait_limit(moist_ctx* ctx, long long cycles);
  * npasses[w] = passes run; pass_ns[w*maxrec + q] = duration of pass q+1 in ns (from its start to
  * the next pass's start, the last one to the moment block 0 leaves the sweep);
  * pass_tiles[w*maxrec + q] = tile-tracer warps that recomputed in that pass (3 per tile at most).
- * Any output pointer may be NULL. Allocates its timing buffers per call. */
+ * In the dataflow form a "pass" is a tile's q-th computation: npasses is the largest count of
+ * any tile, pass_tiles counts the tile-tracer warps that computed a q-th time, and pass_ns is the
+ * difference between the latest starts of computations q+1 and q+2 (or the end). Any output
+ * pointer may be NULL. Allocates its timing buffers per call. */
 int moist_tracer_pass_trace(moist_ctx* ctx, int nsteps, int maxrec, long long* pass_ns, int* pass_tiles,
                             int* npasses);
 

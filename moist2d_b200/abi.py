@@ -19,6 +19,7 @@ MOIST_ERR_IO = 7
 MOIST_FLAG_TRI_NATIVE = 1
 MOIST_FLAG_TRACER_WAVEFRONT = 2
 MOIST_FLAG_TRACER_STREAM = 4
+MOIST_FLAG_TRACER_DATAFLOW = 8
 MOIST_NDIAG = 10
 
 MOIST_KGROUP_PHYSICS = 0

@@ -230,6 +230,7 @@ struct Ctx : CtxBase {
     bool rd_dirty = true;
     // tiled tracer sweep (tracer_tiles.cuh)
     bool use_tiles = false;
+    bool tiles_df = false;  // the tiled sweep without grid barriers (per-tile versions)
     TileCtl tctl{};
     T* strips = nullptr;
     int* pass_hist = nullptr;  // [64] sweeps that converged after p passes
@@ -457,10 +458,12 @@ struct Ctx : CtxBase {
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-        CK(cudaFuncSetAttribute(k_tracer_tiles<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tracer_tiles<T>, 96, tile_smem));
+        CK(cudaFuncSetAttribute(k_tracer_tiles<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_tracer_tiles<T, false>, 96, tile_smem));
         if (!coop || (long)nb * nsm < tctl.ntiles) return MOIST_OK;
-        AL(strips, (size_t)2 * 3 * tctl.ntiles * 4 * TT_W);
+        // the barrier sweep uses two parities of strips, the dataflow sweep TT_RING versions
+        AL(strips, (size_t)std::max(2, TT_RING) * 3 * tctl.ntiles * 4 * TT_W);
+        AL(tctl.ver, (size_t)3 * tctl.ntiles);
         AL(tctl.bar, 2);
         AL(tctl.changed, (size_t)2 * 3 * tctl.ntiles * 2);
         AL(tctl.any_changed, (size_t)tctl.max_pass + 2);
@@ -474,6 +477,8 @@ struct Ctx : CtxBase {
         tctl.spin_limit = (long long)clk * 1000LL * 2;                 // about two seconds
         wait_default = tctl.spin_limit;
         use_tiles = true;
+        tiles_df = (owner->flags & MOIST_FLAG_TRACER_DATAFLOW) != 0;
+        CK(cudaFuncSetAttribute(k_tracer_tiles<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem));
         return MOIST_OK;
     }
 
@@ -772,7 +777,15 @@ struct Ctx : CtxBase {
             T* sp = strips;
             int* e = err;
             void* args[] = {&dp, &tr, &c, &sp, &e};
-            CK(cudaLaunchCooperativeKernel((void*)k_tracer_tiles<T>, dim3(tctl.ntiles), dim3(96), args, tile_smem, st));
+            if (tiles_df) {
+                CK(cudaMemsetAsync(tctl.ver, 0, (size_t)3 * tctl.ntiles * sizeof(int), st));
+                CK(cudaMemsetAsync(tctl.passes, 0, sizeof(int), st));
+                CK(cudaLaunchCooperativeKernel((void*)k_tracer_tiles<T, true>, dim3(tctl.ntiles), dim3(96), args,
+                                               tile_smem, st));
+            } else {
+                CK(cudaLaunchCooperativeKernel((void*)k_tracer_tiles<T, false>, dim3(tctl.ntiles), dim3(96), args,
+                                               tile_smem, st));
+            }
             k_pass_count<<<1, 1, 0, st>>>(tctl.passes, pass_hist);
             CKL();
         } else {
@@ -1145,21 +1158,22 @@ struct Ctx : CtxBase {
         }
         struct Cand {
             int wc;
-            int tracer;  // 0 tiles, 1 stream
+            int tracer;  // 0 tiles, 1 stream, 2 tiles without grid barriers
         };
         std::vector<Cand> cands;
-        for (int tr = 0; tr < 2; tr++) {
-            if (tr == 0 && !strips) continue;  // the tiles need all of them resident (init_tiles)
+        for (int tr = 0; tr < 3; tr++) {
+            if (tr != 1 && !strips) continue;  // the tiles need all of them resident (init_tiles)
             if (tr == 1 && !s_old[0]) continue;
             for (int w : {1, 2, 4, 8})
                 if (w <= nx && strip_smem_bytes<T, TT>(nz, w) <= (size_t)optin) cands.push_back({w, tr});
         }
-        const int wc0 = strip_wc, str0 = use_stream, til0 = use_tiles;
+        const int wc0 = strip_wc, str0 = use_stream, til0 = use_tiles, df0 = tiles_df;
+        auto tracer_name = [](int tr) { return tr == 1 ? "stream" : tr == 2 ? "tiles dataflow" : "tiles"; };
         cudaEvent_t e0, e1;
         CK(cudaEventCreate(&e0));
         CK(cudaEventCreate(&e1));
         float best = 1e30f;
-        Cand bc{wc0, str0 ? 1 : 0};
+        Cand bc{wc0, str0 ? 1 : (df0 ? 2 : 0)};
         char buf[128];
         if (!hash_buf) AL(hash_buf, 64);
         std::vector<unsigned long long> hashes(cands.size());
@@ -1167,8 +1181,9 @@ struct Ctx : CtxBase {
             const Cand& c = cands[ci];
             strip_wc = c.wc;
             strip_smem = strip_smem_bytes<T, TT>(nz, c.wc);
-            use_tiles = c.tracer == 0;
+            use_tiles = c.tracer != 1;
             use_stream = c.tracer == 1;
+            tiles_df = c.tracer == 2;
             if (int rr = restore()) return rr;
             CK(reset_err());
             int r = launch_step();  // warm-up
@@ -1183,12 +1198,12 @@ struct Ctx : CtxBase {
             if (hashes[ci] != hashes[0])
                 return set_err(owner, MOIST_ERR_CUDA,
                                "autotune: strip %d / %s gives another State than the first candidate", c.wc,
-                               c.tracer ? "stream" : "tiles");
+                               tracer_name(c.tracer));
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, e0, e1));
             ms /= nsteps;
             snprintf(buf, sizeof buf, "%sstrip %d, %s: %.3f ms", report.empty() ? "" : "; ", c.wc,
-                     c.tracer ? "stream" : "tiles", ms);
+                     tracer_name(c.tracer), ms);
             report += buf;
             if (ms < best) {
                 best = ms;
@@ -1201,13 +1216,16 @@ struct Ctx : CtxBase {
             strip_wc = wc0;
             use_stream = str0;
             use_tiles = til0;
+            tiles_df = df0;
         } else {
             strip_wc = bc.wc;
-            use_tiles = bc.tracer == 0;
+            use_tiles = bc.tracer != 1;
             use_stream = bc.tracer == 1;
+            tiles_df = bc.tracer == 2;
         }
         strip_smem = strip_smem_bytes<T, TT>(nz, strip_wc);
-        snprintf(buf, sizeof buf, " -> strip %d, %s (%.3f ms per step)", strip_wc, use_stream ? "stream" : "tiles", best);
+        snprintf(buf, sizeof buf, " -> strip %d, %s (%.3f ms per step)", strip_wc,
+                 tracer_name(use_stream ? 1 : (tiles_df ? 2 : 0)), best);
         report += buf;
         if (int rr = restore()) return rr;
         CK(reset_err());

@@ -30,6 +30,7 @@ constexpr int TT_S = TT_W + 2; // staged extent with a two-cell halo
 
 struct TileCtl {
     int tiles_x, tiles_z, ntiles, max_pass;
+    int* ver;           // dataflow sweep: [3][ntiles] words (version << 1 | final) of each tile's strips
     unsigned* bar;      // [0] arrival counter, [1] generation
     int* changed;       // [2][3][ntiles][2] per pass parity: rows whose right-strip entries changed, columns whose top-strip entries changed (bit masks)
     int* any_changed;   // [max_pass + 1]
@@ -295,8 +296,29 @@ template <class T>
 __device__ __forceinline__ T* strip_ptr(T* strips, int parity, int t, int tile, int ntiles) {
     return strips + ((((size_t)parity * 3 + t) * ntiles + tile) * 4) * TT_W;
 }
-
+// the dataflow sweep keeps the last TT_RING versions of each tile's strips:
+// [tracer][tile][version % TT_RING][4][32]
+constexpr int TT_RING = 4;
 template <class T>
+__device__ __forceinline__ T* strip_ver_ptr(T* strips, int t, int tile, int ver, int ntiles) {
+    return strips + ((((size_t)t * ntiles + tile) * TT_RING + (ver % TT_RING)) * 4) * TT_W;
+}
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// DF = false: passes separated by grid barriers (all tiles advance pass by pass). DF = true: no
+// grid barrier; every tile publishes numbered versions of its strips and recomputes whenever its
+// left or lower neighbour publishes a new version, so a chain of changes crosses the tiles at the
+// pace of its own work. A tile is final once it has computed from its neighbours' final strips
+// (the left column and the bottom row of tiles have fixed inputs), which every tile reaches
+// because the dependencies run only left-to-right and bottom-to-top.
+template <class T, bool DF>
 __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<T> a, TileCtl ctl, T* strips,
                                                      const int* err) {
     extern __shared__ unsigned char smem_raw[];
@@ -381,15 +403,15 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
     }
 
     // ---- pass-0 strips: the stage-start values (the speculation)
-    {
+    if constexpr (!DF) {
         T* out = strip_ptr(strips, 0, t, tile, ctl.ntiles);
         const int r = lane;
         __stcg(out + 0 * TT_W + r, sm.s[t][r][TT_W - 2]);
         __stcg(out + 1 * TT_W + r, sm.s[t][r][TT_W - 1]);
         __stcg(out + 2 * TT_W + r, sm.s[t][TT_W - 2][r]);
         __stcg(out + 3 * TT_W + r, sm.s[t][TT_W - 1][r]);
+        if (!grid_barrier(ctl, nblocks)) return;
     }
-    if (!grid_barrier(ctl, nblocks)) return;
 
     // lane-constant row data
     const int r = lane;
@@ -440,22 +462,123 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
     const T* dph = a.dphys[t];
     T* qn = a.q_new[t];
 
+    const int left = tx > 0 ? tile - 1 : -1;
+    const int below = tz > 0 ? tile - ctl.tiles_x : -1;
+    // Dataflow state (DF): the left-strip values (this lane's row) and the bottom strip (sm.bot)
+    // of the last computation, the neighbours' versions they came from and the words read with
+    // them (version << 1 | final), this tile's published version and the values it published.
+    T in_p1 = T(0), in_p2 = T(0);
+    int used_lv = 0, used_bv = 0, lw_cur = 0, bw_cur = 0, my_ver = 0;
+    T pub[4] = {T(0), T(0), T(0), T(0)};
+    // a strip entry the tile does not own (partial tile) keeps its stage-start value
+    auto pass0 = [&](int q) {
+        return q == 0 ? sm.s[t][r][TT_W - 2]
+                      : q == 1 ? sm.s[t][r][TT_W - 1] : q == 2 ? sm.s[t][TT_W - 2][r] : sm.s[t][TT_W - 1][r];
+    };
+    if constexpr (DF) {
+        // the inputs of the first computation are the neighbours' stage-start strips, which every
+        // tile forms from the stage-start values exactly as the neighbour stages them: no wait
+        auto s0 = [&](int kk, int ii) {
+            return (kk >= 0 && kk < nz) ? a.q_old[t][MOIST_IDX(kk, ii)] / a.rho[MOIST_IDX(kk, ii)] : T(0);
+        };
+        in_p1 = row_ok ? s0(k, wrapx(x0 - 1, nx)) : T(0);
+        in_p2 = row_ok ? s0(k, wrapx(x0 - 2, nx)) : T(0);
+        const bool cin = below >= 0 && x0 + r < nx + 2;
+        sm.bot[t][0][r] = cin ? s0(z0 - 2, wrapx(x0 + r, nx)) : T(0);  // row z0-2
+        sm.bot[t][1][r] = cin ? s0(z0 - 1, wrapx(x0 + r, nx)) : T(0);  // row z0-1
+        for (int q = 0; q < 4; q++) pub[q] = pass0(q);
+        __syncwarp();
+    }
+    int* const my_word = ctl.ver + (size_t)t * ctl.ntiles + tile;
     int pass = 1;
-    for (; pass <= ctl.max_pass; pass++) {
+    for (;; pass++) {
+        if constexpr (!DF) {
+            if (pass > ctl.max_pass) break;
+        }
         const int cur = pass & 1, prv = cur ^ 1;
         const int* chg_prev = ctl.changed + ((size_t)prv * 3 * ctl.ntiles + (size_t)t * ctl.ntiles) * 2;
         int* chg_cur = ctl.changed + ((size_t)cur * 3 * ctl.ntiles + (size_t)t * ctl.ntiles) * 2;
-        const int left = tx > 0 ? tile - 1 : -1;
-        const int below = tz > 0 ? tile - ctl.tiles_x : -1;
-        // neighbours' strips and masks are written by other SMs: read them through L2 (__ldcg)
-        const unsigned lmask = left >= 0 ? (unsigned)__ldcg(chg_prev + 2 * left) : 0u;
-        const unsigned bmask = below >= 0 ? (unsigned)__ldcg(chg_prev + 2 * below + 1) : 0u;
+        unsigned lmask = 0u, bmask = 0u;
+        bool df_timeout = false;
+        if constexpr (DF) {
+            if (pass > 1) {
+                // wait until a neighbour has published a version this tile has not used (bounded)
+                const int* lwp = ctl.ver + (size_t)t * ctl.ntiles + left;
+                const int* bwp = ctl.ver + (size_t)t * ctl.ntiles + below;
+                int lw = lw_cur, bw = bw_cur;
+                const long long t0 = clock64();
+                while (true) {
+                    lw = left >= 0 ? ld_acquire(lwp) : 0;
+                    bw = below >= 0 ? ld_acquire(bwp) : 0;
+                    const bool news = (left >= 0 && (lw >> 1) > used_lv) || (below >= 0 && (bw >> 1) > used_bv);
+                    if (__shfl_sync(0xffffffffu, (int)news, 0)) break;
+                    if (__shfl_sync(0xffffffffu, (int)(clock64() - t0 > ctl.spin_limit), 0)) {
+                        df_timeout = true;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+                if (df_timeout) {
+                    if (lane == 0) atomicExch(ctl.timeout, 1);
+                    break;
+                }
+                lw = __shfl_sync(0xffffffffu, lw, 0);
+                bw = __shfl_sync(0xffffffffu, bw, 0);
+                // the newest strips, read from the ring slot of their version; a slot the neighbour
+                // may have begun to overwrite meanwhile (it got TT_RING - 1 versions ahead) is read again
+                T np1 = in_p1, np2 = in_p2, nb0 = sm.bot[t][0][r], nb1 = sm.bot[t][1][r];
+                if (left >= 0 && (lw >> 1) > used_lv) {
+                    for (int tries = 0;; tries++) {
+                        const int v = lw >> 1;
+                        const T* ls = strip_ver_ptr(strips, t, left, v, ctl.ntiles);
+                        np2 = __ldcg(ls + 0 * TT_W + r);
+                        np1 = __ldcg(ls + 1 * TT_W + r);
+                        const int again = __shfl_sync(0xffffffffu, ld_acquire(lwp), 0);
+                        if ((again >> 1) <= v + TT_RING - 2 || tries > 1000) break;
+                        lw = again;
+                    }
+                    used_lv = lw >> 1;
+                    lw_cur = lw;
+                }
+                if (below >= 0 && (bw >> 1) > used_bv) {
+                    for (int tries = 0;; tries++) {
+                        const int v = bw >> 1;
+                        const T* bs = strip_ver_ptr(strips, t, below, v, ctl.ntiles);
+                        nb0 = __ldcg(bs + 2 * TT_W + r);
+                        nb1 = __ldcg(bs + 3 * TT_W + r);
+                        const int again = __shfl_sync(0xffffffffu, ld_acquire(bwp), 0);
+                        if ((again >> 1) <= v + TT_RING - 2 || tries > 1000) break;
+                        bw = again;
+                    }
+                    used_bv = bw >> 1;
+                    bw_cur = bw;
+                }
+                auto differs = [](T x, T y) { return !(x == y || (x != x && y != y)); };
+                lmask = __ballot_sync(0xffffffffu, differs(np1, in_p1) || differs(np2, in_p2));
+                bmask = __ballot_sync(0xffffffffu, differs(nb0, sm.bot[t][0][r]) || differs(nb1, sm.bot[t][1][r]));
+                in_p1 = np1;
+                in_p2 = np2;
+                sm.bot[t][0][r] = nb0;
+                sm.bot[t][1][r] = nb1;
+                __syncwarp();
+            }
+        } else {
+            // neighbours' strips and masks are written by other SMs: read them through L2 (__ldcg)
+            lmask = left >= 0 ? (unsigned)__ldcg(chg_prev + 2 * left) : 0u;
+            bmask = below >= 0 ? (unsigned)__ldcg(chg_prev + 2 * below + 1) : 0u;
+        }
         const bool compute = !halt && (pass == 1 || lmask != 0u || bmask != 0u);
         // Rows below the lowest changed row of the left strip have unchanged inputs when the
         // lower strip did not change: a repair pass replays their last values (Float32)
         const int rmin = (pass == 1 || bmask != 0u || !kStageQ<T>) ? 0 : __ffs((int)lmask) - 1;
-        if (ctl.pass_ts && blockIdx.x == 0 && threadIdx.x == 0) ctl.pass_ts[pass] = globaltimer_ns();
-        if (ctl.pass_work && compute && lane == 0) atomicAdd(ctl.pass_work + pass, 1);
+        if (ctl.pass_ts && pass <= ctl.max_pass) {
+            if constexpr (DF) {
+                if (lane == 0) atomicMax(ctl.pass_ts + pass, globaltimer_ns());
+            } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+                ctl.pass_ts[pass] = globaltimer_ns();
+            }
+        }
+        if (ctl.pass_work && compute && lane == 0 && pass <= ctl.max_pass) atomicAdd(ctl.pass_work + pass, 1);
         const T* sp_prev = strip_ptr(strips, prv, t, tile, ctl.ntiles);
         T* sp_cur = strip_ptr(strips, cur, t, tile, ctl.ntiles);
         bool right_changed = false, top_changed = false;
@@ -463,17 +586,22 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
             // left inputs: the left tile's right strip, or at the periodic seam the halo columns'
             // stage-start values; bottom inputs: the lower tile's top strip (none at k = 0)
             T prev1, prev2;
-            if (left >= 0) {
-                const T* ls = strip_ptr(strips, prv, t, left, ctl.ntiles);
-                prev2 = __ldcg(ls + 0 * TT_W + r);
-                prev1 = __ldcg(ls + 1 * TT_W + r);
+            if constexpr (DF) {
+                prev1 = in_p1;
+                prev2 = in_p2;
             } else {
-                prev1 = row_ok ? a.q_old[t][MOIST_IDX(k, nx - 1)] / a.rho[MOIST_IDX(k, nx - 1)] : T(0);
-                prev2 = row_ok ? a.q_old[t][MOIST_IDX(k, nx - 2)] / a.rho[MOIST_IDX(k, nx - 2)] : T(0);
+                if (left >= 0) {
+                    const T* ls = strip_ptr(strips, prv, t, left, ctl.ntiles);
+                    prev2 = __ldcg(ls + 0 * TT_W + r);
+                    prev1 = __ldcg(ls + 1 * TT_W + r);
+                } else {
+                    prev1 = row_ok ? a.q_old[t][MOIST_IDX(k, nx - 1)] / a.rho[MOIST_IDX(k, nx - 1)] : T(0);
+                    prev2 = row_ok ? a.q_old[t][MOIST_IDX(k, nx - 2)] / a.rho[MOIST_IDX(k, nx - 2)] : T(0);
+                }
+                const T* bs = below >= 0 ? strip_ptr(strips, prv, t, below, ctl.ntiles) : nullptr;
+                sm.bot[t][0][r] = bs ? __ldcg(bs + 2 * TT_W + r) : T(0);  // row z0-2
+                sm.bot[t][1][r] = bs ? __ldcg(bs + 3 * TT_W + r) : T(0);  // row z0-1
             }
-            const T* bs = below >= 0 ? strip_ptr(strips, prv, t, below, ctl.ntiles) : nullptr;
-            sm.bot[t][0][r] = bs ? __ldcg(bs + 2 * TT_W + r) : T(0);  // row z0-2
-            sm.bot[t][1][r] = bs ? __ldcg(bs + 3 * TT_W + r) : T(0);  // row z0-1
             __syncwarp();
             T sn_last = T(0), km1_used = T(0);
             const int nsteps = width + TT_W - 1;
@@ -642,15 +770,43 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
             }
             // publish this pass's strips; a strip entry the tile does not own (partial tile)
             // keeps the speculative value so it never registers a change
+            if constexpr (!DF) {
+                for (int q = 0; q < 4; q++) {
+                    const bool owned =
+                        (q < 2) ? (row_ok && width == TT_W) : ((z0 + 30 + (q - 2)) < nz && r < width);
+                    const T old = __ldcg(sp_prev + q * TT_W + r);
+                    const T v = owned ? sm.strip_out[t][q][r] : old;
+                    __stcg(sp_cur + q * TT_W + r, v);
+                    if (!(v == old || (v != v && old != old))) (q < 2 ? right_changed : top_changed) = true;
+                }
+            }
+        } else if constexpr (!DF) {
+            for (int q = 0; q < 4; q++) __stcg(sp_cur + q * TT_W + r, __ldcg(sp_prev + q * TT_W + r));
+        }
+        if constexpr (DF) {
+            // a new version when the strips changed, or when the tile became final: it computed
+            // from (or is unchanged by) its neighbours' final strips
+            T v[4];
+            bool chg = false;
             for (int q = 0; q < 4; q++) {
                 const bool owned = (q < 2) ? (row_ok && width == TT_W) : ((z0 + 30 + (q - 2)) < nz && r < width);
-                const T old = __ldcg(sp_prev + q * TT_W + r);
-                const T v = owned ? sm.strip_out[t][q][r] : old;
-                __stcg(sp_cur + q * TT_W + r, v);
-                if (!(v == old || (v != v && old != old))) (q < 2 ? right_changed : top_changed) = true;
+                v[q] = (compute && owned) ? sm.strip_out[t][q][r] : pub[q];
+                chg |= !(v[q] == pub[q] || (v[q] != v[q] && pub[q] != pub[q]));
             }
-        } else {
-            for (int q = 0; q < 4; q++) __stcg(sp_cur + q * TT_W + r, __ldcg(sp_prev + q * TT_W + r));
+            const bool fin = (left < 0 || (lw_cur & 1)) && (below < 0 || (bw_cur & 1));
+            if (__any_sync(0xffffffffu, chg) || fin) {
+                T* out = strip_ver_ptr(strips, t, tile, my_ver + 1, ctl.ntiles);
+                for (int q = 0; q < 4; q++) {
+                    __stcg(out + q * TT_W + r, v[q]);
+                    pub[q] = v[q];
+                }
+                __threadfence();
+                __syncwarp();
+                my_ver++;
+                if (lane == 0) st_release(my_word, (my_ver << 1) | (fin ? 1 : 0));
+            }
+            if (fin || halt) break;
+            continue;
         }
         // lane r: row r of the right strip, column r of the top strip
         const unsigned rmask = __ballot_sync(0xffffffffu, right_changed);
@@ -663,7 +819,12 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
         if (!grid_barrier(ctl, nblocks)) return;
         if (__ldcg(ctl.any_changed + pass) == 0) break;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if constexpr (DF) {  // the deepest tile's count of computations, and the moment the last tile leaves
+        if (lane == 0) {
+            atomicMax(ctl.passes, pass);
+            if (ctl.pass_ts) atomicMax(ctl.pass_ts + ctl.max_pass + 2, globaltimer_ns());
+        }
+    } else if (blockIdx.x == 0 && threadIdx.x == 0) {
         *ctl.passes = pass;
         if (ctl.pass_ts) ctl.pass_ts[ctl.max_pass + 2] = globaltimer_ns();  // block 0 leaves the sweep
     }

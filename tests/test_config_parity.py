@@ -84,9 +84,9 @@ def test_sounding_full_size_autotuned(sounding_oracle):
     compare(a, b, p)
 
 
-def test_sounding_full_size_default_and_stream(sounding_oracle):
+def test_sounding_full_size_default_stream_and_dataflow(sounding_oracle):
     p, s, b = sounding_oracle
-    for flags in (0, abi.MOIST_FLAG_TRACER_STREAM):
+    for flags in (0, abi.MOIST_FLAG_TRACER_STREAM, abi.MOIST_FLAG_TRACER_DATAFLOW):
         a = s.copy()
         model.rk3_step(a, p, 10, flags=flags)
         compare(a, b, p)

@@ -127,20 +127,23 @@ def test_invalid_params_rejected():
 
 @pytest.mark.parametrize("T,tri_native", MODES, ids=MODE_IDS)
 def test_tiled_tracer_sweep_matches_wavefront_and_oracle(T, tri_native):
-    """Multi-tile domain (8 x 3 tiles, a partial top tile): the tiled sweep, the exact wavefront
-    and the oracle agree bit for bit over several steps with clouds, rain and both wind signs."""
+    """Multi-tile domain (8 x 3 tiles, a partial top tile): the tiled sweep (with grid-wide passes
+    and without, as dataflow), the streaming sweep, the exact wavefront and the oracle agree bit
+    for bit over several steps with clouds, rain and both wind signs."""
     from moist2d_b200.init import sounding_bubbles
     from states import perturb
     p, s = sounding_bubbles(T, nx=256, nz=72, nbub=2)
     perturb(s, p, 21, wind=6.0, w=2.0)
-    a, b, c, d = s.copy(), s.copy(), s.copy(), s.copy()
+    a, b, c, d, e = s.copy(), s.copy(), s.copy(), s.copy(), s.copy()
     model.rk3_step(a, p, 3, flags=_flags(tri_native))
     model.rk3_step(b, p, 3, flags=_flags(tri_native) | abi.MOIST_FLAG_TRACER_WAVEFRONT)
     model.rk3_step(d, p, 3, flags=_flags(tri_native) | abi.MOIST_FLAG_TRACER_STREAM)
+    model.rk3_step(e, p, 3, flags=_flags(tri_native) | abi.MOIST_FLAG_TRACER_DATAFLOW)
     bind.rk3_step(c, p, 3, tri64=_tri64(T, tri_native))
     compare(a, b, p)
     compare(a, c, p)
     compare(d, c, p)
+    compare(e, c, p)
 
 
 @pytest.mark.parametrize("T,tri_native", MODES, ids=MODE_IDS)
@@ -199,3 +202,17 @@ def test_tiled_sweep_pass_trace():
         assert tiles[w * maxrec] == 3 * ntiles
         assert all(tiles[w * maxrec + q] <= 3 * ntiles for q in range(n))
     assert hist == list(counts)
+
+
+@pytest.mark.parametrize("T", [np.float32, np.float64])
+@pytest.mark.parametrize("nx,nz", [(70, 40), (33, 97), (200, 33)])
+def test_dataflow_tiled_sweep_partial_tiles(T, nx, nz):
+    """The dataflow sweep on domains whose last tile column and row are partial, against the
+    oracle."""
+    from states import perturb
+    p, s = small_case(T, nx, nz)
+    perturb(s, p, 8, wind=5.0, w=1.5)
+    a, c = s.copy(), s.copy()
+    model.rk3_step(a, p, 2, flags=abi.MOIST_FLAG_TRACER_DATAFLOW)
+    bind.rk3_step(c, p, 2, tri64=True)
+    compare(a, c, p)

@@ -1,8 +1,9 @@
 """Bounded device-side waits: a wait that runs out ends the step with MOIST_ERR_TIMEOUT instead of
 hanging, and the context stays usable.
 
-The tiled tracer sweep's blocks wait for each other between repair passes (the reference's
-in-place sweep, moist.jl:1469-1518, has no such wait; its threads never synchronise). Here the
+The tiled tracer sweep's blocks wait for each other between repair passes, or, in its dataflow
+form, for their left and lower neighbours' new strips (the reference's in-place sweep,
+moist.jl:1469-1518, has no such wait; its threads never synchronise). Here the
 wait limit is set to one SM clock cycle, so that waits give up almost at once; nothing faults
 and nothing spins without bound. The same context, with the default limit restored and the
 State uploaded again, then steps bit for bit like the oracle."""
@@ -21,9 +22,10 @@ from states import compare
 pytestmark = pytest.mark.gpu
 
 
-def test_wait_that_runs_out_returns_timeout_and_context_recovers():
+@pytest.mark.parametrize("flags", [0, abi.MOIST_FLAG_TRACER_DATAFLOW], ids=["passes", "dataflow"])
+def test_wait_that_runs_out_returns_timeout_and_context_recovers(flags):
     p, s = sounding_bubbles(np.float32, nx=512, nz=96, nbub=2)
-    with model.Model(p) as m:
+    with model.Model(p, flags=flags) as m:
         assert lib().moist_set_wait_limit(m.ctx, 1) == abi.MOIST_OK
         m.upload(s)
         rc = lib().moist_rk3_step(m.ctx, 2)
@@ -39,7 +41,7 @@ def test_wait_that_runs_out_returns_timeout_and_context_recovers():
     compare(a, b, p)
     # a fresh context is unaffected
     c = s.copy()
-    model.rk3_step(c, p, 2)
+    model.rk3_step(c, p, 2, flags=flags)
     compare(c, b, p)
 
 
