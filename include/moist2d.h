@@ -323,14 +323,27 @@ int moist_adjoint_run(moist_ctx* ctx, int nsteps, int ckpt_every, const moist_ad
                       moist_adjoint_grad* out);
 
 /* moist_adjoint_run for every member of a batch (no counterpart in the reference): seeds[m] and
- * out[m] belong to member m (seeds may be NULL: J = 0). The members' adjoint buffers are
- * allocated one member at a time, then the members run concurrently from up to nthreads host
- * threads (nthreads <= 0: one per member), each on its member context's stream, so that their
- * kernels share the GPU. Each member is left at its final State; the next moist_batch_step
- * continues from there. The first failing member's status is returned, its index in
- * moist_batch_last_error. */
+ * out[m] belong to member m (seeds may be NULL: J = 0). nthreads <= 0: the members' kernels run
+ * packed, one launch per kernel of the forward step, of the recomputed (taped) step and of the
+ * reverse step for all members (the forward through the batch's step graphs); every member gets
+ * the gradient of its own moist_adjoint_run (atomic sums may round in another order).
+ * forward_ms and reverse_ms are the batch's. nthreads > 0: every member's own
+ * moist_adjoint_run from up to nthreads host threads, each on its member context's stream.
+ * Each member is left at its final State; the next moist_batch_step continues from there. The
+ * first failing member's status is returned, its index in moist_batch_last_error. */
 int moist_batch_adjoint_run(moist_batch* b, int nsteps, int ckpt_every, const moist_adjoint_seed* seeds,
                             moist_adjoint_grad* out, int nthreads);
+
+/* Tape mode of moist_adjoint_run (no counterpart in the reference). The reverse sweep
+ * recomputes each segment of ckpt_every steps from its checkpoint. mode 1: a tape of every step
+ * of the segment, the segment recomputed once; mode 0: the segment's States and one tape, every
+ * step recomputed from its State (one more forward step per step, ckpt_every - 1 States instead
+ * of ckpt_every tapes of 3*ns + 40 fields); mode -1 (the default): mode 1 when the tapes fit in
+ * half the free device memory. The gradients do not depend on the mode. */
+int moist_set_adjoint_tapes(moist_ctx* ctx, int mode);
+/* The same for moist_batch_adjoint_run: every member runs in one mode (-1: decided from the
+ * members' tapes together). */
+int moist_batch_set_adjoint_tapes(moist_batch* b, int mode);
 
 /* output_history's primitive variables (moist.jl:1795-1835) computed on the device from the
  * context State, so that a run_sim-style driver reads only what it writes to its history file:

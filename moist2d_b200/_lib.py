@@ -25,7 +25,7 @@ EXPORTS = ("moist_abi_version", "moist_status_string", "moist_ctx_create", "mois
            "moist_history_close", "moist_restart_read", "moist_surface_fluxes", "moist_gray_radiation",
            "moist_set_wait_limit", "moist_uniform", "moist_init_state", "moist_init_warm_bubble",
            "moist_init_sounding", "moist_sounding_bubble_row", "moist_ensemble_member_draw",
-           "moist_tracer_pass_trace")
+           "moist_tracer_pass_trace", "moist_set_adjoint_tapes", "moist_batch_set_adjoint_tapes")
 
 
 def lib():
@@ -87,6 +87,8 @@ def lib():
         L.moist_history_diagnostics.argtypes = [Ctx, C.POINTER(V), C.POINTER(D)]
         L.moist_batch_autotune.argtypes = [B, I, C.c_char_p, C.c_size_t]
         L.moist_batch_adjoint_run.argtypes = [B, I, I, C.POINTER(moist_adjoint_seed), C.POINTER(moist_adjoint_grad), I]
+        L.moist_set_adjoint_tapes.argtypes = [Ctx, I]
+        L.moist_batch_set_adjoint_tapes.argtypes = [B, I]
         H = C.c_void_p
         L.moist_io_last_error.restype = C.c_char_p
         L.moist_history_create.argtypes = [C.c_char_p, P, I, C.POINTER(H)]

@@ -363,8 +363,8 @@ struct AdjSub {
 };
 
 #define ADJ_CELL(k, i)                                                  \
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;                \
-    const int k = blockIdx.y;                                           \
+    const int i = bid_x * blockDim.x + threadIdx.x;                     \
+    const int k = bid_y;                                                \
     const int nx = p.nx, nz = p.nz, P = p.P;                            \
     if (i >= nx || k >= nz) return;                                     \
     const size_t c = MOIST_IDX(k, i);                                   \
@@ -376,7 +376,8 @@ __device__ __forceinline__ void aadd(double* a, double v) { atomicAdd(a, v); }
 
 // w-p coefficients a, b, c of implicit_correction! (moist.jl:982-1008) in double, per cell
 template <class T>
-__global__ void k_adj_tri_coef(DevParams<double> p, AdjStage<T> a) {
+__device__ __forceinline__ void b_adj_tri_coef(const DevParams<double>& p, const AdjStage<T>& a, int bid_x, int bid_y,
+                                               int bid_z) {
     ADJ_CELL(k, i);
     const int ke = nz - 1, n = nz - 1;
     if (k >= n) return;
@@ -392,12 +393,18 @@ __global__ void k_adj_tri_coef(DevParams<double> p, AdjStage<T> a) {
     a.Ta[c] = k > 0 ? -C * (r_k * thh(k - 1) / (dzc * dz[k]) - p.GRAV / (dz[k] + dz[k + 1])) : 0.0;
     a.Tc[c] = k < ke - 1 ? -C * (r_kp * thh(k + 1) / (dzc * dz[k + 1]) + p.GRAV / (dz[k] + dz[k + 1])) : 0.0;
 }
+template <class T>
+__global__ void k_adj_tri_coef(const __grid_constant__ DevParams<double> p, const __grid_constant__ AdjStage<T> a) {
+    b_adj_tri_coef(p, a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // elimination of the transposed system A^T (sub-diagonal c_{j-1}, diagonal b_j + 1,
 // super-diagonal a_{j+1}), once per stage and column: modified super-diagonal and 1 / pivot
-__global__ void k_adj_tri_fact(int nx, int nz, int P, const double* __restrict__ Ta, const double* __restrict__ Tb,
-                               const double* __restrict__ Tc, double* __restrict__ Tcp, double* __restrict__ Trd) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void b_adj_tri_fact(int nx, int nz, int P, const double* __restrict__ Ta,
+                                               const double* __restrict__ Tb, const double* __restrict__ Tc,
+                                               double* __restrict__ Tcp, double* __restrict__ Trd, int bid_x, int bid_y,
+                                               int bid_z) {
+    const int i = bid_x * blockDim.x + threadIdx.x;
     if (i >= nx) return;
     const int n = nz - 1;
     double cp = 0.0;
@@ -410,12 +417,17 @@ __global__ void k_adj_tri_fact(int nx, int nz, int P, const double* __restrict__
         Trd[cj] = rd;
     }
 }
+__global__ void k_adj_tri_fact(int nx, int nz, int P, const double* __restrict__ Ta, const double* __restrict__ Tb,
+                               const double* __restrict__ Tc, double* __restrict__ Tcp, double* __restrict__ Trd) {
+    b_adj_tri_fact(nx, nz, P, Ta, Tb, Tc, Tcp, Trd, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // adjoint of the state update (moist.jl:1522-1539): the stage output's lambda goes to the
 // stage input (already in Lst) and to the last perturbations; the tracers' lambda moves to
 // the sweep results
 template <class T>
-__global__ void k_adj_update(DevParams<double> p, AdjStage<T> a, DP<4> LP) {
+__device__ __forceinline__ void b_adj_update(const DevParams<double>& p, const AdjStage<T>& a, const DP<4>& LP,
+                                             int bid_x, int bid_y, int bid_z) {
     ADJ_CELL(k, i);
     LP.f[0][c] = a.Lst[0][c];
     LP.f[1][c] = a.Lst[1][c];
@@ -425,6 +437,11 @@ __global__ void k_adj_update(DevParams<double> p, AdjStage<T> a, DP<4> LP) {
         a.Lqout[t][c] = a.Lst[4 + t][c];
         a.Lst[4 + t][c] = 0.0;
     }
+}
+template <class T>
+__global__ void k_adj_update(const __grid_constant__ DevParams<double> p, const __grid_constant__ AdjStage<T> a,
+                             const __grid_constant__ DP<4> LP) {
+    b_adj_update(p, a, LP, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ----------------------------------------------------------------------------- tracer sweep
@@ -473,24 +490,32 @@ __device__ __forceinline__ void tracer_slots(const DevParams<double>& p, const A
 
 // partial derivatives of every tracer cell with respect to its 24 reads: J[t][slot][cell]
 template <class T>
-__global__ void __launch_bounds__(ADJ_THREADS) k_adj_tr_jac(DevParams<double> p, AdjStage<T> a, double* J) {
+__device__ __forceinline__ void b_adj_tr_jac(const DevParams<double>& p, const AdjStage<T>& a, double* J, int bid_x,
+                                             int bid_y, int bid_z) {
     ADJ_CELL(k, i);
-    const int t = blockIdx.z;
+    const int t = bid_z;
     double v[TR_SLOTS];
     tracer_slots(p, a, t, k, i, v);
     const size_t fsz = (size_t)nz * P;
     double* Jt = J + (size_t)t * TR_SLOTS * fsz;
-    local_jacobian<ADJ_DUAL>(v, [&](const auto& get) { return gen_tracer<Dual<ADJ_DUAL>>(p, k, 0.0, 0.0, a.dt_stage, get); },
-                             [&](int s, double d) { Jt[(size_t)s * fsz + c] = d; });
+    local_jacobian<ADJ_DUAL>(
+        v, [&](const auto& get) { return gen_tracer<Dual<ADJ_DUAL>>(p, k, 0.0, 0.0, a.dt_stage, get); },
+        [&](int s, double d) { Jt[(size_t)s * fsz + c] = d; });
+}
+template <class T>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_tr_jac(const __grid_constant__ DevParams<double> p,
+                                  const __grid_constant__ AdjStage<T> a, double* J) {
+    b_adj_tr_jac(p, a, J, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // reverse sweep: mu(k,i) = lambda_new(k,i) + sum over the later cells that read the new value
 // of (k, i): (k, i+1) [slot L1], (k, i+2) [L2], (k+1, i) [B1], (k+2, i) [B2]. One block per
 // tracer, thread k owns row k; row k handles column nx-1-(d-(nz-1-k)) at step d, after the rows
 // above it, whose results come through a 3-step ring in shared memory.
-__global__ void k_adj_tr_rev(int nx, int nz, int P, const double* __restrict__ J, DP<3> lam_new, DP<3> mu) {
+__device__ __forceinline__ void b_adj_tr_rev(int nx, int nz, int P, const double* __restrict__ J, const DP<3>& lam_new,
+                                             const DP<3>& mu, int bid_x, int bid_y, int bid_z) {
     extern __shared__ double ring[];  // [3][nz]
-    const int t = blockIdx.x;
+    const int t = bid_x;
     const int k = threadIdx.x;
     const size_t fsz = (size_t)nz * P;
     const double* Jt = J + (size_t)t * TR_SLOTS * fsz;
@@ -542,13 +567,18 @@ __global__ void k_adj_tr_rev(int nx, int nz, int P, const double* __restrict__ J
         __syncthreads();
     }
 }
+__global__ void k_adj_tr_rev(int nx, int nz, int P, const double* __restrict__ J, const __grid_constant__ DP<3> lam_new,
+                             const __grid_constant__ DP<3> mu) {
+    b_adj_tr_rev(nx, nz, P, J, lam_new, mu, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // the sweep's lambda contributions to everything read through "old" values, rho, the
 // momentum fluxes, s0 tracers and the phys tendencies
 template <class T>
-__global__ void k_adj_tr_scatter(DevParams<double> p, AdjStage<T> a, const double* J, DP<3> mu) {
+__device__ __forceinline__ void b_adj_tr_scatter(const DevParams<double>& p, const AdjStage<T>& a, const double* J,
+                                                 const DP<3>& mu, int bid_x, int bid_y, int bid_z) {
     ADJ_CELL(k, i);
-    const int t = blockIdx.z;
+    const int t = bid_z;
     const size_t fsz = (size_t)nz * P;
     const double* Jt = J + (size_t)t * TR_SLOTS * fsz;
     const double m = mu.f[t][c];
@@ -584,13 +614,23 @@ __global__ void k_adj_tr_scatter(DevParams<double> p, AdjStage<T> a, const doubl
     aadd(a.LS0[4 + t] + c, m);
     aadd(a.Lph[2 + t] + c, a.dt_stage * m);
 }
+template <class T>
+__global__ void k_adj_tr_scatter(const __grid_constant__ DevParams<double> p, const __grid_constant__ AdjStage<T> a,
+                                 const double* J, const __grid_constant__ DP<3> mu) {
+    b_adj_tr_scatter(p, a, J, mu, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // mom_flux_x = s.rho_u, mom_flux_z = s.rho_w before the averages (moist.jl:1347-1348)
 template <class T>
-__global__ void k_adj_mf(DevParams<double> p, AdjStage<T> a) {
+__device__ __forceinline__ void b_adj_mf(const DevParams<double>& p, const AdjStage<T>& a, int bid_x, int bid_y,
+                                         int bid_z) {
     ADJ_CELL(k, i);
     a.Lst[1][c] += a.Lmfx[c];
     a.Lst[2][c] += a.Lmfz[c];
+}
+template <class T>
+__global__ void k_adj_mf(const __grid_constant__ DevParams<double> p, const __grid_constant__ AdjStage<T> a) {
+    b_adj_mf(p, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ----------------------------------------------------------------------------- acoustic substep
@@ -599,7 +639,8 @@ __global__ void k_adj_mf(DevParams<double> p, AdjStage<T> a) {
 // rho_w_p: lambda of the w-p solution x = rho_w_p(k), k < nz-1; theta's share of the vertical
 // theta fluxes
 template <class T>
-__global__ void k_adj_sub_vert(DevParams<double> p, AdjStage<T> a, AdjSub<T> b) {
+__device__ __forceinline__ void b_adj_sub_vert(const DevParams<double>& p, const AdjStage<T>& a, const AdjSub<T>& b,
+                                               int bid_x, int bid_y, int bid_z) {
     ADJ_CELL(k, i);
     const int ke = nz - 1;
     if (k >= ke) return;
@@ -650,6 +691,11 @@ __global__ void k_adj_sub_vert(DevParams<double> p, AdjStage<T> a, AdjSub<T> b) 
     }
     a.Lx[c] = lx;
 }
+template <class T>
+__global__ void k_adj_sub_vert(const __grid_constant__ DevParams<double> p, const __grid_constant__ AdjStage<T> a,
+                               const __grid_constant__ AdjSub<T> b) {
+    b_adj_sub_vert(p, a, b, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // (2a) y = A^-T lambda_x with the stage's elimination (A = tri(a, b + 1, c), the w-p system of
 // moist.jl:1009-1018). A block of ADJ_SOLVE_THREADS threads owns `wc` adjacent columns: all of
@@ -664,14 +710,13 @@ __host__ __device__ inline int adj_solve_cols(int nz) {  // widest of 32, 16, 8,
 }
 __host__ __device__ inline size_t adj_solve_smem(int nz) { return (size_t)4 * nz * adj_solve_cols(nz) * sizeof(double); }
 
-__global__ void __launch_bounds__(ADJ_SOLVE_THREADS) k_adj_sub_solve(int nx, int nz, int P, const double* __restrict__ Tc,
-                                                                     const double* __restrict__ Tcp,
-                                                                     const double* __restrict__ Trd,
-                                                                     const double* __restrict__ Lx,
-                                                                     double* __restrict__ Ly) {
+__device__ __forceinline__ void b_adj_sub_solve(int nx, int nz, int P, const double* __restrict__ Tc,
+                                                const double* __restrict__ Tcp, const double* __restrict__ Trd,
+                                                const double* __restrict__ Lx, double* __restrict__ Ly, int bid_x,
+                                                int bid_y, int bid_z) {
     extern __shared__ double sm[];
     const int wc = adj_solve_cols(nz);
-    const int i0 = blockIdx.x * wc;
+    const int i0 = bid_x * wc;
     const int n = nz - 1;
     double* sg = sm;                 // [n][wc] right-hand side, then g', then y
     double* ssub = sm + nz * wc;     // c_{j-1}
@@ -708,12 +753,19 @@ __global__ void __launch_bounds__(ADJ_SOLVE_THREADS) k_adj_sub_solve(int nx, int
         if (i < nx) Ly[MOIST_IDX(j, i)] = sg[e];
     }
 }
+__global__ void __launch_bounds__(ADJ_SOLVE_THREADS) k_adj_sub_solve(int nx, int nz, int P,
+                                  const double* __restrict__ Tc, const double* __restrict__ Tcp,
+                                  const double* __restrict__ Trd, const double* __restrict__ Lx,
+                                  double* __restrict__ Ly) {
+    b_adj_sub_solve(nx, nz, P, Tc, Tcp, Trd, Lx, Ly, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // (2b) per cell k, from y of faces k and k-1: the coefficients' lambda -y x^T, the right-hand
 // side d = rho_w_p + drho_w - fact (a, b, c) rho_w_p (moist.jl:1009-1018) and
 // drho_w = dt_s (R_rho_w - rt2pres_h buoyancy + grav) (1397-1408)
 template <class T>
-__global__ void k_adj_sub_rhs(DevParams<double> p, DevParams<T> pt, AdjStage<T> a, AdjSub<T> b) {
+__device__ __forceinline__ void b_adj_sub_rhs(const DevParams<double>& p, const DevParams<T>& pt, const AdjStage<T>& a,
+                                              const AdjSub<T>& b, int bid_x, int bid_y, int bid_z) {
     ADJ_CELL(k, i);
     const int n = nz - 1;
     const double* z = p.z;
@@ -766,10 +818,16 @@ __global__ void k_adj_sub_rhs(DevParams<double> p, DevParams<T> pt, AdjStage<T> 
     a.Ltp_rho[c] = ltp_rho;
     b.LPo[2][c] = lpw;
 }
+template <class T>
+__global__ void k_adj_sub_rhs(const __grid_constant__ DevParams<double> p, const __grid_constant__ DevParams<T> pt,
+                              const __grid_constant__ AdjStage<T> a, const __grid_constant__ AdjSub<T> b) {
+    b_adj_sub_rhs(p, pt, a, b, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // (3) explicit rho_p / rho_theta_p updates and their off-centred values (moist.jl:1367-1396)
 template <class T>
-__global__ void k_adj_sub_expl(DevParams<double> p, AdjStage<T> a, AdjSub<T> b) {
+__device__ __forceinline__ void b_adj_sub_expl(const DevParams<double>& p, const AdjStage<T>& a, const AdjSub<T>& b,
+                                               int bid_x, int bid_y, int bid_z) {
     ADJ_CELL(k, i);
     const double f = a.fact_tp64, dts = a.dt_s;
     const double lrho = b.LPn[0][c], lrt = b.LPn[3][c];
@@ -784,11 +842,17 @@ __global__ void k_adj_sub_expl(DevParams<double> p, AdjStage<T> a, AdjSub<T> b) 
     a.LRrho[c] += dts * li_rho;
     a.LRt[c] += dts * li_rt;
 }
+template <class T>
+__global__ void k_adj_sub_expl(const __grid_constant__ DevParams<double> p, const __grid_constant__ AdjStage<T> a,
+                               const __grid_constant__ AdjSub<T> b) {
+    b_adj_sub_expl(p, a, b, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // (4) per face i+1/2: the horizontal forward step of rho_u_p (moist.jl:1355-1366), its
 // momentum-flux average and its use in the explicit updates
 template <class T>
-__global__ void k_adj_sub_horiz(DevParams<double> p, AdjStage<T> a, AdjSub<T> b) {
+__device__ __forceinline__ void b_adj_sub_horiz(const DevParams<double>& p, const AdjStage<T>& a, const AdjSub<T>& b,
+                                                int bid_x, int bid_y, int bid_z) {
     ADJ_CELL(k, i);
     const int ip = wrapx(i + 1, nx);
     const size_t cp = MOIST_IDX(k, ip);
@@ -815,10 +879,16 @@ __global__ void k_adj_sub_horiz(DevParams<double> p, AdjStage<T> a, AdjSub<T> b)
     aadd(old + cp, -gam * lG / dx);
     aadd(old + c, gam * lG / dx);
 }
+template <class T>
+__global__ void k_adj_sub_horiz(const __grid_constant__ DevParams<double> p, const __grid_constant__ AdjStage<T> a,
+                                const __grid_constant__ AdjSub<T> b) {
+    b_adj_sub_horiz(p, a, b, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // perturbation start rho_p = s0.rho - s.rho etc. (moist.jl:1339-1346)
 template <class T>
-__global__ void k_adj_p0(DevParams<double> p, AdjStage<T> a, DP<4> LP) {
+__device__ __forceinline__ void b_adj_p0(const DevParams<double>& p, const AdjStage<T>& a, const DP<4>& LP, int bid_x,
+                                         int bid_y, int bid_z) {
     ADJ_CELL(k, i);
     for (int f = 0; f < 4; f++) {
         const double l = LP.f[f][c];
@@ -826,13 +896,19 @@ __global__ void k_adj_p0(DevParams<double> p, AdjStage<T> a, DP<4> LP) {
         a.LS0[f][c] += l;
     }
 }
+template <class T>
+__global__ void k_adj_p0(const __grid_constant__ DevParams<double> p, const __grid_constant__ AdjStage<T> a,
+                         const __grid_constant__ DP<4> LP) {
+    b_adj_p0(p, a, LP, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // ----------------------------------------------------------------------------- stage tendencies
 
 // lambda of the w-p coefficients -> theta, rt2pres, per cell: theta_h(j) enters b_j, a_{j+1},
 // c_{j-1}; rt2pres(k) enters b_k, a_k, b_{k-1}, c_{k-1}
 template <class T>
-__global__ void k_adj_tri_coef_T(DevParams<double> p, AdjStage<T> a) {
+__device__ __forceinline__ void b_adj_tri_coef_T(const DevParams<double>& p, const AdjStage<T>& a, int bid_x, int bid_y,
+                                                 int bid_z) {
     ADJ_CELL(k, i);
     const int n = nz - 1;
     const double* dz = p.dz;
@@ -866,10 +942,15 @@ __global__ void k_adj_tri_coef_T(DevParams<double> p, AdjStage<T> a) {
     a.Ltheta[c] += lth;
     a.Lrt2[c] += lr;
 }
+template <class T>
+__global__ void k_adj_tri_coef_T(const __grid_constant__ DevParams<double> p, const __grid_constant__ AdjStage<T> a) {
+    b_adj_tri_coef_T(p, a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // lambda of R_rho, R_rho_u, R_rho_w, R_rho_theta -> their inputs
 template <class T>
-__global__ void __launch_bounds__(ADJ_THREADS) k_adj_tend_T(DevParams<double> p, AdjStage<T> a) {
+__device__ __forceinline__ void b_adj_tend_T(const DevParams<double>& p, const AdjStage<T>& a, int bid_x, int bid_y,
+                                             int bid_z) {
     ADJ_CELL(k, i);
     const int ke = nz - 1;
     const double dx = p.dx;
@@ -978,7 +1059,8 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_tend_T(DevParams<double> p,
         const double l = a.LRw[c];
         if (l != 0.0) {
             const T* wf = a.wf;
-            auto atw = [&](int kk, int ii) -> double { return (kk >= 0 && kk < ke) ? (double)wf[MOIST_IDX(kk, ii)] : 0.0; };
+            auto atw = [&](int kk,
+                           int ii) -> double { return (kk >= 0 && kk < ke) ? (double)wf[MOIST_IDX(kk, ii)] : 0.0; };
             double v[24] = {at(ru, k, i), at(ru, k + 1, i), at(ru, k, im), at(ru, k + 1, im),
                             at(rw, k - 1, i), at(rw, k, i), k + 1 < ke ? at(rw, k + 1, i) : 0.0,
                             atw(k, im2), atw(k, im), atw(k, i), atw(k, ip), atw(k, ip2),
@@ -1019,11 +1101,17 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_tend_T(DevParams<double> p,
         }
     }
 }
+template <class T>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_tend_T(const __grid_constant__ DevParams<double> p,
+                                  const __grid_constant__ AdjStage<T> a) {
+    b_adj_tend_T(p, a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // face velocities u_face = rho_u 2 / (rho_i + rho_i+1), w_face = rho_w / f2h(rho) (moist.jl:1091-1097,
 // 1185-1189)
 template <class T>
-__global__ void k_adj_face_T(DevParams<double> p, AdjStage<T> a) {
+__device__ __forceinline__ void b_adj_face_T(const DevParams<double>& p, const AdjStage<T>& a, int bid_x, int bid_y,
+                                             int bid_z) {
     ADJ_CELL(k, i);
     const int ip = wrapx(i + 1, nx);
     const double* dz = p.dz;
@@ -1050,10 +1138,15 @@ __global__ void k_adj_face_T(DevParams<double> p, AdjStage<T> a) {
         }
     }
 }
+template <class T>
+__global__ void k_adj_face_T(const __grid_constant__ DevParams<double> p, const __grid_constant__ AdjStage<T> a) {
+    b_adj_face_T(p, a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // diagnostics pres, theta, rt2pres -> rho, rho_theta, rho_q*
 template <class T>
-__global__ void __launch_bounds__(ADJ_THREADS) k_adj_diag_T(DevParams<double> p, AdjStage<T> a) {
+__device__ __forceinline__ void b_adj_diag_T(const DevParams<double>& p, const AdjStage<T>& a, int bid_x, int bid_y,
+                                             int bid_z) {
     ADJ_CELL(k, i);
     const double lo[3] = {a.Lpres[c], a.Ltheta[c], a.Lrt2[c]};
     if (lo[0] == 0.0 && lo[1] == 0.0 && lo[2] == 0.0) return;
@@ -1066,6 +1159,11 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_diag_T(DevParams<double> p,
                                  [&](int s, double d) { acc[s] += lo[o] * d; });
     }
     for (int s = 0; s < 5; s++) a.Lst[f_of_slot[s]][c] += acc[s];
+}
+template <class T>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_diag_T(const __grid_constant__ DevParams<double> p,
+                                  const __grid_constant__ AdjStage<T> a) {
+    b_adj_diag_T(p, a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ----------------------------------------------------------------------------- physics
@@ -1083,9 +1181,10 @@ struct AdjPhys {
 
 // phys assembly (moist.jl:1633-1643) and Kessler microphysics (554-671)
 template <class T>
-__global__ void __launch_bounds__(ADJ_THREADS) k_adj_kessler(DevParams<double> p, AdjPhys<T> a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = blockIdx.y;
+__device__ __forceinline__ void b_adj_kessler(const DevParams<double>& p, const AdjPhys<T>& a, int bid_x, int bid_y,
+                                              int bid_z) {
+    const int i = bid_x * blockDim.x + threadIdx.x;
+    const int k = bid_y;
     const int nx = p.nx, nz = p.nz, P = p.P;
     double par[2] = {0.0, 0.0};
     if (i < nx && k < nz) {
@@ -1129,11 +1228,17 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_kessler(DevParams<double> p
         if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(a.Lpar + j, v);
     }
 }
+template <class T>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_kessler(const __grid_constant__ DevParams<double> p,
+                                  const __grid_constant__ AdjPhys<T> a) {
+    b_adj_kessler(p, a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // rain sedimentation (moist.jl:674-707): sed(k) = (F(k+1) - F(k)) / dz(k), F = rho_qr Vt,
 // d_prec = F(0), prec += d_prec dt
 template <class T>
-__global__ void __launch_bounds__(ADJ_THREADS) k_adj_sed(DevParams<double> p, AdjPhys<T> a) {
+__device__ __forceinline__ void b_adj_sed(const DevParams<double>& p, const AdjPhys<T>& a, int bid_x, int bid_y,
+                                          int bid_z) {
     ADJ_CELL(k, i);
     if (!(p.do_mp && p.do_sed)) return;
     const double* dz = p.dz;
@@ -1153,11 +1258,17 @@ __global__ void __launch_bounds__(ADJ_THREADS) k_adj_sed(DevParams<double> p, Ad
     a.Lst[6][c] += acc[0];
     a.Lst[0][c] += acc[1];
 }
+template <class T>
+__global__ void __launch_bounds__(ADJ_THREADS) k_adj_sed(const __grid_constant__ DevParams<double> p,
+                                  const __grid_constant__ AdjPhys<T> a) {
+    b_adj_sed(p, a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 // lambda(S^n) = lambda of the first stage's input + lambda of s0
-__global__ void k_adj_step_end(int nx, int nz, int P, DP<7> Lst, DP<7> LS0, DP<5> Lph) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = blockIdx.y;
+__device__ __forceinline__ void b_adj_step_end(int nx, int nz, int P, const DP<7>& Lst, const DP<7>& LS0,
+                                               const DP<5>& Lph, int bid_x, int bid_y, int bid_z) {
+    const int i = bid_x * blockDim.x + threadIdx.x;
+    const int k = bid_y;
     if (i >= nx || k >= nz) return;
     const size_t c = MOIST_IDX(k, i);
     for (int f = 0; f < 7; f++) {
@@ -1165,6 +1276,10 @@ __global__ void k_adj_step_end(int nx, int nz, int P, DP<7> Lst, DP<7> LS0, DP<5
         LS0.f[f][c] = 0.0;
     }
     for (int f = 0; f < 5; f++) Lph.f[f][c] = 0.0;
+}
+__global__ void k_adj_step_end(int nx, int nz, int P, const __grid_constant__ DP<7> Lst,
+                               const __grid_constant__ DP<7> LS0, const __grid_constant__ DP<5> Lph) {
+    b_adj_step_end(nx, nz, P, Lst, LS0, Lph, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ----------------------------------------------------------------------------- host layout
@@ -1188,8 +1303,8 @@ __global__ void k_adj_to_ref(int nx, int nz, int halo, int P, const double* src,
 
 // objective J = sum_i w_i prec_i + sum_f <seed_f, state_f> over the interior
 template <class T>
-__global__ void k_adj_objective(int nx, int nz, int P, StateP<T> s, const T* prec, const double* prec_w,
-                                DP<7> seed, double* out) {
+__global__ void k_adj_objective(int nx, int nz, int P, StateP<T> s, const T* prec, const double* prec_w, DP<7> seed,
+                                double* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;
     double v = 0.0;

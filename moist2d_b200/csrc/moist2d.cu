@@ -20,7 +20,7 @@
 #include "../../include/moist2d.h"
 #include "kernels.cuh"
 #include "batch.cuh"
-#include "adjoint.cuh"
+#include "adjoint_batch.cuh"
 
 using namespace moist;
 
@@ -55,6 +55,7 @@ struct CtxBase {
     virtual int rk3_host(moist_state_host* s, int nsteps) = 0;
     virtual int pass_counts(int* counts, int n) = 0;
     virtual int set_wait_limit(long long cycles) = 0;
+    virtual int set_tape_mode(int mode) = 0;
     virtual int pass_trace(int nsteps, int maxrec, long long* pass_ns, int* pass_tiles, int* npasses) = 0;
     virtual int adjoint_run(int nsteps, int ckpt, const moist_adjoint_seed* seed, moist_adjoint_grad* out) = 0;
     virtual int autotune(int nsteps, std::string& report) = 0;
@@ -69,6 +70,7 @@ struct BatchBase {
     virtual int autotune(int nsteps, std::string& report) = 0;
     virtual int time_steps(int nsteps, float* ms) = 0;
     virtual int profile(int nsteps, float* total_ms, float* group_ms) = 0;
+    virtual int set_tape_mode(int mode) = 0;
 };
 
 }  // namespace
@@ -322,14 +324,20 @@ struct Ctx : CtxBase {
     } while (0)
 
     // device copies of nf whole fields (up to 8) in one launch
+    // copies of whole fields (n = fsz) are recorded when rec is set (the adjoint's tape)
     int copyf(const T* const* src, T* const* dst, int nf, size_t n = 0) {
         if (n == 0) n = fsz;
+        if (rec && n != fsz) return set_err(owner, MOIST_ERR_ARG, "a recorded copy covers whole fields");
         for (int f0 = 0; f0 < nf; f0 += 8) {
             CopyList<T> l{};
             l.nf = std::min(8, nf - f0);
             for (int j = 0; j < l.nf; j++) {
                 l.src[j] = src[f0 + j];
                 l.dst[j] = dst[f0 + j];
+            }
+            if (rec) {
+                rec->put(BK_COPY, BCopy<T>{l, n, bz_blocks(fsz)});
+                continue;
             }
             k_copy_fields<T><<<std::min<size_t>(1184, (n + 255) / 256), 256, 0, st>>>(l, n);
             CKL();
@@ -723,11 +731,11 @@ struct Ctx : CtxBase {
             sa.dprime = dprime;
             if (rec) {
                 rec->put(BK_SUB, BSub<T, TT>{dp, sa, dt_s, T(ns_s), fact_tp64, strip_wc, err});
-                continue;
+            } else {
+                k_substep_strip<T, TT><<<gs, STRIP_THREADS, strip_smem, st>>>(dp, sa, dt_s, T(ns_s), fact_tp64,
+                                                                              strip_wc, err);
+                CKL();
             }
-            k_substep_strip<T, TT><<<gs, STRIP_THREADS, strip_smem, st>>>(dp, sa, dt_s, T(ns_s), fact_tp64, strip_wc,
-                                                                          err);
-            CKL();
             if (tape) {
                 const T* src[4] = {rho_p, ru_p[n % 2], rw_p, rt_p[n % 3]};
                 if (int r = copyf(src, tape->sub[js][n].data(), 4)) return r;
@@ -964,6 +972,12 @@ struct Ctx : CtxBase {
     // bound of every device-side wait of the context's kernels, in SM clock cycles (<= 0: the
     // default of about two seconds)
     long long wait_default = 0;
+    int tape_mode = -1;  // moist_set_adjoint_tapes
+    int set_tape_mode(int mode) override {
+        tape_mode = mode;
+        return MOIST_OK;
+    }
+
     int set_wait_limit(long long cycles) override {
         if (!use_tiles)
             return set_err(owner, MOIST_ERR_UNSUPPORTED, "the context runs no kernel that waits on other blocks");
@@ -1237,7 +1251,9 @@ struct Ctx : CtxBase {
         return j == 0 ? std::max(1, (int)std::ceil(ns / 3.0)) : (j == 1 ? std::max(1, (int)std::ceil(ns / 2.0)) : ns);
     }
 
-    int adj_alloc(int nsteps, int ckpt) {
+    // seg_mode: -1 decides the tape mode from the free memory; 0 / 1 sets one tape / a tape per
+    // step of a segment (the packed batch adjoint runs every member in the same mode)
+    int adj_alloc(int nsteps, int ckpt, int seg_mode = -1) {
         if (!adj) {
             adj = new Adj();
             Adj& A = *adj;
@@ -1288,7 +1304,10 @@ struct Ctx : CtxBase {
         Adj& A = *adj;
         // a tape per step of a segment when that fits in half the free device memory (the
         // segment is then recomputed once), else one tape and the segment's States
-        if (ckpt != adj_ckpt) {  // decided once per checkpoint interval
+        if (seg_mode >= 0) {
+            seg_tapes = seg_mode == 1;
+            adj_ckpt = -1;  // a later moist_adjoint_run decides again
+        } else if (ckpt != adj_ckpt) {  // decided once per checkpoint interval
             size_t free_b = 0, total_b = 0;
             CK(cudaMemGetInfo(&free_b, &total_b));
             const size_t need =
@@ -1346,7 +1365,8 @@ struct Ctx : CtxBase {
     std::array<T*, 7> cur_fields() const { return {cur.rho, cur.ru, cur.rw, cur.rt, cur.qv, cur.qc, cur.qr}; }
 
     // the adjoint of one large step: lambda of the step's output State in A.Lst becomes the
-    // lambda of its input State; the tape holds the step's internals
+    // lambda of its input State; the tape holds the step's internals. With rec set, every
+    // launch is recorded for a packed batch launch (adjoint_batch.cuh) instead.
     int adj_step(const Tape& tp) {
         Adj& A = *adj;
         const dim3 b(ADJ_THREADS), gc(cdiv(nx, ADJ_THREADS), nz), gc3(cdiv(nx, ADJ_THREADS), nz, 3);
@@ -1359,7 +1379,10 @@ struct Ctx : CtxBase {
         for (int j = 2; j >= 0; j--) {
             const int m = stage_substeps(j);
             const StateP<T> s{tp.in[j][0], tp.in[j][1], tp.in[j][2], tp.in[j][3], tp.in[j][4], tp.in[j][5], tp.in[j][6]};
-            k_diag<T><<<g2, b2, 0, st>>>(dp, s, pres, theta, rt2p, uface, wface, err);
+            if (rec)
+                rec->put(BK_DIAG, BDiag<T>{dp, s, pres, theta, rt2p, uface, wface, err});
+            else
+                k_diag<T><<<g2, b2, 0, st>>>(dp, s, pres, theta, rt2p, uface, wface, err);
             AdjStage<T> a{};
             a.s = s;
             a.theta = theta;
@@ -1414,16 +1437,27 @@ struct Ctx : CtxBase {
             a.Ltp_rt = A.Ltp_rt;
             a.Linc_rho = A.Linc_rho;
             a.Linc_rt = A.Linc_rt;
-            CK(cudaMemsetAsync(A.acc, 0, 16 * fsz * sizeof(double), st));
-            k_adj_tri_coef<T><<<gc, b, 0, st>>>(A.pd, a);
-            k_adj_tri_fact<<<gcol, 32, 0, st>>>(nx, nz, P, A.Ta, A.Tb, A.Tc, A.Tcp, A.Trd);
             DP<4> LPc{{A.LP[lp][0], A.LP[lp][1], A.LP[lp][2], A.LP[lp][3]}};
-            k_adj_update<T><<<gc, b, 0, st>>>(A.pd, a, LPc);
-            k_adj_tr_jac<T><<<gc3, b, 0, st>>>(A.pd, a, A.J);
             const DP<3> lq{{A.Lqout[0], A.Lqout[1], A.Lqout[2]}}, mu{{A.mu[0], A.mu[1], A.mu[2]}};
-            k_adj_tr_rev<<<3, (nz + 31) / 32 * 32, 3 * nz * sizeof(double), st>>>(nx, nz, P, A.J, lq, mu);
-            k_adj_tr_scatter<T><<<gc3, b, 0, st>>>(A.pd, a, A.J, mu);
-            k_adj_mf<T><<<gc, b, 0, st>>>(A.pd, a);
+            if (rec) {
+                rec->put(BK_ZERO, BZero{A.acc, 16 * fsz, bz_blocks(fsz)});
+                rec->put(AK_TRI_COEF, AStage<T>{A.pd, a});
+                rec->put(AK_TRI_FACT, ATriFact{nx, nz, P, A.Ta, A.Tb, A.Tc, A.Tcp, A.Trd});
+                rec->put(AK_UPDATE, AStageLP<T>{A.pd, a, LPc});
+                rec->put(AK_TR_JAC, ATrJac<T>{A.pd, a, A.J});
+                rec->put(AK_TR_REV, ATrRev{nx, nz, P, A.J, lq, mu});
+                rec->put(AK_TR_SCATTER, ATrScatter<T>{A.pd, a, A.J, mu});
+                rec->put(AK_MF, AStage<T>{A.pd, a});
+            } else {
+                CK(cudaMemsetAsync(A.acc, 0, 16 * fsz * sizeof(double), st));
+                k_adj_tri_coef<T><<<gc, b, 0, st>>>(A.pd, a);
+                k_adj_tri_fact<<<gcol, 32, 0, st>>>(nx, nz, P, A.Ta, A.Tb, A.Tc, A.Tcp, A.Trd);
+                k_adj_update<T><<<gc, b, 0, st>>>(A.pd, a, LPc);
+                k_adj_tr_jac<T><<<gc3, b, 0, st>>>(A.pd, a, A.J);
+                k_adj_tr_rev<<<3, (nz + 31) / 32 * 32, 3 * nz * sizeof(double), st>>>(nx, nz, P, A.J, lq, mu);
+                k_adj_tr_scatter<T><<<gc3, b, 0, st>>>(A.pd, a, A.J, mu);
+                k_adj_mf<T><<<gc, b, 0, st>>>(A.pd, a);
+            }
             for (int n = m; n >= 1; n--) {
                 AdjSub<T> sb;
                 sb.prev_rt = tp.sub[j][n - 1][3];
@@ -1436,21 +1470,38 @@ struct Ctx : CtxBase {
                     sb.LPo[f] = A.LP[1 - lp][f];
                 }
                 sb.n = n;
-                k_adj_sub_vert<T><<<gc, b, 0, st>>>(A.pd, a, sb);
-                k_adj_sub_solve<<<cdiv(nx, adj_solve_cols(nz)), ADJ_SOLVE_THREADS, adj_solve_smem(nz), st>>>(
-                    nx, nz, P, A.Tc, A.Tcp, A.Trd, A.Lx, A.Ly);
-                k_adj_sub_rhs<T><<<gc, b, 0, st>>>(A.pd, dp, a, sb);
-                k_adj_sub_expl<T><<<gc, b, 0, st>>>(A.pd, a, sb);
-                k_adj_sub_horiz<T><<<gc, b, 0, st>>>(A.pd, a, sb);
+                if (rec) {
+                    const ASub<T> as{A.pd, dp, a, sb};
+                    rec->put(AK_SUB_VERT, as);
+                    rec->put(AK_SUB_SOLVE, ASolve{nx, nz, P, A.Tc, A.Tcp, A.Trd, A.Lx, A.Ly});
+                    rec->put(AK_SUB_RHS, as);
+                    rec->put(AK_SUB_EXPL, as);
+                    rec->put(AK_SUB_HORIZ, as);
+                } else {
+                    k_adj_sub_vert<T><<<gc, b, 0, st>>>(A.pd, a, sb);
+                    k_adj_sub_solve<<<cdiv(nx, adj_solve_cols(nz)), ADJ_SOLVE_THREADS, adj_solve_smem(nz), st>>>(
+                        nx, nz, P, A.Tc, A.Tcp, A.Trd, A.Lx, A.Ly);
+                    k_adj_sub_rhs<T><<<gc, b, 0, st>>>(A.pd, dp, a, sb);
+                    k_adj_sub_expl<T><<<gc, b, 0, st>>>(A.pd, a, sb);
+                    k_adj_sub_horiz<T><<<gc, b, 0, st>>>(A.pd, a, sb);
+                }
                 lp = 1 - lp;
             }
             DP<4> LP0{{A.LP[lp][0], A.LP[lp][1], A.LP[lp][2], A.LP[lp][3]}};
-            k_adj_p0<T><<<gc, b, 0, st>>>(A.pd, a, LP0);
-            k_adj_tri_coef_T<T><<<gc, b, 0, st>>>(A.pd, a);
-            k_adj_tend_T<T><<<gc, b, 0, st>>>(A.pd, a);
-            k_adj_face_T<T><<<gc, b, 0, st>>>(A.pd, a);
-            k_adj_diag_T<T><<<gc, b, 0, st>>>(A.pd, a);
-            CKL();
+            if (rec) {
+                rec->put(AK_P0, AStageLP<T>{A.pd, a, LP0});
+                rec->put(AK_TRI_COEF_T, AStage<T>{A.pd, a});
+                rec->put(AK_TEND_T, AStage<T>{A.pd, a});
+                rec->put(AK_FACE_T, AStage<T>{A.pd, a});
+                rec->put(AK_DIAG_T, AStage<T>{A.pd, a});
+            } else {
+                k_adj_p0<T><<<gc, b, 0, st>>>(A.pd, a, LP0);
+                k_adj_tri_coef_T<T><<<gc, b, 0, st>>>(A.pd, a);
+                k_adj_tend_T<T><<<gc, b, 0, st>>>(A.pd, a);
+                k_adj_face_T<T><<<gc, b, 0, st>>>(A.pd, a);
+                k_adj_diag_T<T><<<gc, b, 0, st>>>(A.pd, a);
+                CKL();
+            }
         }
         AdjPhys<T> ph;
         ph.s = StateP<T>{tp.in[0][0], tp.in[0][1], tp.in[0][2], tp.in[0][3], tp.in[0][4], tp.in[0][5], tp.in[0][6]};
@@ -1460,8 +1511,6 @@ struct Ctx : CtxBase {
         ph.Lsed = A.Lsed;
         ph.prec_w = A.prec_w;
         ph.Lpar = A.Lpar;
-        k_adj_kessler<T><<<gc, b, 0, st>>>(A.pd, ph);
-        k_adj_sed<T><<<gc, b, 0, st>>>(A.pd, ph);
         DP<7> L7, S7;
         DP<5> L5;
         for (int f = 0; f < 7; f++) {
@@ -1469,38 +1518,125 @@ struct Ctx : CtxBase {
             S7.f[f] = A.LS0[f];
         }
         for (int f = 0; f < 5; f++) L5.f[f] = A.Lph[f];
+        if (rec) {
+            rec->put(AK_KESSLER, APhys<T>{A.pd, ph});
+            rec->put(AK_SED, APhys<T>{A.pd, ph});
+            rec->put(AK_STEP_END, AStepEnd{nx, nz, P, L7, S7, L5});
+            return MOIST_OK;
+        }
+        k_adj_kessler<T><<<gc, b, 0, st>>>(A.pd, ph);
+        k_adj_sed<T><<<gc, b, 0, st>>>(A.pd, ph);
         k_adj_step_end<<<gc, b, 0, st>>>(nx, nz, P, L7, S7, L5);
         CKL();
         return MOIST_OK;
     }
 
-    int adjoint_run(int nsteps, int ckpt, const moist_adjoint_seed* seed, moist_adjoint_grad* out) override {
+    // moist_adjoint_run in phases; the packed batch adjoint runs the same phases around its
+    // packed forward and reverse steps
+    bool adj_seed_on[7] = {false, false, false, false, false, false, false};
+    bool adj_prec_on = false;
+
+    int adj_check(int nsteps, int ckpt, const void* out) {
         if (int r = check_stage_shape()) return r;
         if (!out || nsteps < 1 || ckpt < 1)
             return set_err(owner, MOIST_ERR_ARG, "moist_adjoint_run needs out != NULL, nsteps >= 1 and ckpt_every >= 1");
         if (dp.do_sf || dp.do_rd)
             return set_err(owner, MOIST_ERR_UNSUPPORTED,
                            "moist_adjoint_run covers do_sf = do_rd = 0 (surface fluxes and radiation are not differentiated)");
-        ckpt = std::min(ckpt, nsteps);
-        if (int r = adj_alloc(nsteps, ckpt)) return r;
+        return MOIST_OK;
+    }
+
+    // the seeds on the device, the error words reset
+    int adj_seeds(const moist_adjoint_seed* seed) {
         Adj& A = *adj;
+        const dim3 b(ADJ_THREADS), gc(cdiv(nx, ADJ_THREADS), nz);
         const int ia = nx + 2 * halo;
-        const dim3 b(ADJ_THREADS), gc(cdiv(nx, ADJ_THREADS), nz), gr(cdiv(ia, ADJ_THREADS), nz);
-        // seeds
-        bool seed_on[7];
         for (int f = 0; f < 7; f++) {
             const double* h = seed ? seed->state[f] : nullptr;
-            seed_on[f] = h != nullptr;
+            adj_seed_on[f] = h != nullptr;
             if (h) {
                 CK(cudaMemcpyAsync(A.stage, h, (size_t)nz * ia * sizeof(double), cudaMemcpyHostToDevice, st));
                 k_adj_from_ref<<<gc, b, 0, st>>>(nx, nz, halo, P, A.stage, A.seed[f]);
                 CKL();
             }
         }
-        const bool prec_on = seed && seed->prec_weight;
-        if (prec_on) CK(cudaMemcpyAsync(A.prec_w, seed->prec_weight + halo, nx * sizeof(double), cudaMemcpyHostToDevice, st));
+        adj_prec_on = seed && seed->prec_weight;
+        if (adj_prec_on)
+            CK(cudaMemcpyAsync(A.prec_w, seed->prec_weight + halo, nx * sizeof(double), cudaMemcpyHostToDevice, st));
         CK(reset_err());
+        return MOIST_OK;
+    }
+
+    // after the forward run: the objective, the final State kept, lambda of the final State
+    int adj_begin() {
+        Adj& A = *adj;
+        const dim3 b(ADJ_THREADS), gc(cdiv(nx, ADJ_THREADS), nz);
+        CK(cudaMemsetAsync(A.obj, 0, sizeof(double), st));
+        DP<7> sd;
+        for (int f = 0; f < 7; f++) sd.f[f] = adj_seed_on[f] ? A.seed[f] : nullptr;
+        k_adj_objective<T><<<gc, b, 0, st>>>(nx, nz, P, cur, prec, adj_prec_on ? A.prec_w : nullptr, sd, A.obj);
+        CKL();
         int r;
+        {
+            const auto src = cur_fields();
+            if ((r = copyf(src.data(), A.fin.data(), 7)) != MOIST_OK) return r;
+            CK(cudaMemcpyAsync(A.fin[7], prec, P * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        }
+        for (int f = 0; f < 7; f++) {
+            if (adj_seed_on[f])
+                CK(cudaMemcpyAsync(A.Lst[f], A.seed[f], fsz * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            else
+                CK(cudaMemsetAsync(A.Lst[f], 0, fsz * sizeof(double), st));
+            CK(cudaMemsetAsync(A.LS0[f], 0, fsz * sizeof(double), st));
+        }
+        for (int f = 0; f < 5; f++) CK(cudaMemsetAsync(A.Lph[f], 0, fsz * sizeof(double), st));
+        CK(cudaMemsetAsync(A.Lpar, 0, 2 * sizeof(double), st));
+        if (!adj_prec_on) CK(cudaMemsetAsync(A.prec_w, 0, P * sizeof(double), st));
+        return MOIST_OK;
+    }
+
+    // after the reverse sweep: the gradients to the host, the context back at the final State
+    int adj_results(const moist_adjoint_seed* seed, moist_adjoint_grad* out, double forward_ms, double reverse_ms) {
+        Adj& A = *adj;
+        const int ia = nx + 2 * halo;
+        const dim3 b(ADJ_THREADS), gr(cdiv(ia, ADJ_THREADS), nz);
+        int r;
+        for (int f = 0; f < 7; f++) {
+            if (!out->state[f]) continue;
+            k_adj_to_ref<<<gr, b, 0, st>>>(nx, nz, halo, P, A.Lst[f], A.stage);
+            CKL();
+            CK(cudaMemcpyAsync(out->state[f], A.stage, (size_t)nz * ia * sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
+        double hp[3];
+        CK(cudaMemcpyAsync(hp, A.Lpar, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hp + 2, A.obj, sizeof(double), cudaMemcpyDeviceToHost, st));
+        {
+            const auto dstf = cur_fields();
+            if ((r = copyf(A.fin.data(), dstf.data(), 7)) != MOIST_OK) return r;
+            CK(cudaMemcpyAsync(prec, A.fin[7], P * sizeof(T), cudaMemcpyDeviceToDevice, st));
+        }
+        CK(cudaStreamSynchronize(st));
+        if (out->prec) {
+            for (int j = 0; j < ia; j++) {
+                const int i = j - halo;
+                out->prec[j] = (adj_prec_on && i >= 0 && i < nx) ? seed->prec_weight[j] : 0.0;
+            }
+        }
+        out->k_auto = hp[0];
+        out->qc_threshold = hp[1];
+        out->objective = hp[2];
+        out->forward_ms = forward_ms;
+        out->reverse_ms = reverse_ms;
+        return finish();
+    }
+
+    int adjoint_run(int nsteps, int ckpt, const moist_adjoint_seed* seed, moist_adjoint_grad* out) override {
+        if (int r = adj_check(nsteps, ckpt, out)) return r;
+        ckpt = std::min(ckpt, nsteps);
+        if (int r = adj_alloc(nsteps, ckpt, tape_mode)) return r;
+        Adj& A = *adj;
+        int r;
+        if ((r = adj_seeds(seed)) != MOIST_OK) return r;
         // forward run, keeping the State every ckpt steps
         const auto t0 = std::chrono::steady_clock::now();
         for (int n = 0; n < nsteps; n++) {
@@ -1512,28 +1648,7 @@ struct Ctx : CtxBase {
         }
         CK(cudaStreamSynchronize(st));
         const auto t1 = std::chrono::steady_clock::now();
-        // objective and the final State
-        CK(cudaMemsetAsync(A.obj, 0, sizeof(double), st));
-        DP<7> sd;
-        for (int f = 0; f < 7; f++) sd.f[f] = seed_on[f] ? A.seed[f] : nullptr;
-        k_adj_objective<T><<<gc, b, 0, st>>>(nx, nz, P, cur, prec, prec_on ? A.prec_w : nullptr, sd, A.obj);
-        CKL();
-        {
-            const auto src = cur_fields();
-            if ((r = copyf(src.data(), A.fin.data(), 7)) != MOIST_OK) return r;
-            CK(cudaMemcpyAsync(A.fin[7], prec, P * sizeof(T), cudaMemcpyDeviceToDevice, st));
-        }
-        // lambda of the final State = the seeds
-        for (int f = 0; f < 7; f++) {
-            if (seed_on[f])
-                CK(cudaMemcpyAsync(A.Lst[f], A.seed[f], fsz * sizeof(double), cudaMemcpyDeviceToDevice, st));
-            else
-                CK(cudaMemsetAsync(A.Lst[f], 0, fsz * sizeof(double), st));
-            CK(cudaMemsetAsync(A.LS0[f], 0, fsz * sizeof(double), st));
-        }
-        for (int f = 0; f < 5; f++) CK(cudaMemsetAsync(A.Lph[f], 0, fsz * sizeof(double), st));
-        CK(cudaMemsetAsync(A.Lpar, 0, 2 * sizeof(double), st));
-        if (!prec_on) CK(cudaMemsetAsync(A.prec_w, 0, P * sizeof(double), st));
+        if ((r = adj_begin()) != MOIST_OK) return r;
         // reverse sweep, one segment of ckpt steps at a time
         const int nck = (nsteps + ckpt - 1) / ckpt;
         for (int sg = nck - 1; sg >= 0; sg--) {
@@ -1573,35 +1688,8 @@ struct Ctx : CtxBase {
         }
         CK(cudaStreamSynchronize(st));
         const auto t2 = std::chrono::steady_clock::now();
-        // results
-        for (int f = 0; f < 7; f++) {
-            if (!out->state[f]) continue;
-            k_adj_to_ref<<<gr, b, 0, st>>>(nx, nz, halo, P, A.Lst[f], A.stage);
-            CKL();
-            CK(cudaMemcpyAsync(out->state[f], A.stage, (size_t)nz * ia * sizeof(double), cudaMemcpyDeviceToHost, st));
-        }
-        double hp[3];
-        CK(cudaMemcpyAsync(hp, A.Lpar, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(hp + 2, A.obj, sizeof(double), cudaMemcpyDeviceToHost, st));
-        // the context keeps the final State
-        {
-            const auto dstf = cur_fields();
-            if ((r = copyf(A.fin.data(), dstf.data(), 7)) != MOIST_OK) return r;
-            CK(cudaMemcpyAsync(prec, A.fin[7], P * sizeof(T), cudaMemcpyDeviceToDevice, st));
-        }
-        CK(cudaStreamSynchronize(st));
-        if (out->prec) {
-            for (int j = 0; j < ia; j++) {
-                const int i = j - halo;
-                out->prec[j] = (prec_on && i >= 0 && i < nx) ? seed->prec_weight[j] : 0.0;
-            }
-        }
-        out->k_auto = hp[0];
-        out->qc_threshold = hp[1];
-        out->objective = hp[2];
-        out->forward_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-        out->reverse_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
-        return finish();
+        return adj_results(seed, out, std::chrono::duration<double, std::milli>(t1 - t0).count(),
+                           std::chrono::duration<double, std::milli>(t2 - t1).count());
     }
 };
 
@@ -1833,7 +1921,7 @@ struct BatchImpl : BatchBase {
     void items_of(int kind, std::vector<BItem>& it, dim3& block, size_t& smem, int group) {
         const int n = (int)m.size();
         smem = 0;
-        auto in_group = [&](int i) { return grp[i] == group; };
+        auto in_group = [&](int i) { return group < 0 || grp[i] == group; };  // group < 0: every member
         auto cells = [&](int i) {
             for (unsigned by = 0; by < cdiv(m[i]->nz, 8); by++)
                 for (unsigned bx = 0; bx < cdiv(m[i]->nx, 32); bx++) it.push_back({i, (int)bx, (int)by});
@@ -1894,6 +1982,63 @@ struct BatchImpl : BatchBase {
                 block = dim3(32);
                 for (int i = 0; i < n; i++)
                     if (in_group(i)) it.push_back({i, 0, 0});
+                break;
+            // the adjoint's launches (adjoint_batch.cuh)
+            case BK_ZERO:
+            case BK_COPY:
+                block = dim3(256);
+                for (int i = 0; i < n; i++)
+                    if (in_group(i))
+                        for (unsigned bx = 0; bx < bz_blocks(m[i]->fsz); bx++) it.push_back({i, (int)bx, 0});
+                break;
+            case AK_TRI_FACT:
+                block = dim3(32);
+                for (int i = 0; i < n; i++)
+                    if (in_group(i))
+                        for (unsigned bx = 0; bx < cdiv(m[i]->nx, 32); bx++) it.push_back({i, (int)bx, 0});
+                break;
+            case AK_TR_REV: {  // one block per member and tracer, the longest sweeps first
+                block = dim3(max_rows);
+                int maxnz = 1;
+                std::vector<int> order;
+                for (int i = 0; i < n; i++)
+                    if (in_group(i)) {
+                        order.push_back(i);
+                        maxnz = std::max(maxnz, m[i]->nz);
+                    }
+                smem = (size_t)3 * maxnz * sizeof(double);
+                std::stable_sort(order.begin(), order.end(),
+                                 [&](int a, int b) { return m[a]->nx + m[a]->nz > m[b]->nx + m[b]->nz; });
+                for (int i : order)
+                    for (int t = 0; t < 3; t++) it.push_back({i, t, 0});
+                break;
+            }
+            case AK_SUB_SOLVE:
+                block = dim3(ADJ_SOLVE_THREADS);
+                for (int i = 0; i < n; i++)
+                    if (in_group(i)) {
+                        smem = std::max(smem, adj_solve_smem(m[i]->nz));
+                        for (unsigned bx = 0; bx < cdiv(m[i]->nx, adj_solve_cols(m[i]->nz)); bx++)
+                            it.push_back({i, (int)bx, 0});
+                    }
+                break;
+            case AK_TR_JAC:
+            case AK_TR_SCATTER:  // by = row + nz * tracer
+                block = dim3(ADJ_THREADS);
+                for (int i = 0; i < n; i++)
+                    if (in_group(i))
+                        for (int by = 0; by < 3 * m[i]->nz; by++)
+                            for (unsigned bx = 0; bx < cdiv(m[i]->nx, ADJ_THREADS); bx++) it.push_back({i, (int)bx, by});
+                break;
+            default:  // the adjoint's cell kernels: (x block of ADJ_THREADS cells, row)
+                if (kind >= AK_TRI_COEF && kind < AK_NKINDS) {
+                    block = dim3(ADJ_THREADS);
+                    for (int i = 0; i < n; i++)
+                        if (in_group(i))
+                            for (int by = 0; by < m[i]->nz; by++)
+                                for (unsigned bx = 0; bx < cdiv(m[i]->nx, ADJ_THREADS); bx++)
+                                    it.push_back({i, (int)bx, by});
+                }
                 break;
         }
     }
@@ -1956,6 +2101,33 @@ struct BatchImpl : BatchBase {
             BATCH_LAUNCH(BK_UPD, BUpd<T>, FUpd<T>, 4)
             BATCH_LAUNCH(BK_STAGE_END, BStageEnd, FStageEnd, 1)
             BATCH_LAUNCH(BK_PREC, BPrec<T>, FPrec<T>, 1)
+            BATCH_LAUNCH(BK_ZERO, BZero, FZero, 1)
+            BATCH_LAUNCH(BK_COPY, BCopy<T>, FCopy<T>, 1)
+            BATCH_LAUNCH(AK_TRI_COEF, AStage<T>, FATriCoef<T>, 1)
+            BATCH_LAUNCH(AK_TRI_FACT, ATriFact, FATriFact, 1)
+            BATCH_LAUNCH(AK_UPDATE, AStageLP<T>, FAUpdate<T>, 1)
+            BATCH_LAUNCH(AK_TR_REV, ATrRev, FATrRev, 1)
+            BATCH_LAUNCH(AK_TR_SCATTER, ATrScatter<T>, FATrScatter<T>, 1)
+            BATCH_LAUNCH(AK_MF, AStage<T>, FAMf<T>, 1)
+            BATCH_LAUNCH(AK_SUB_VERT, ASub<T>, FASubVert<T>, 1)
+            BATCH_LAUNCH(AK_SUB_RHS, ASub<T>, FASubRhs<T>, 1)
+            BATCH_LAUNCH(AK_SUB_EXPL, ASub<T>, FASubExpl<T>, 1)
+            BATCH_LAUNCH(AK_SUB_HORIZ, ASub<T>, FASubHoriz<T>, 1)
+            BATCH_LAUNCH(AK_P0, AStageLP<T>, FAP0<T>, 1)
+            BATCH_LAUNCH(AK_TRI_COEF_T, AStage<T>, FATriCoefT<T>, 1)
+            BATCH_LAUNCH(AK_FACE_T, AStage<T>, FAFaceT<T>, 1)
+            BATCH_LAUNCH(AK_STEP_END, AStepEnd, FAStepEnd, 1)
+#define BATCH_LAUNCH_B(KIND, A, F, MAXT)                                                               \
+    case KIND:                                                                                         \
+        k_batched_b<A, F, MAXT, 1><<<s.nitems, s.block, s.smem, ls>>>(s.items, (const A*)s.args, F{}); \
+        break;
+            BATCH_LAUNCH_B(AK_TR_JAC, ATrJac<T>, FATrJac<T>, ADJ_THREADS)
+            BATCH_LAUNCH_B(AK_SUB_SOLVE, ASolve, FASubSolve, ADJ_SOLVE_THREADS)
+            BATCH_LAUNCH_B(AK_TEND_T, AStage<T>, FATendT<T>, ADJ_THREADS)
+            BATCH_LAUNCH_B(AK_DIAG_T, AStage<T>, FADiagT<T>, ADJ_THREADS)
+            BATCH_LAUNCH_B(AK_KESSLER, APhys<T>, FAKessler<T>, ADJ_THREADS)
+            BATCH_LAUNCH_B(AK_SED, APhys<T>, FASed<T>, ADJ_THREADS)
+#undef BATCH_LAUNCH_B
             default:
                 return set_berr(owner, MOIST_ERR_ARG, "unknown launch kind %d", s.kind);
         }
@@ -1987,14 +2159,22 @@ struct BatchImpl : BatchBase {
         return MOIST_OK;
     }
 
-    // every member's moist_adjoint_run, the members' device buffers allocated one member at a
-    // time first, then the runs from up to nthreads host threads (each member works on its own
-    // stream, so their kernels overlap on the GPU)
+    // moist_batch_adjoint_run. nthreads <= 0: packed, every kernel of the members' forward,
+    // recomputation and reverse steps one launch for all members (adjoint_packed); nthreads > 0:
+    // every member's own moist_adjoint_run from up to nthreads host threads (adjoint_threads)
     int adjoint(int nsteps, int ckpt, const moist_adjoint_seed* seeds, moist_adjoint_grad* out,
                 int nthreads) override {
-        const int n = (int)m.size();
         if (!out || nsteps < 1 || ckpt < 1)
             return set_berr(owner, MOIST_ERR_ARG, "moist_batch_adjoint_run needs out != NULL, nsteps >= 1, ckpt_every >= 1");
+        return nthreads > 0 ? adjoint_threads(nsteps, ckpt, seeds, out, nthreads) : adjoint_packed(nsteps, ckpt, seeds, out);
+    }
+
+    // the members' device buffers allocated one member at a time first, then the members' runs
+    // from up to nthreads host threads (each member works on its own stream, so their kernels
+    // overlap on the GPU)
+    int adjoint_threads(int nsteps, int ckpt, const moist_adjoint_seed* seeds, moist_adjoint_grad* out,
+                        int nthreads) {
+        const int n = (int)m.size();
         BCK(cudaStreamSynchronize(st));
         const int ck = std::min(ckpt, nsteps);
         for (int i = 0; i < n; i++) {
@@ -2010,7 +2190,7 @@ struct BatchImpl : BatchBase {
             for (int i; (i = next.fetch_add(1)) < n;)
                 rc[i] = m[i]->adjoint_run(nsteps, ckpt, seeds ? seeds + i : nullptr, out + i);
         };
-        const int nt = std::max(1, std::min(nthreads > 0 ? nthreads : n, n));
+        const int nt = std::max(1, std::min(nthreads, n));
         std::vector<std::thread> th;
         for (int t = 1; t < nt; t++) th.emplace_back(work);
         work();
@@ -2020,6 +2200,222 @@ struct BatchImpl : BatchBase {
                 if (rc[i] == MOIST_ERR_NAN) owner->nan_member = i;
                 return set_berr(owner, rc[i], "member %d: %s", i, m[i]->owner->err.c_str());
             }
+        return MOIST_OK;
+    }
+
+    int tape_mode = -1;  // moist_batch_set_adjoint_tapes
+    int set_tape_mode(int mode) override {
+        tape_mode = mode;
+        for (auto* c : m) c->tape_mode = mode;
+        return MOIST_OK;
+    }
+
+    // ------------------------------------------------------------------ packed adjoint
+    // Work lists per launch kind (built once per packed adjoint run) and the argument arrays of
+    // its recorded phases, released when the run ends.
+    std::vector<Slot> adj_kslot;
+    std::vector<void*> adj_mem;
+
+    void adj_release() {
+        cudaStreamSynchronize(st);
+        for (void* a : adj_mem) cudaFree(a);
+        adj_mem.clear();
+        adj_kslot.clear();
+    }
+
+    // the members' records of one phase as packed launches: every launch's argument structs
+    // side by side in one device allocation, its work list shared by the launches of its kind
+    int adj_pack(std::vector<StepRecord>& rec, std::vector<Slot>& out) {
+        const int n = (int)m.size();
+        for (int i = 1; i < n; i++)
+            if (rec[i].kind != rec[0].kind)
+                return set_berr(owner, MOIST_ERR_ARG, "member %d takes other adjoint launches than member 0", i);
+        std::vector<size_t> off(rec[0].kind.size());
+        size_t total = 0;
+        for (size_t j = 0; j < rec[0].kind.size(); j++) {
+            off[j] = total;
+            total += (rec[0].args[j].size() * n + 255) / 256 * 256;
+        }
+        std::vector<unsigned char> h(std::max<size_t>(total, 1));
+        for (size_t j = 0; j < rec[0].kind.size(); j++) {
+            const size_t sz = rec[0].args[j].size();
+            for (int i = 0; i < n; i++) std::memcpy(h.data() + off[j] + sz * i, rec[i].args[j].data(), sz);
+        }
+        void* d = nullptr;
+        if (cudaMalloc(&d, h.size()) != cudaSuccess)
+            return set_berr(owner, MOIST_ERR_NOMEM, "cudaMalloc of %zu bytes of adjoint launch arguments failed", h.size());
+        adj_mem.push_back(d);
+        BCK(cudaMemcpy(d, h.data(), h.size(), cudaMemcpyHostToDevice));
+        if (adj_kslot.empty()) adj_kslot.resize(AK_NKINDS);
+        for (size_t j = 0; j < rec[0].kind.size(); j++) {
+            const int kind = rec[0].kind[j];
+            Slot& ks = adj_kslot[kind];
+            if (!ks.items) {
+                std::vector<BItem> it;
+                ks.kind = kind;
+                items_of(kind, it, ks.block, ks.smem, -1);
+                void* di = nullptr;
+                if (cudaMalloc(&di, std::max<size_t>(it.size(), 1) * sizeof(BItem)) != cudaSuccess)
+                    return set_berr(owner, MOIST_ERR_NOMEM, "cudaMalloc of an adjoint work list failed");
+                adj_mem.push_back(di);
+                BCK(cudaMemcpy(di, it.data(), it.size() * sizeof(BItem), cudaMemcpyHostToDevice));
+                ks.items = (const BItem*)di;
+                ks.nitems = (unsigned)it.size();
+            }
+            Slot sl = ks;
+            sl.args = (const unsigned char*)d + off[j];
+            sl.group = 0;
+            if (sl.nitems) out.push_back(sl);
+        }
+        return MOIST_OK;
+    }
+
+    int run_slots(const std::vector<Slot>& sl) {
+        for (const Slot& s : sl)
+            if (int r = launch(s, st)) return r;
+        return MOIST_OK;
+    }
+
+    // the members' current State in the buffers the graph of parity 0 reads
+    void at_parity0() {
+        for (size_t i = 0; i < m.size(); i++) {
+            m[i]->cur = cur0[i];
+            m[i]->nxt = nxt0[i];
+        }
+        parity = 0;
+    }
+
+    int adjoint_packed(int nsteps, int ckpt, const moist_adjoint_seed* seeds, moist_adjoint_grad* out) {
+        const int n = (int)m.size();
+        for (int i = 0; i < n; i++)
+            if (int r = m[i]->adj_check(nsteps, ckpt, out + i))
+                return set_berr(owner, r, "member %d: %s", i, m[i]->owner->err.c_str());
+        if (int r = sync_members()) return r;
+        BCK(cudaStreamSynchronize(st));
+        const int ck = std::min(ckpt, nsteps);
+        // one tape mode for every member: a tape per step of a segment when all of them fit in
+        // half the free device memory, else one tape and the segment's States
+        size_t free_b = 0, total_b = 0;
+        BCK(cudaMemGetInfo(&free_b, &total_b));
+        size_t need = 0;
+        for (int i = 0; i < n; i++) {
+            const size_t have = m[i]->adj ? m[i]->adj->tapes.size() : 0;
+            if (have < (size_t)ck) need += (ck - have) * m[i]->tape_fields() * m[i]->fsz * sizeof(T);
+        }
+        const bool seg = tape_mode >= 0 ? tape_mode == 1 : need <= free_b / 2;
+        for (int i = 0; i < n; i++)
+            if (int r = m[i]->adj_alloc(nsteps, ck, seg ? 1 : 0))
+                return set_berr(owner, r, "member %d: %s", i, m[i]->owner->err.c_str());
+        // every member's work on the batch stream for the run
+        std::vector<cudaStream_t> own(n);
+        for (int i = 0; i < n; i++) {
+            own[i] = m[i]->st;
+            m[i]->st = st;
+        }
+        int r = adjoint_packed_run(nsteps, ck, seg, seeds, out);
+        for (int i = 0; i < n; i++) {
+            m[i]->rec = nullptr;
+            m[i]->tape = nullptr;
+            m[i]->st = own[i];
+        }
+        adj_release();
+        return r;
+    }
+
+    int adjoint_packed_run(int nsteps, int ck, bool seg, const moist_adjoint_seed* seeds, moist_adjoint_grad* out) {
+        const int n = (int)m.size();
+        int r;
+        auto member_err = [&](int i, int rc) {
+            if (rc == MOIST_ERR_NAN) owner->nan_member = i;
+            return set_berr(owner, rc, "member %d: %s", i, m[i]->owner->err.c_str());
+        };
+        for (int i = 0; i < n; i++)
+            if ((r = m[i]->adj_seeds(seeds ? seeds + i : nullptr)) != MOIST_OK) return member_err(i, r);
+        // the recomputed (taped) forward steps and the reverse steps, per tape: with a tape per
+        // step of a segment, step j of a segment starts from the States of parity j % 2
+        const int ntapes = seg ? ck : 1;
+        std::vector<std::vector<Slot>> taped(ntapes), rev(ntapes);
+        for (int j = 0; j < ntapes; j++) {
+            std::vector<StepRecord> rf(n), ra(n);
+            const int pj = seg ? j % 2 : 0;
+            for (int i = 0; i < n; i++) {
+                m[i]->cur = pj == 0 ? cur0[i] : nxt0[i];
+                m[i]->nxt = pj == 0 ? nxt0[i] : cur0[i];
+                m[i]->tape = &m[i]->adj->tapes[j];
+                m[i]->rec = &rf[i];
+                r = m[i]->launch_step();
+                m[i]->tape = nullptr;
+                if (r == MOIST_OK) {
+                    m[i]->rec = &ra[i];
+                    r = m[i]->adj_step(m[i]->adj->tapes[j]);
+                }
+                m[i]->rec = nullptr;
+                if (r != MOIST_OK) return member_err(i, r);
+            }
+            if ((r = adj_pack(rf, taped[j])) != MOIST_OK) return r;
+            if ((r = adj_pack(ra, rev[j])) != MOIST_OK) return r;
+        }
+        for (int i = 0; i < n; i++) {  // back to the members' current States
+            m[i]->cur = parity == 0 ? cur0[i] : nxt0[i];
+            m[i]->nxt = parity == 0 ? nxt0[i] : cur0[i];
+        }
+        auto copy_to = [&](int i, const std::array<T*, 7>& src, const std::array<T*, 7>& dst) {
+            return m[i]->copyf(src.data(), dst.data(), 7);
+        };
+        // forward run through the step graphs, keeping the States every ck steps
+        const auto t0 = std::chrono::steady_clock::now();
+        for (int s = 0; s < nsteps; s++) {
+            if (s % ck == 0)
+                for (int i = 0; i < n; i++)
+                    if ((r = copy_to(i, m[i]->cur_fields(), m[i]->adj->ck[s / ck])) != MOIST_OK) return member_err(i, r);
+            if ((r = launch_steps(1)) != MOIST_OK) return r;
+        }
+        BCK(cudaStreamSynchronize(st));
+        const auto t1 = std::chrono::steady_clock::now();
+        for (int i = 0; i < n; i++)
+            if ((r = m[i]->adj_begin()) != MOIST_OK) return member_err(i, r);
+        // reverse sweep, one segment of ck steps at a time
+        const int nck = (nsteps + ck - 1) / ck;
+        for (int sg = nck - 1; sg >= 0; sg--) {
+            const int n0 = sg * ck, n1 = std::min(n0 + ck, nsteps);
+            at_parity0();
+            for (int i = 0; i < n; i++) {
+                if ((r = copy_to(i, m[i]->adj->ck[sg], m[i]->cur_fields())) != MOIST_OK) return member_err(i, r);
+                if (!seg && (r = copy_to(i, m[i]->adj->ck[sg], m[i]->adj->seg[0])) != MOIST_OK) return member_err(i, r);
+            }
+            if (seg) {  // recompute the segment once, taping every step
+                for (int s = n0; s < n1; s++) {
+                    if ((r = run_slots(taped[s - n0])) != MOIST_OK) return r;
+                    parity ^= 1;
+                    for (auto* c : m) std::swap(c->cur, c->nxt);
+                }
+                for (int s = n1 - 1; s >= n0; s--)
+                    if ((r = run_slots(rev[s - n0])) != MOIST_OK) return r;
+                continue;
+            }
+            for (int s = n0; s < n1 - 1; s++) {
+                if ((r = launch_steps(1)) != MOIST_OK) return r;
+                for (int i = 0; i < n; i++)
+                    if ((r = copy_to(i, m[i]->cur_fields(), m[i]->adj->seg[s - n0 + 1])) != MOIST_OK)
+                        return member_err(i, r);
+            }
+            for (int s = n1 - 1; s >= n0; s--) {
+                at_parity0();
+                for (int i = 0; i < n; i++)
+                    if ((r = copy_to(i, m[i]->adj->seg[s - n0], m[i]->cur_fields())) != MOIST_OK) return member_err(i, r);
+                if ((r = run_slots(taped[0])) != MOIST_OK) return r;
+                parity = 1;
+                for (auto* c : m) std::swap(c->cur, c->nxt);
+                if ((r = run_slots(rev[0])) != MOIST_OK) return r;
+            }
+        }
+        BCK(cudaStreamSynchronize(st));
+        const auto t2 = std::chrono::steady_clock::now();
+        const double fwd = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        const double rv = std::chrono::duration<double, std::milli>(t2 - t1).count();
+        for (int i = 0; i < n; i++)
+            if ((r = m[i]->adj_results(seeds ? seeds + i : nullptr, out + i, fwd, rv)) != MOIST_OK)
+                return member_err(i, r);
         return MOIST_OK;
     }
 
@@ -2052,6 +2448,8 @@ struct BatchImpl : BatchBase {
             BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSubAsync<T, TT, 2>), 2>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
             BCK(cudaFuncSetAttribute(k_batched<SINGLE_ARG(BSub<T, TT>), SINGLE_ARG(FSubAsync<T, TT, 3>), 2>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+            BCK(cudaFuncSetAttribute(k_batched_b<ASolve, FASubSolve, ADJ_SOLVE_THREADS, 1>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
         }
         for (int q = 0; q < 2; q++) {
@@ -2730,6 +3128,16 @@ int moist_tracer_pass_trace(moist_ctx* c, int nsteps, int maxrec, long long* pas
     if (!c || nsteps < 1 || maxrec < 0) return MOIST_ERR_ARG;
     CTX_DEVICE(c);
     return c->impl->pass_trace(nsteps, maxrec, pass_ns, pass_tiles, npasses);
+}
+
+int moist_set_adjoint_tapes(moist_ctx* c, int mode) {
+    if (!c || mode < -1 || mode > 1) return MOIST_ERR_ARG;
+    return c->impl->set_tape_mode(mode);
+}
+
+int moist_batch_set_adjoint_tapes(moist_batch* b, int mode) {
+    if (!b || mode < -1 || mode > 1) return MOIST_ERR_ARG;
+    return b->impl->set_tape_mode(mode);
 }
 
 int moist_set_wait_limit(moist_ctx* c, long long cycles) {

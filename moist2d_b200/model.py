@@ -113,6 +113,11 @@ class Model:
         _raise(lib().moist_autotune(self.ctx, int(nsteps), buf, len(buf)), self.ctx, "moist_autotune")
         return buf.value.decode()
 
+    def set_adjoint_tapes(self, mode):
+        """moist_set_adjoint_tapes: 1 a tape per step of a checkpoint segment, 0 one tape and
+        the segment's States, -1 (default) chosen from the free device memory."""
+        _raise(lib().moist_set_adjoint_tapes(self.ctx, int(mode)), self.ctx, "moist_set_adjoint_tapes")
+
     def adjoint(self, nsteps, ckpt_every=50, prec_weight=None, state_seed=None):
         """Advance the resident State nsteps large steps and return the gradient of
         J = sum(prec_weight * prec_final) + sum_f sum(state_seed[f] * S_final.f)
@@ -322,9 +327,11 @@ class Ensemble:
         return buf.value.decode()
 
     def adjoint(self, nsteps, ckpt_every=50, prec_weights=None, state_seeds=None, nthreads=0):
-        """moist_batch_adjoint_run: Model.adjoint for every member, run concurrently.
-        prec_weights / state_seeds: per-member lists (entries as for Model.adjoint) or None.
-        Returns one gradient dict per member; every member is left at its final State."""
+        """moist_batch_adjoint_run: Model.adjoint for every member. nthreads = 0: the members'
+        kernels run packed (one launch per kernel for all members); nthreads > 0: every member's
+        own moist_adjoint_run from that many host threads. prec_weights / state_seeds: per-member
+        lists (entries as for Model.adjoint) or None. Returns one gradient dict per member;
+        every member is left at its final State."""
         n = len(self.params)
         keep = []
 
@@ -358,6 +365,10 @@ class Ensemble:
             g.update(k_auto=o.k_auto, qc_threshold=o.qc_threshold, objective=o.objective,
                      forward_ms=o.forward_ms, reverse_ms=o.reverse_ms)
         return grads
+
+    def set_adjoint_tapes(self, mode):
+        """moist_batch_set_adjoint_tapes (modes as for Model.set_adjoint_tapes)."""
+        self._check(lib().moist_batch_set_adjoint_tapes(self.b, int(mode)), "moist_batch_set_adjoint_tapes")
 
     def budget(self, i):
         out = (C.c_double * 4)()

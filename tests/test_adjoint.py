@@ -123,9 +123,10 @@ def state_seeds(p, s, seed):
     return out
 
 
-def run_adjoint(p, s, nsteps, ckpt, prec_w, seeds, flags=0):
+def run_adjoint(p, s, nsteps, ckpt, prec_w, seeds, flags=0, tapes=-1):
     with model.Model(p, flags) as m:
         m.upload(s)
+        m.set_adjoint_tapes(tapes)
         g = m.adjoint(nsteps, ckpt, prec_weight=prec_w, state_seed=seeds)
         fin = s.copy()
         m.download(fin)
@@ -151,13 +152,15 @@ def test_adjoint_rain_objective_f64():
     fd_check(p, s, 12, prec_w, {}, g, ndir=3, seed=5, rtol=1e-3)
 
 
-def test_adjoint_checkpoint_interval_invariance():
+def test_adjoint_checkpoint_interval_and_tape_mode_invariance():
+    """The gradient does not depend on the checkpoint interval or on the tape mode (a tape per
+    step of a segment, or one tape and the segment's States)."""
     p, s = bubble_case(np.float64, nx=24, nz=16)
     prec_w = rain_weight(p)
     seeds = state_seeds(p, s, 3)
-    ref, _ = run_adjoint(p, s, 6, 6, prec_w, seeds)
-    for ck in (1, 4):
-        g, _ = run_adjoint(p, s, 6, ck, prec_w, seeds)
+    ref, _ = run_adjoint(p, s, 6, 6, prec_w, seeds, tapes=1)
+    for ck, tapes in ((1, 1), (4, 1), (4, 0), (6, 0)):
+        g, _ = run_adjoint(p, s, 6, ck, prec_w, seeds, tapes=tapes)
         for f in FIELDS:
             scale = np.max(np.abs(ref[f]))
             assert np.max(np.abs(g[f] - ref[f])) <= 1e-12 * scale, f

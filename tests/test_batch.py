@@ -103,11 +103,14 @@ def lib_step(ctx, n):
     return lib().moist_rk3_step(ctx, n)
 
 
+@pytest.mark.parametrize("nthreads,tapes", [(0, 1), (0, 0), (3, -1)], ids=["packed", "packed-one-tape", "threads"])
 @pytest.mark.parametrize("T", [np.float32, np.float64], ids=["f32", "f64"])
-def test_batch_adjoint_matches_single_adjoints(T):
+def test_batch_adjoint_matches_single_adjoints(T, nthreads, tapes):
     """moist_batch_adjoint_run gives every member the gradient of its own moist_adjoint_run
     (a context with the same streaming tracer sweep; the adjoint's atomic sums may round in a
-    different order) and leaves the members where the batch continues from."""
+    different order) and leaves the members where the batch continues from: with the members'
+    kernels packed (a tape per step of a segment, or one tape and the segment's States; 3 steps
+    in segments of 2 and 1) and with every member's own run from host threads."""
     mem = members(T)
     rng = np.random.default_rng(4)
     weights = []
@@ -119,7 +122,8 @@ def test_batch_adjoint_matches_single_adjoints(T):
     with model.Ensemble([p for p, _ in mem]) as e:
         for i, (_, s) in enumerate(mem):
             e.upload(i, s)
-        got = e.adjoint(3, 2, prec_weights=weights, state_seeds=seeds, nthreads=3)
+        e.set_adjoint_tapes(tapes)
+        got = e.adjoint(3, 2, prec_weights=weights, state_seeds=seeds, nthreads=nthreads)
         e.step(1)
         fin = [e.download(i, s.copy()) for i, (_, s) in enumerate(mem)]
     for i, (p, s) in enumerate(mem):
