@@ -167,9 +167,13 @@ int moist_nan_field(const moist_ctx* ctx);
 
 /* Copy a host State into the context (reference layout, halos included in the host arrays).
  * The library keeps interior columns; halo columns are re-derived periodically, as every
- * reference code path on the large step does before reading them. */
+ * reference code path on the large step does before reading them. Host arrays in page-locked,
+ * mapped memory (cudaHostAlloc, cudaHostRegister) are read in place by the layout kernels, the
+ * seven prognostic fields in one launch; pageable arrays go through a staging copy. */
 int moist_upload_state(moist_ctx* ctx, const moist_state_host* s);
-/* Copy the context State to host arrays; halo columns are written as periodic copies. */
+/* Copy the context State to host arrays; halo columns are written as periodic copies (the
+ * phys tendencies keep the caller's halo columns). Page-locked, mapped host arrays are written
+ * in place, as moist_upload_state reads them. */
 int moist_download_state(moist_ctx* ctx, moist_state_host* s);
 
 /* rk3_step!(s, p) applied nsteps times (moist.jl:1589-1683). */
@@ -178,7 +182,8 @@ int moist_rk3_step(moist_ctx* ctx, int nsteps);
 /* rk3_step!(s, p) on a host State, the reference's calling convention (moist.jl:1589): copy s
  * to the device, apply nsteps large steps, copy the State back into s. Equivalent to
  * moist_upload_state + moist_rk3_step + moist_download_state with one synchronisation. Host
- * arrays in page-locked memory let the copies run at full bus speed. */
+ * arrays in page-locked memory are read and written in place by the layout kernels over the
+ * bus, without staging copies. */
 int moist_rk3_step_host(moist_ctx* ctx, moist_state_host* s, int nsteps);
 
 /* compute_step!(d_rho_phys, d_rho_u_phys, d_rho_theta_phys, d_rho_qv_phys, d_rho_qc_phys,

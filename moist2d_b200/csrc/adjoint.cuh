@@ -262,48 +262,101 @@ __device__ __forceinline__ S gen_R_t(const DevParams<double>& p, int k, const G&
 //      U1 (k+1,i), U2 (k+2,i); 9-10 the linear-index clamp reads rho_q[1, 1] and rho_q[nz, 1]
 //      (row 0 and row nz-1 of reference column 1); 11-19 rho at the same nine positions;
 //  20-21 mom_flux_x (k,i) (k,i-1); 22-23 mom_flux_z (k,i) (k-1,i)
+// The update is q0 + dt (-(adv_x + adv_z) + (diff_x + diff_z) + dph): its x half (adv_x,
+// diff_x) reads the slots TR_X, its z half (adv_z, diff_z) the slots TR_Z; only C and rho_C
+// are in both.
+constexpr int TR_SLOTS = 24;
+constexpr int TR_NX = 12, TR_NZ = 14;
+__device__ constexpr int TR_X[TR_NX] = {0, 1, 2, 3, 4, 11, 12, 13, 14, 15, 20, 21};
+__device__ constexpr int TR_Z[TR_NZ] = {0, 5, 6, 7, 8, 9, 10, 11, 16, 17, 18, 19, 22, 23};
+
 template <class S, class G>
-__device__ __forceinline__ S gen_tracer(const DevParams<double>& p, int k, double q0, double dph, double dt_stage,
-                                        const G& v) {
-    const int nz = p.nz, ke = nz - 1;
-    const S EPS = p.EPS, dx = p.dx, dtb = p.dt;
-    const double* dz = p.dz;
-    const double* z = p.z;
+__device__ __forceinline__ void gen_tracer_x(const DevParams<double>& p, const G& v, S& adv_x, S& diff_x) {
+    const S EPS = p.EPS, dx = p.dx;
     const S s_c = v(0) / v(11);
     const S s_im1 = v(1) / v(12);
     const S s_im2 = v(2) / v(13);
     const S s_ip1 = v(3) / v(14);
     const S s_ip2 = v(4) / v(15);
+    const S fx_ip = limited_flux_x(v(20), s_im1, s_c, s_ip1, s_ip2, EPS);
+    const S fx_im = limited_flux_x(v(21), s_im2, s_im1, s_c, s_ip1, EPS);
+    adv_x = (fx_ip - fx_im) / dx;
+    const S r_c = v(11);
+    const S dsdx_ip = (v(14) + r_c) * S(0.5) * (s_ip1 - s_c) / dx;
+    const S dsdx_im = (r_c + v(12)) * S(0.5) * (s_c - s_im1) / dx;
+    diff_x = S(p.kappa) * (dsdx_ip - dsdx_im) / dx;
+}
+
+// limited_flux_z (model.cuh) with its clamp quotient formed only on the two faces that can
+// select it (kk = 0 upward, kk = nz-2 downward); the selected operations are the same
+template <class S>
+__device__ __forceinline__ S gen_flux_z(S vel, S s_m1, S s_0, S s_p1, S s_p2, int kk, int nz, S dz_k, S dz_kp1,
+                                        S lin_k, S lin_kp1, S dt_big, S EPS) {
+    const bool pos = vel > EPS, neg = vel < -EPS;
+    const S f2 = f2h(s_0, s_p1, dz_k, dz_kp1);
+    const bool use_clamp = (pos && kk == 0) || (!pos && neg && kk == nz - 2);
+    S face;
+    if (use_clamp) {
+        face = jmin(f2, (pos ? lin_k : lin_kp1) / (pos ? (vel * dt_big) : (-vel * dt_big)));
+    } else if (pos || neg) {
+        const S r_num = pos ? (s_p1 - s_0) : (s_0 - s_p1);
+        const S r_den = pos ? (s_0 - s_m1) : (s_p1 - s_p2);
+        const S q = r_num / r_den;
+        const S r = mm::mabs(r_den) < EPS ? S(1.0) : q;
+        const S half = S(0.5) * koren(r) * r_den;
+        face = pos ? (s_0 + half) : (s_p1 - half);
+    } else {
+        face = f2;
+    }
+    return face * vel;
+}
+
+template <class S, class G>
+__device__ __forceinline__ void gen_tracer_z(const DevParams<double>& p, int k, const G& v, S& adv_z, S& diff_z) {
+    const int nz = p.nz, ke = nz - 1;
+    const S EPS = p.EPS, dtb = p.dt;
+    const double* dz = p.dz;
+    const double* z = p.z;
+    const S s_c = v(0) / v(11);
     const S s_km1 = k >= 1 ? v(5) / v(16) : S(0.0);
     const S s_km2 = k >= 2 ? v(6) / v(17) : S(0.0);
     const S s_kp1 = k + 1 < nz ? v(7) / v(18) : S(0.0);
     const S s_kp2 = k + 2 < nz ? v(8) / v(19) : S(0.0);
-    const S one = S(1.0);  // clamp operand of faces that are not boundary faces (never selected)
-    const S fx_ip = limited_flux_x(v(20), s_im1, s_c, s_ip1, s_ip2, EPS);
-    const S fx_im = limited_flux_x(v(21), s_im2, s_im1, s_c, s_ip1, EPS);
-    const S adv_x = (fx_ip - fx_im) / dx;
     S fz_kp = S(0.0), fz_km = S(0.0);
     if (k < ke)
-        fz_kp = limited_flux_z(v(22), s_km1, s_c, s_kp1, s_kp2, k, nz, S(dz[k]), S(dz[k + 1]),
-                               k == 0 ? v(9) : one, k == nz - 2 ? v(10) : one, dtb, EPS);
+        fz_kp = gen_flux_z(v(22), s_km1, s_c, s_kp1, s_kp2, k, nz, S(dz[k]), S(dz[k + 1]), v(9), v(10), dtb, EPS);
     if (k > 0)
-        fz_km = limited_flux_z(v(23), s_km2, s_km1, s_c, s_kp1, k - 1, nz, S(dz[k - 1]), S(dz[k]),
-                               k - 1 == 0 ? v(9) : one, k - 1 == nz - 2 ? v(10) : one, dtb, EPS);
-    const S adv_z = (fz_kp - fz_km) / S(dz[k]);
-    const S advection = -(adv_x + adv_z);
+        fz_km = gen_flux_z(v(23), s_km2, s_km1, s_c, s_kp1, k - 1, nz, S(dz[k - 1]), S(dz[k]), v(9), v(10), dtb, EPS);
+    adv_z = (fz_kp - fz_km) / S(dz[k]);
     const S r_c = v(11);
     const S scalar_kp = k == ke ? S(0.0) : s_kp1;
     const S scalar_km = k == 0 ? S(0.0) : s_km1;
-    const S dsdx_ip = (v(14) + r_c) * S(0.5) * (s_ip1 - s_c) / dx;
-    const S dsdx_im = (r_c + v(12)) * S(0.5) * (s_c - s_im1) / dx;
-    const S diff_x = S(p.kappa) * (dsdx_ip - dsdx_im) / dx;
     const S dsdz_kp = k == ke ? S(0.0)
                               : f2h(v(18), r_c, S(dz[k + 1]), S(dz[k])) * (scalar_kp - s_c) / S(z[k + 1] - z[k]);
     const S dsdz_km = k == 0 ? S(0.0)
                              : f2h(r_c, v(16), S(dz[k]), S(dz[k - 1])) * (s_c - scalar_km) / S(z[k] - z[k - 1]);
-    const S diff_z = S(p.kappa) * (dsdz_kp - dsdz_km) / S(dz[k]);
-    const S diffusion = diff_x + diff_z;
-    return S(q0) + S(dt_stage) * (advection + diffusion + S(dph));
+    diff_z = S(p.kappa) * (dsdz_kp - dsdz_km) / S(dz[k]);
+}
+
+// Partial derivatives of the two outputs (a, b) of f with respect to the NS slots sl, N
+// directions per evaluation: emit(slot, da/dslot, db/dslot). f(get, a, b) evaluates the function;
+// get(s) returns slot s as a Dual<N> seeded in its direction of the pass (0 when not in it).
+template <int N, int NS, class F, class E>
+__device__ __forceinline__ void local_jacobian2(const double (&val)[TR_SLOTS], const int (&sl)[NS], F f, E emit) {
+#pragma unroll
+    for (int s0 = 0; s0 < NS; s0 += N) {
+        auto get = [&](int s) {
+            Dual<N> d(val[s]);
+#pragma unroll
+            for (int q = 0; q < N; q++) d.d[q] = (s0 + q < NS && sl[s0 + q] == s) ? 1.0 : 0.0;
+            return d;
+        };
+        Dual<N> a, b;
+        f(get, a, b);
+#pragma unroll
+        for (int q = 0; q < N; q++)
+            if (s0 + q < NS) emit(sl[s0 + q], a.d[q], b.d[q]);
+    }
 }
 
 // diagnostics pres, theta, rt2pres of one cell (moist.jl:1048-1062). Slots: rho, rho_theta,
@@ -446,8 +499,6 @@ __global__ void k_adj_update(const __grid_constant__ DevParams<double> p, const 
 
 // ----------------------------------------------------------------------------- tracer sweep
 
-constexpr int TR_SLOTS = 24;
-
 // the reads of tracer cell (k, i) from the sweep's stage-start ("old") and result ("new")
 // arrays: new values at (k, i-1), (k, i-2) unless they wrap around (periodic halo copies of the
 // stage start), new values below, old values at the cell, right and above
@@ -498,9 +549,31 @@ __device__ __forceinline__ void b_adj_tr_jac(const DevParams<double>& p, const A
     tracer_slots(p, a, t, k, i, v);
     const size_t fsz = (size_t)nz * P;
     double* Jt = J + (size_t)t * TR_SLOTS * fsz;
-    local_jacobian<ADJ_DUAL>(
-        v, [&](const auto& get) { return gen_tracer<Dual<ADJ_DUAL>>(p, k, 0.0, 0.0, a.dt_stage, get); },
-        [&](int s, double d) { Jt[(size_t)s * fsz + c] = d; });
+    // dq/dslot = dt (-(d adv_x + d adv_z) + (d diff_x + d diff_z)); slots C and rho_C take both
+    // halves, the others one
+    const double dt = a.dt_stage;
+    double ax_c = 0.0, dx_c = 0.0, ax_r = 0.0, dx_r = 0.0;
+    using D = Dual<ADJ_DUAL>;
+    local_jacobian2<ADJ_DUAL>(
+        v, TR_X, [&](const auto& get, D& ax, D& dfx) { gen_tracer_x<D>(p, get, ax, dfx); },
+        [&](int s, double ax, double dfx) {
+            if (s == 0) {
+                ax_c = ax;
+                dx_c = dfx;
+            } else if (s == 11) {
+                ax_r = ax;
+                dx_r = dfx;
+            } else {
+                Jt[(size_t)s * fsz + c] = dt * (-ax + dfx);
+            }
+        });
+    local_jacobian2<ADJ_DUAL>(
+        v, TR_Z, [&](const auto& get, D& az, D& dfz) { gen_tracer_z<D>(p, k, get, az, dfz); },
+        [&](int s, double az, double dfz) {
+            const double ax = s == 0 ? ax_c : (s == 11 ? ax_r : 0.0);
+            const double dfx = s == 0 ? dx_c : (s == 11 ? dx_r : 0.0);
+            Jt[(size_t)s * fsz + c] = dt * (-(ax + az) + (dfx + dfz));
+        });
 }
 template <class T>
 __global__ void __launch_bounds__(ADJ_THREADS) k_adj_tr_jac(const __grid_constant__ DevParams<double> p,

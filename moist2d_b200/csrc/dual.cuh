@@ -68,11 +68,30 @@ MM_HD Dual<N> operator*(const Dual<N>& a, const Dual<N>& b) {
     for (int j = 0; j < N; j++) r.d[j] = a.d[j] * b.v + a.v * b.d[j];
     return r;
 }
+// 1/b for the derivative part of a quotient. On the device: the hardware approximation refined
+// by two Newton-Raphson steps y <- y + y (1 - b y) (each squares the relative error, from about
+// 2^-22 to below the double rounding), for |b| in [2^-1000, 2^1000]; elsewhere, and on the
+// host, the IEEE quotient. The value part of every quotient stays the IEEE quotient.
+MM_HD double drcp(double b) {
+#ifdef __CUDA_ARCH__
+    const double ab = fabs(b);
+    if (ab >= 0x1p-1000 && ab <= 0x1p1000) {
+        double y;
+        asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+        double e = fma(-b, y, 1.0);
+        y = fma(y, e, y);
+        e = fma(-b, y, 1.0);
+        return fma(y, e, y);
+    }
+#endif
+    return 1.0 / b;
+}
+
 template <int N>
 MM_HD Dual<N> operator/(const Dual<N>& a, const Dual<N>& b) {
     Dual<N> r;
     const double q = a.v / b.v;
-    const double rb = 1.0 / b.v;
+    const double rb = drcp(b.v);
     r.v = q;
 #pragma unroll
     for (int j = 0; j < N; j++) r.d[j] = (a.d[j] - q * b.d[j]) * rb;

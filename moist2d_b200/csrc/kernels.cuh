@@ -1780,9 +1780,10 @@ __global__ void k_budget_final(const CSum* part, double* res) {
 
 // (ka, ia) column-major host layout <-> [nz][P] interior device layout, through a 32x32 tile
 template <class T>
-__global__ void k_from_ref(int nx, int nz, int halo, int P, const T* __restrict__ src, T* __restrict__ dst) {
+__device__ __forceinline__ void b_from_ref(int nx, int nz, int halo, int P, const T* __restrict__ src,
+                                           T* __restrict__ dst, int bx, int by) {
     __shared__ T tile[32][33];
-    const int k0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+    const int k0 = bx * 32, i0 = by * 32;
     const int ka = nz;
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
         const int i = i0 + r, k = k0 + threadIdx.x;
@@ -1794,13 +1795,18 @@ __global__ void k_from_ref(int nx, int nz, int halo, int P, const T* __restrict_
         if (i < nx && k < nz) dst[(size_t)k * P + i] = tile[threadIdx.x][r];
     }
 }
+template <class T>
+__global__ void k_from_ref(int nx, int nz, int halo, int P, const T* __restrict__ src, T* __restrict__ dst) {
+    b_from_ref(nx, nz, halo, P, src, dst, blockIdx.x, blockIdx.y);
+}
 
 template <class T>
-__global__ void k_to_ref(int nx, int nz, int halo, int P, const T* __restrict__ src, T* __restrict__ dst) {
+__device__ __forceinline__ void b_to_ref(int nx, int nz, int halo, int P, const T* __restrict__ src,
+                                         T* __restrict__ dst, int bx, int by) {
     __shared__ T tile[32][33];
-    const int k0 = blockIdx.x * 32;
+    const int k0 = bx * 32;
     const int ia = nx + 2 * halo;
-    const int j0 = blockIdx.y * 32;  // reference column index
+    const int j0 = by * 32;  // reference column index
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
         const int k = k0 + r, j = j0 + threadIdx.x;
         if (j < ia && k < nz) {
@@ -1814,6 +1820,27 @@ __global__ void k_to_ref(int nx, int nz, int halo, int P, const T* __restrict__ 
         const int j = j0 + r, k = k0 + threadIdx.x;
         if (j < ia && k < nz) dst[(size_t)j * nz + k] = tile[threadIdx.x][r];
     }
+}
+template <class T>
+__global__ void k_to_ref(int nx, int nz, int halo, int P, const T* __restrict__ src, T* __restrict__ dst) {
+    b_to_ref(nx, nz, halo, P, src, dst, blockIdx.x, blockIdx.y);
+}
+
+// Up to 7 fields moved in one launch (blockIdx.z = field): the State's layout moves when the
+// host arrays are page-locked and mapped, so that the kernel reads or writes them over the bus
+// directly, every field's transfer in flight at once, without a staging copy.
+template <class T>
+struct FieldSet {
+    const T* src[7];
+    T* dst[7];
+};
+template <class T>
+__global__ void k_from_ref_n(int nx, int nz, int halo, int P, FieldSet<T> f) {
+    b_from_ref(nx, nz, halo, P, f.src[blockIdx.z], f.dst[blockIdx.z], blockIdx.x, blockIdx.y);
+}
+template <class T>
+__global__ void k_to_ref_n(int nx, int nz, int halo, int P, FieldSet<T> f) {
+    b_to_ref(nx, nz, halo, P, f.src[blockIdx.z], f.dst[blockIdx.z], blockIdx.x, blockIdx.y);
 }
 
 }  // namespace moist

@@ -516,8 +516,65 @@ struct Ctx : CtxBase {
     }
 
     // ------------------------------------------------------------------ layout moves
+    // The device address of a host array the kernels can read and write directly (page-locked
+    // and mapped: cudaHostAlloc or cudaHostRegister memory under unified addressing), else null.
+    static void* mapped(const void* host) {
+        cudaPointerAttributes at;
+        if (!host || cudaPointerGetAttributes(&at, host) != cudaSuccess) {
+            cudaGetLastError();  // pageable memory may report an error on older runtimes: clear it
+            return nullptr;
+        }
+        return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
+    }
+
+    // the prognostic fields of a host State in one launch when every given array is mapped
+    // (done = false, and nothing moved, otherwise)
+    int put2d_mapped(const void* const host[7], T* const dev[7], bool& done) {
+        done = false;
+        FieldSet<T> fs{};
+        int nf = 0;
+        for (int j = 0; j < 7; j++) {
+            if (!host[j]) continue;
+            const void* hd = mapped(host[j]);
+            if (!hd) return MOIST_OK;
+            fs.src[nf] = (const T*)hd;
+            fs.dst[nf] = dev[j];
+            nf++;
+        }
+        if (nf == 0) return MOIST_OK;
+        k_from_ref_n<T><<<dim3(cdiv(nz, 32), cdiv(nx, 32), nf), dim3(32, 8), 0, st>>>(nx, nz, halo, P, fs);
+        CKL();
+        done = true;
+        return MOIST_OK;
+    }
+    int get2d_mapped(const T* const dev[7], void* const host[7], bool& done) {
+        done = false;
+        FieldSet<T> fs{};
+        int nf = 0;
+        for (int j = 0; j < 7; j++) {
+            if (!host[j]) continue;
+            void* hd = mapped(host[j]);
+            if (!hd) return MOIST_OK;
+            fs.src[nf] = dev[j];
+            fs.dst[nf] = (T*)hd;
+            nf++;
+        }
+        if (nf == 0) return MOIST_OK;
+        const int ia = nx + 2 * halo;
+        k_to_ref_n<T><<<dim3(cdiv(nz, 32), cdiv(ia, 32), nf), dim3(32, 8), 0, st>>>(nx, nz, halo, P, fs);
+        CKL();
+        done = true;
+        return MOIST_OK;
+    }
+
     int put2d(const void* host, T* dev) {
         if (!host) return MOIST_OK;
+        if (const void* hd = mapped(host)) {
+            dim3 b(32, 8), g(cdiv(nz, 32), cdiv(nx, 32));
+            k_from_ref<T><<<g, b, 0, st>>>(nx, nz, halo, P, (const T*)hd, dev);
+            CKL();
+            return MOIST_OK;
+        }
         const size_t n = (size_t)nz * (nx + 2 * halo);
         CK(cudaMemcpyAsync(staging, host, n * sizeof(T), cudaMemcpyHostToDevice, st));
         dim3 b(32, 8), g(cdiv(nz, 32), cdiv(nx, 32));
@@ -529,6 +586,15 @@ struct Ctx : CtxBase {
         if (!host) return MOIST_OK;
         const int ia = nx + 2 * halo;
         const size_t n = (size_t)nz * ia;
+        if (void* hd = mapped(host)) {  // written in place: the caller's halo columns stay as they are
+            dim3 b(32, 8), g(cdiv(nz, 32), cdiv(halos ? ia : nx, 32));
+            if (halos)
+                k_to_ref<T><<<g, b, 0, st>>>(nx, nz, halo, P, dev, (T*)hd);
+            else
+                k_to_ref<T><<<g, b, 0, st>>>(nx, nz, 0, P, dev, (T*)hd + (size_t)halo * nz);
+            CKL();
+            return MOIST_OK;
+        }
         if (!halos) {  // keep the caller's halo columns: start from their current values
             CK(cudaMemcpyAsync(staging, host, n * sizeof(T), cudaMemcpyHostToDevice, st));
         }
@@ -568,7 +634,9 @@ struct Ctx : CtxBase {
         StateP<T>& d = cur;
         const void* f2[7] = {s->rho, s->rho_u, s->rho_w, s->rho_theta, s->rho_qv, s->rho_qc, s->rho_qr};
         T* dv[7] = {d.rho, d.ru, d.rw, d.rt, d.qv, d.qc, d.qr};
-        for (int j = 0; j < 7; j++)
+        bool done = false;
+        if ((r = put2d_mapped(f2, dv, done)) != MOIST_OK) return r;
+        for (int j = 0; j < 7 && !done; j++)
             if ((r = put2d(f2[j], dv[j])) != MOIST_OK) return r;
         const void* g2[6] = {s->d_rho_theta_mp, s->d_rho_qv_mp, s->d_rho_qc_mp, s->d_rho_qr_mp, s->d_rho_qr_sed,
                              s->d_rho_theta_rd};
@@ -599,10 +667,12 @@ struct Ctx : CtxBase {
 
     int queue_download(moist_state_host* s) {
         int r;
-        const void* f2[7] = {s->rho, s->rho_u, s->rho_w, s->rho_theta, s->rho_qv, s->rho_qc, s->rho_qr};
-        T* dv[7] = {cur.rho, cur.ru, cur.rw, cur.rt, cur.qv, cur.qc, cur.qr};
-        for (int j = 0; j < 7; j++) {
-            if ((r = get2d(dv[j], const_cast<void*>(f2[j]), true)) != MOIST_OK) return r;
+        void* f2[7] = {s->rho, s->rho_u, s->rho_w, s->rho_theta, s->rho_qv, s->rho_qc, s->rho_qr};
+        const T* dv[7] = {cur.rho, cur.ru, cur.rw, cur.rt, cur.qv, cur.qc, cur.qr};
+        bool done = false;
+        if ((r = get2d_mapped(dv, f2, done)) != MOIST_OK) return r;
+        for (int j = 0; j < 7 && !done; j++) {
+            if ((r = get2d(dv[j], f2[j], true)) != MOIST_OK) return r;
         }
         void* g2[6] = {s->d_rho_theta_mp, s->d_rho_qv_mp, s->d_rho_qc_mp, s->d_rho_qr_mp, s->d_rho_qr_sed,
                        s->d_rho_theta_rd};
@@ -2121,7 +2191,12 @@ struct BatchImpl : BatchBase {
     case KIND:                                                                                         \
         k_batched_b<A, F, MAXT, 1><<<s.nitems, s.block, s.smem, ls>>>(s.items, (const A*)s.args, F{}); \
         break;
-            BATCH_LAUNCH_B(AK_TR_JAC, ATrJac<T>, FATrJac<T>, ADJ_THREADS)
+#define BATCH_LAUNCH_B3(KIND, A, F, MAXT)                                                              \
+    case KIND:                                                                                         \
+        k_batched_b<A, F, MAXT, 3><<<s.nitems, s.block, s.smem, ls>>>(s.items, (const A*)s.args, F{}); \
+        break;
+            BATCH_LAUNCH_B3(AK_TR_JAC, ATrJac<T>, FATrJac<T>, ADJ_THREADS)  // registers for 3 blocks per SM
+#undef BATCH_LAUNCH_B3
             BATCH_LAUNCH_B(AK_SUB_SOLVE, ASolve, FASubSolve, ADJ_SOLVE_THREADS)
             BATCH_LAUNCH_B(AK_TEND_T, AStage<T>, FATendT<T>, ADJ_THREADS)
             BATCH_LAUNCH_B(AK_DIAG_T, AStage<T>, FADiagT<T>, ADJ_THREADS)
