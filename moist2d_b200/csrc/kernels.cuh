@@ -1213,20 +1213,22 @@ constexpr int STRIP_THREADS = 256;
 template <class T, class TT>
 __host__ __device__ inline size_t strip_smem_bytes(int nz, int wc) {
     const size_t n = (size_t)(nz - 1) * wc;
-    return 3 * n * sizeof(TT) + (2 * n + 2 * (size_t)nz * wc + (size_t)nz * (wc + 1)) * sizeof(T);
+    return 5 * n * sizeof(TT) + (2 * n + 2 * (size_t)nz * wc + (size_t)nz * (wc + 1)) * sizeof(T);
 }
 
 template <class T, class TT>
 struct StripSmem {
-    TT *D, *piv, *cp;      // [n][wc]: right-hand side then d', pivots, modified super-diagonal
-    T *a, *w;              // [n][wc]: sub-diagonal, new rho_w_p
-    T *rho_tp, *rt_tp;     // [nz][wc]: off-centred rho_p, rho_theta_p
-    T* u;                  // [nz][wc+1]: rho_u_p at faces i0-1/2 .. i0+wc-1/2
+    TT *D, *Dp, *piv, *rp, *cp;  // [n][wc]: right-hand side, d', pivots, 1/pivots, modified super-diagonal
+    T *a, *w;                    // [n][wc]: sub-diagonal, new rho_w_p
+    T *rho_tp, *rt_tp;           // [nz][wc]: off-centred rho_p, rho_theta_p
+    T* u;                        // [nz][wc+1]: rho_u_p at faces i0-1/2 .. i0+wc-1/2
     __device__ StripSmem(unsigned char* base, int nz, int wc) {
         const size_t n = (size_t)(nz - 1) * wc;
         D = (TT*)base;
-        piv = D + n;
-        cp = piv + n;
+        Dp = D + n;
+        piv = Dp + n;
+        rp = piv + n;
+        cp = rp + n;
         a = (T*)(cp + n);
         w = a + n;
         rho_tp = w + n;
@@ -1377,25 +1379,69 @@ __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a
         if (j < n - 1) d -= ro(a.tc + cj) * fact * a.rw_p[c];
         sm.D[j * wc + col] = (TT)d;
         sm.a[j * wc + col] = aj;
-        sm.piv[j * wc + col] = ro(a.tpiv + cj);
+        const TT pv = ro(a.tpiv + cj);
+        sm.piv[j * wc + col] = pv;
+        if constexpr (sizeof(TT) == 8) sm.rp[j * wc + col] = (TT)1 / pv;  // for the checked quotients of (4)
         sm.cp[j * wc + col] = ro(a.tcp + cj);
     }
     __syncthreads();
-    // (4) Thomas elimination per column (moist.jl:956-970)
+    // (4) Thomas elimination per column (moist.jl:956-970). The loops read the next level's
+    // operands one level ahead (clamped at the ends), unrolled so that the loads leave the
+    // dependent path.
     if (tid < ncol) {
         const int cc = tid;
-        TT dprev = sm.D[cc] / sm.piv[cc];
-        sm.D[cc] = dprev;
-        for (int j = 1; j < n; j++) {
-            const TT dp = (sm.D[j * wc + cc] - (TT)sm.a[j * wc + cc] * dprev) / sm.piv[j * wc + cc];
-            sm.D[j * wc + cc] = dp;
-            dprev = dp;
+        const TT* __restrict__ sD = sm.D;
+        const T* __restrict__ sa = sm.a;
+        const TT* __restrict__ sp = sm.piv;
+        TT* __restrict__ sDp = sm.Dp;
+        TT dprev = (TT)0;
+        bool ok = sizeof(TT) == 8;
+        if constexpr (sizeof(TT) == 8) {
+            // d'_j = (d_j - a_j d'_{j-1}) / piv_j with each quotient formed from 1/piv_j (divided in
+            // (3) by all threads) and checked exact (qdiv_checked, fastdiv.cuh): 68 instead of 171
+            // cycles per level. A column with any unproven quotient is eliminated again with IEEE
+            // division below (the right-hand sides stay in D).
+            const TT* __restrict__ sr = sm.rp;
+            dprev = qdiv_checked(sD[cc], sp[cc], sr[cc], ok);
+            sDp[cc] = dprev;
+            const int j1 = n > 1 ? 1 : 0;
+            TT dn = sD[j1 * wc + cc], an = (TT)sa[j1 * wc + cc], pn = sp[j1 * wc + cc], yn = sr[j1 * wc + cc];
+#pragma unroll 4
+            for (int j = 1; j < n; j++) {
+                const TT dj = dn, aj = an, pj = pn, yj = yn;
+                const int jn = j + 1 < n ? j + 1 : n - 1;
+                dn = sD[jn * wc + cc];
+                an = (TT)sa[jn * wc + cc];
+                pn = sp[jn * wc + cc];
+                yn = sr[jn * wc + cc];
+                dprev = qdiv_checked(dj - aj * dprev, pj, yj, ok);
+                sDp[j * wc + cc] = dprev;
+            }
         }
+        if (!ok) {
+            dprev = sD[cc] / sp[cc];
+            sDp[cc] = dprev;
+            for (int j = 1; j < n; j++) {
+                const TT dp = (sD[j * wc + cc] - (TT)sa[j * wc + cc] * dprev) / sp[j * wc + cc];
+                sDp[j * wc + cc] = dp;
+                dprev = dp;
+            }
+        }
+        // back substitution x_j = d'_j - c'_j x_{j+1}: 43 instead of 64 cycles per level
+        const TT* __restrict__ sc = sm.cp;
+        T* __restrict__ sw = sm.w;
         TT x = dprev;
-        sm.w[(n - 1) * wc + cc] = (T)x;
+        sw[(n - 1) * wc + cc] = (T)x;
+        const int jb = n >= 2 ? n - 2 : 0;
+        TT dpn = sDp[jb * wc + cc], cpn = sc[jb * wc + cc];
+#pragma unroll 4
         for (int j = n - 2; j >= 0; j--) {
-            x = sm.D[j * wc + cc] - sm.cp[j * wc + cc] * x;
-            sm.w[j * wc + cc] = (T)x;
+            const TT dpj = dpn, cpj = cpn;
+            const int jn = j >= 1 ? j - 1 : 0;
+            dpn = sDp[jn * wc + cc];
+            cpn = sc[jn * wc + cc];
+            x = dpj - cpj * x;
+            sw[j * wc + cc] = (T)x;
         }
     }
     __syncthreads();
