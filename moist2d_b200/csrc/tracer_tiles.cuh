@@ -291,6 +291,34 @@ struct TileSmem {
     T cl[3][2][2][TT_W];     // per tracer: clamp quotients of the vertical limiter [kp, km][low, high row][column]
 };
 
+// the staging loops of k_tracer_tiles: every thread loads TT_BATCH elements (load(j) returns
+// an element's values), then stores them (store(j, v)); elements j = threadIdx.x + u blockDim.x
+constexpr int TT_BATCH = 8;
+template <class T>
+struct Pair {
+    T x, y;
+};
+template <class T>
+struct Triple {
+    T x, y, z;
+};
+template <class V, class L, class S>
+__device__ __forceinline__ void stage_batched(int total, L load, S store) {
+    for (int j0 = threadIdx.x; j0 < total; j0 += TT_BATCH * (int)blockDim.x) {
+        V v[TT_BATCH];
+#pragma unroll
+        for (int u = 0; u < TT_BATCH; u++) {
+            const int j = j0 + u * (int)blockDim.x;
+            if (j < total) v[u] = load(j);
+        }
+#pragma unroll
+        for (int u = 0; u < TT_BATCH; u++) {
+            const int j = j0 + u * (int)blockDim.x;
+            if (j < total) store(j, v[u]);
+        }
+    }
+}
+
 // strips in global memory: [parity][tracer][tile][4][32]
 template <class T>
 __device__ __forceinline__ T* strip_ptr(T* strips, int parity, int t, int tile, int ntiles) {
@@ -331,49 +359,63 @@ __global__ void __launch_bounds__(96) k_tracer_tiles(DevParams<T> p, TracerArgs<
     const unsigned nblocks = gridDim.x;
     const bool halt = halted(err);  // uniform across the grid: every block still meets every barrier
 
-    // ---- stage the stage-start values this tile reads (coalesced rows)
-    for (int j = threadIdx.x; j < TT_S * TT_S; j += blockDim.x) {
+    // ---- stage the stage-start values this tile reads (coalesced rows). Each thread issues the
+    // loads of TT_BATCH elements before it stores (or divides) any, so that it waits for one
+    // memory round trip per batch rather than per element.
+    stage_batched<T>(TT_S * TT_S, [&](int j) {
         const int rr = j / TT_S, cc = j % TT_S;
         const int k = z0 - 1 + rr, i = wrapx(x0 - 1 + cc, nx);
         // columns beyond nx+1 are never read; the bound also keeps wrapx within one period
-        sm.rho[rr][cc] = (k >= 0 && k < nz && x0 - 1 + cc < nx + 2) ? a.rho[MOIST_IDX(k, i)] : T(1);
-    }
-    for (int j = threadIdx.x; j < TT_W * (TT_W + 1); j += blockDim.x) {
+        return (k >= 0 && k < nz && x0 - 1 + cc < nx + 2) ? a.rho[MOIST_IDX(k, i)] : T(1);
+    }, [&](int j, T v) { sm.rho[j / TT_S][j % TT_S] = v; });
+    stage_batched<T>(TT_W * (TT_W + 1), [&](int j) {
         const int rr = j / (TT_W + 1), cc = j % (TT_W + 1);
         const int k = z0 + rr, i = wrapx(x0 - 1 + cc, nx);
         // faces x0-1 .. nx-1 only: face i-1 and i of the cells i < nx
-        sm.mx[rr][cc] = (k < nz && x0 - 1 + cc < nx) ? a.mfx[MOIST_IDX(k, i)] : T(0);
-    }
-    for (int j = threadIdx.x; j < (TT_W + 1) * TT_W; j += blockDim.x) {
+        return (k < nz && x0 - 1 + cc < nx) ? a.mfx[MOIST_IDX(k, i)] : T(0);
+    }, [&](int j, T v) { sm.mx[j / (TT_W + 1)][j % (TT_W + 1)] = v; });
+    stage_batched<T>((TT_W + 1) * TT_W, [&](int j) {
         const int rr = j / TT_W, cc = j % TT_W;
         const int k = z0 - 1 + rr, i = x0 + cc;
-        sm.mz[rr][cc] = (k >= 0 && k < nz && i < nx) ? a.mfz[MOIST_IDX(k, i)] : T(0);
-    }
+        return (k >= 0 && k < nz && i < nx) ? a.mfz[MOIST_IDX(k, i)] : T(0);
+    }, [&](int j, T v) { sm.mz[j / TT_W][j % TT_W] = v; });
     for (int t = 0; t < 3; t++) {
         const T* qo = a.q_old[t];
-        for (int j = threadIdx.x; j < TT_S * TT_S; j += blockDim.x) {
+        // s = rho_q / rho, the quotient formed after the batch's loads
+        stage_batched<Pair<T>>(TT_S * TT_S, [&](int j) {
             const int rr = j / TT_S, cc = j % TT_S;
             const int k = z0 + rr, i = wrapx(x0 + cc, nx);
-            T v = T(0);
+            Pair<T> v{T(0), T(1)};
             if (k < nz && x0 + cc < nx + 2) {
                 const size_t c = MOIST_IDX(k, i);
-                v = qo[c] / a.rho[c];
+                v.x = qo[c];
+                v.y = a.rho[c];
             }
-            sm.s[t][rr][cc] = v;
-        }
+            return v;
+        }, [&](int j, Pair<T> v) { sm.s[t][j / TT_S][j % TT_S] = v.x / v.y; });
         for (int j = threadIdx.x; j < TT_S + 1; j += blockDim.x) {
             const int k = z0 - 1 + j;
             sm.lin[t][j] = (k >= 0 && k < nz) ? qo[MOIST_IDX(k, nx - 2)] : T(0);
         }
         if constexpr (kStageQ<T>) {
-            for (int j = threadIdx.x; j < TT_W * TT_W; j += blockDim.x) {
+            stage_batched<Triple<T>>(TT_W * TT_W, [&](int j) {
                 const int rr = j / TT_W, cc = j % TT_W;
                 const int k = z0 + rr, i = x0 + cc;
                 const bool ok = k < nz && i < nx;
-                sm.q.q0[t][rr][cc] = ok ? a.q0[t][MOIST_IDX(k, i)] : T(0);
-                sm.q.dph[t][rr][cc] = ok ? a.dphys[t][MOIST_IDX(k, i)] : T(0);
-                if (t == 0) sm.q.rrho[rr][cc] = FastDiv::rcp(ok ? a.rho[MOIST_IDX(k, i)] : T(1));
-            }
+                Triple<T> v{T(0), T(0), T(1)};
+                if (ok) {
+                    const size_t c = MOIST_IDX(k, i);
+                    v.x = a.q0[t][c];
+                    v.y = a.dphys[t][c];
+                    if (t == 0) v.z = a.rho[c];
+                }
+                return v;
+            }, [&](int j, Triple<T> v) {
+                const int rr = j / TT_W, cc = j % TT_W;
+                sm.q.q0[t][rr][cc] = v.x;
+                sm.q.dph[t][rr][cc] = v.y;
+                if (t == 0) sm.q.rrho[rr][cc] = FastDiv::rcp(v.z);
+            });
         }
     }
     __syncthreads();
