@@ -1216,6 +1216,33 @@ __host__ __device__ inline size_t strip_smem_bytes(int nz, int wc) {
     return 5 * n * sizeof(TT) + (2 * n + 2 * (size_t)nz * wc + (size_t)nz * (wc + 1)) * sizeof(T);
 }
 
+// A loop whose iterations load from global memory and then compute, in batches: every thread
+// loads the operands of SUB_BATCH iterations (load(e) returns them) before computing any
+// (work(e, v)), so that it waits for one memory round trip per batch instead of one per
+// iteration; a division in the computation ends the compiler's scheduling region, so it would
+// not move the next iteration's loads above it.
+constexpr int SUB_BATCH = 4;
+template <class V, class L, class W>
+__device__ __forceinline__ void batched_loop(int first, int end, int stride, L load, W work) {
+    for (int b0 = first; b0 < end; b0 += SUB_BATCH * stride) {
+        V v[SUB_BATCH];
+#pragma unroll
+        for (int u = 0; u < SUB_BATCH; u++) {
+            const int e = b0 + u * stride;
+            if (e < end) v[u] = load(e);
+        }
+#pragma unroll
+        for (int u = 0; u < SUB_BATCH; u++) {
+            const int e = b0 + u * stride;
+            if (e < end) work(e, v[u]);
+        }
+    }
+}
+template <class T, int N>
+struct Vals {
+    T v[N];
+};
+
 template <class T, class TT>
 struct StripSmem {
     TT *D, *Dp, *piv, *rp, *cp;  // [n][wc]: right-hand side, d', pivots, 1/pivots, modified super-diagonal
@@ -1323,17 +1350,23 @@ __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a
     // (1) horizontal forward step of rho_u_p at the ncol + 1 faces (1355-1366)
     {
         const int nf = ncol + 1, wf = wc + 1;
-        #pragma unroll 4
-        for (int e = tid; e < nz * nf; e += STRIP_THREADS) {
-            const int k = e / nf, f = e - k * nf;
-            const int cc = wrapx(i0 + f - 1, nx), cn = wrapx(cc + 1, nx);
-            const size_t a0 = MOIST_IDX(k, cc), a1 = MOIST_IDX(k, cn);
-            T grad_x = (ro(a.rt_in + a1) - ro(a.rt_in + a0)) / dx;
-            const T grad_x_old = (ro(a.rt_old + a1) - ro(a.rt_old + a0)) / dx;
-            grad_x = grad_x + p.gamma_d * (grad_x - grad_x_old);
-            const T rt2pres_h = (ro(a.rt2pres + a0) + ro(a.rt2pres + a1)) * T(0.5);
-            sm.u[k * wf + f] = ro(a.ru_in + a0) + dt_s * (ro(a.R_ru + a0) - rt2pres_h * grad_x);
-        }
+        batched_loop<Vals<T, 8>>(
+            tid, nz * nf, STRIP_THREADS,
+            [&](int e) {
+                const int k = e / nf, f = e - k * nf;
+                const int cc = wrapx(i0 + f - 1, nx), cn = wrapx(cc + 1, nx);
+                const size_t a0 = MOIST_IDX(k, cc), a1 = MOIST_IDX(k, cn);
+                return Vals<T, 8>{{ro(a.rt_in + a0), ro(a.rt_in + a1), ro(a.rt_old + a0), ro(a.rt_old + a1),
+                                   ro(a.rt2pres + a0), ro(a.rt2pres + a1), ro(a.ru_in + a0), ro(a.R_ru + a0)}};
+            },
+            [&](int e, const Vals<T, 8>& v) {
+                const int k = e / nf, f = e - k * nf;
+                T grad_x = (v.v[1] - v.v[0]) / dx;
+                const T grad_x_old = (v.v[3] - v.v[2]) / dx;
+                grad_x = grad_x + p.gamma_d * (grad_x - grad_x_old);
+                const T rt2pres_h = (v.v[4] + v.v[5]) * T(0.5);
+                sm.u[k * wf + f] = v.v[6] + dt_s * (v.v[7] - rt2pres_h * grad_x);
+            });
     }
     __syncthreads();
     const int col = tid % wc, r0 = tid / wc, rs = STRIP_THREADS / wc;
@@ -1341,49 +1374,63 @@ __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a
     const int i = i0 + col;
     const int im = wrapx(i - 1, nx), ip = wrapx(i + 1, nx);
     // (2) explicit rho_p, rho_theta_p and their off-centred values (1367-1396)
-    #pragma unroll 4
-    for (int k = r0; k < nz && own; k += rs) {
-        const size_t c = MOIST_IDX(k, i);
-        const T u_m = sm.u[k * (wc + 1) + col], u_p = sm.u[k * (wc + 1) + col + 1];
-        a.ru_out[c] = u_p;
-        a.mfx[c] = a.mfx[c] + u_p / ns_T;
-        T advection = -(u_p - u_m) / dx;
-        T inc = dt_s * (ro(a.R_rho + c) + advection);
-        const T rho_old = a.rho_p[c];
-        sm.rho_tp[k * wc + col] = (T)((double)rho_old + fact_tp64 * (double)inc);
-        a.rho_p[c] = rho_old + inc;
-        const T th_i = ro(a.theta + c), th_ip = ro(a.theta + MOIST_IDX(k, ip)), th_im = ro(a.theta + MOIST_IDX(k, im));
-        const T flux_ip = (th_ip + th_i) * T(0.5) * u_p;
-        const T flux_im = (th_i + th_im) * T(0.5) * u_m;
-        advection = -(flux_ip - flux_im) / dx;
-        inc = dt_s * (ro(a.R_rt + c) + advection);
-        const T rtp = ro(a.rt_in + c);
-        sm.rt_tp[k * wc + col] = (T)((double)rtp + fact_tp64 * (double)inc);
-        a.rt_out[c] = rtp + inc;
-    }
+    batched_loop<Vals<T, 8>>(
+        r0, own ? nz : 0, rs,
+        [&](int k) {
+            const size_t c = MOIST_IDX(k, i);
+            return Vals<T, 8>{{a.mfx[c], ro(a.R_rho + c), a.rho_p[c], ro(a.theta + c), ro(a.theta + MOIST_IDX(k, ip)),
+                               ro(a.theta + MOIST_IDX(k, im)), ro(a.R_rt + c), ro(a.rt_in + c)}};
+        },
+        [&](int k, const Vals<T, 8>& v) {
+            const size_t c = MOIST_IDX(k, i);
+            const T u_m = sm.u[k * (wc + 1) + col], u_p = sm.u[k * (wc + 1) + col + 1];
+            a.ru_out[c] = u_p;
+            a.mfx[c] = v.v[0] + u_p / ns_T;
+            T advection = -(u_p - u_m) / dx;
+            T inc = dt_s * (v.v[1] + advection);
+            const T rho_old = v.v[2];
+            sm.rho_tp[k * wc + col] = (T)((double)rho_old + fact_tp64 * (double)inc);
+            a.rho_p[c] = rho_old + inc;
+            const T th_i = v.v[3], th_ip = v.v[4], th_im = v.v[5];
+            const T flux_ip = (th_ip + th_i) * T(0.5) * u_p;
+            const T flux_im = (th_i + th_im) * T(0.5) * u_m;
+            advection = -(flux_ip - flux_im) / dx;
+            inc = dt_s * (v.v[6] + advection);
+            const T rtp = v.v[7];
+            sm.rt_tp[k * wc + col] = (T)((double)rtp + fact_tp64 * (double)inc);
+            a.rt_out[c] = rtp + inc;
+        });
     __syncthreads();
     // (3) right-hand side of the w-p system (1397-1408) and the stage factors
-    #pragma unroll 4
-    for (int j = r0; j < n && own; j += rs) {
-        const int k = j + 1;
-        const size_t c = MOIST_IDX(k, i), cj = c - P;
-        const T buoyancy = (sm.rt_tp[k * wc + col] - sm.rt_tp[j * wc + col]) / (z[k] - z[j]);
-        const T grav = -p.GRAV * T(0.5) * (sm.rho_tp[k * wc + col] + sm.rho_tp[j * wc + col]);
-        const T rt2pres_h = (ro(a.rt2pres + cj) + ro(a.rt2pres + c)) * T(0.5);
-        const T drho_w = dt_s * (ro(a.R_rw + cj) - rt2pres_h * buoyancy + grav);
-        const T w_j = a.rw_p[cj];
-        const T aj = ro(a.ta + cj);
-        T d = w_j + drho_w;
-        if (j > 0) d -= aj * fact * w_j;
-        d -= ro(a.tb + cj) * fact * w_j;
-        if (j < n - 1) d -= ro(a.tc + cj) * fact * a.rw_p[c];
-        sm.D[j * wc + col] = (TT)d;
-        sm.a[j * wc + col] = aj;
-        const TT pv = ro(a.tpiv + cj);
-        sm.piv[j * wc + col] = pv;
-        if constexpr (sizeof(TT) == 8) sm.rp[j * wc + col] = (TT)1 / pv;  // for the checked quotients of (4)
-        sm.cp[j * wc + col] = ro(a.tcp + cj);
-    }
+    struct RhsIn {
+        T r2j, r2k, rrw, wj, wk, ta, tb, tc;
+        TT piv, cp;
+    };
+    batched_loop<RhsIn>(
+        r0, own ? n : 0, rs,
+        [&](int j) {
+            const size_t c = MOIST_IDX(j + 1, i), cj = c - P;
+            return RhsIn{ro(a.rt2pres + cj), ro(a.rt2pres + c), ro(a.R_rw + cj), a.rw_p[cj], a.rw_p[c],
+                         ro(a.ta + cj),      ro(a.tb + cj),      ro(a.tc + cj),   ro(a.tpiv + cj), ro(a.tcp + cj)};
+        },
+        [&](int j, const RhsIn& v) {
+            const int k = j + 1;
+            const T buoyancy = (sm.rt_tp[k * wc + col] - sm.rt_tp[j * wc + col]) / (z[k] - z[j]);
+            const T grav = -p.GRAV * T(0.5) * (sm.rho_tp[k * wc + col] + sm.rho_tp[j * wc + col]);
+            const T rt2pres_h = (v.r2j + v.r2k) * T(0.5);
+            const T drho_w = dt_s * (v.rrw - rt2pres_h * buoyancy + grav);
+            const T w_j = v.wj;
+            const T aj = v.ta;
+            T d = w_j + drho_w;
+            if (j > 0) d -= aj * fact * w_j;
+            d -= v.tb * fact * w_j;
+            if (j < n - 1) d -= v.tc * fact * v.wk;
+            sm.D[j * wc + col] = (TT)d;
+            sm.a[j * wc + col] = aj;
+            sm.piv[j * wc + col] = v.piv;
+            if constexpr (sizeof(TT) == 8) sm.rp[j * wc + col] = (TT)1 / v.piv;  // for the checked quotients of (4)
+            sm.cp[j * wc + col] = v.cp;
+        });
     __syncthreads();
     // (4) Thomas elimination per column (moist.jl:956-970). The loops read the next level's
     // operands one level ahead (clamped at the ends), unrolled so that the loads leave the
@@ -1446,47 +1493,57 @@ __device__ __forceinline__ void b_substep_strip(DevParams<T> p, SubArgs<T, TT> a
     }
     __syncthreads();
     // (5) vertical rho_p, rho_theta_p updates (1412-1446), momentum flux averages (1452-1458)
+    // every value a branch may read is loaded, in bounds, before the branches select
     const T* th = a.theta;
-    #pragma unroll 4
-    for (int k = r0; k < nz && own; k += rs) {
-        const size_t c = MOIST_IDX(k, i);
-        const T w_k = k < ke ? sm.w[k * wc + col] : T(0.0);
-        const T w_km = k > 0 ? sm.w[(k - 1) * wc + col] : T(0.0);
-        if (k < ke) a.rw_p[c] = w_k;
-        {
-            const T flux_kp = k == ke ? T(0.0) : w_k;
-            const T flux_km = k == 0 ? T(0.0) : w_km;
+    batched_loop<Vals<T, 10>>(
+        r0, own ? nz : 0, rs,
+        [&](int k) {
+            const size_t c = MOIST_IDX(k, i);
+            return Vals<T, 10>{{a.rho_p[c], a.rt_out[c], k < ke ? a.mfz[c] : T(0), ro(a.s_rw + c),
+                                k > 0 ? ro(a.s_rw + c - P) : T(0), k >= 2 ? ro(th + c - 2 * P) : T(0),
+                                k >= 1 ? ro(th + c - P) : T(0), ro(th + c), k + 1 <= ke ? ro(th + c + P) : T(0),
+                                k + 2 <= ke ? ro(th + c + 2 * P) : T(0)}};
+        },
+        [&](int k, const Vals<T, 10>& v) {
+            const size_t c = MOIST_IDX(k, i);
+            const T th_m2 = v.v[5], th_m1 = v.v[6], th_0 = v.v[7], th_p1 = v.v[8], th_p2 = v.v[9];
+            const T w_k = k < ke ? sm.w[k * wc + col] : T(0.0);
+            const T w_km = k > 0 ? sm.w[(k - 1) * wc + col] : T(0.0);
+            if (k < ke) a.rw_p[c] = w_k;
+            {
+                const T flux_kp = k == ke ? T(0.0) : w_k;
+                const T flux_km = k == 0 ? T(0.0) : w_km;
+                const T advection = -(flux_kp - flux_km) / dz[k];
+                a.rho_p[c] = v.v[0] + dt_s * advection;
+            }
+            T flux_kp, flux_km;
+            if (k == ke) {
+                flux_kp = T(0.0);
+            } else {
+                const T wp = w_k;
+                if (wp > EPS && k > 0)
+                    flux_kp = up3(wp, th_m1, th_0, th_p1);
+                else if (v.v[3] < -EPS && k < ke - 1)  // selector on s.rho_w, as written (1426)
+                    flux_kp = up3(wp, th_p2, th_p1, th_0);
+                else
+                    flux_kp = wp * f2h(th_0, th_p1, dz[k], dz[k + 1]);
+            }
+            if (k == 0) {
+                flux_km = T(0.0);
+            } else {
+                const T wp = w_km;
+                const T sw = v.v[4];
+                if (sw > EPS && k > 1)
+                    flux_km = up3(wp, th_m2, th_m1, th_0);
+                else if (sw < -EPS && k < ke)
+                    flux_km = up3(wp, th_p1, th_0, th_m1);
+                else
+                    flux_km = wp * f2h(th_m1, th_0, dz[k - 1], dz[k]);
+            }
             const T advection = -(flux_kp - flux_km) / dz[k];
-            a.rho_p[c] = a.rho_p[c] + dt_s * advection;
-        }
-        T flux_kp, flux_km;
-        if (k == ke) {
-            flux_kp = T(0.0);
-        } else {
-            const T wp = w_k;
-            if (wp > EPS && k > 0)
-                flux_kp = up3(wp, ro(th + c - P), ro(th + c), ro(th + c + P));
-            else if (ro(a.s_rw + c) < -EPS && k < ke - 1)  // selector on s.rho_w, as written (1426)
-                flux_kp = up3(wp, ro(th + c + 2 * P), ro(th + c + P), ro(th + c));
-            else
-                flux_kp = wp * f2h(ro(th + c), ro(th + c + P), dz[k], dz[k + 1]);
-        }
-        if (k == 0) {
-            flux_km = T(0.0);
-        } else {
-            const T wp = w_km;
-            const T sw = ro(a.s_rw + c - P);
-            if (sw > EPS && k > 1)
-                flux_km = up3(wp, ro(th + c - 2 * P), ro(th + c - P), ro(th + c));
-            else if (sw < -EPS && k < ke)
-                flux_km = up3(wp, ro(th + c + P), ro(th + c), ro(th + c - P));
-            else
-                flux_km = wp * f2h(ro(th + c - P), ro(th + c), dz[k - 1], dz[k]);
-        }
-        const T advection = -(flux_kp - flux_km) / dz[k];
-        a.rt_out[c] = a.rt_out[c] + dt_s * advection;
-        if (k < ke) a.mfz[c] = a.mfz[c] + w_k / ns_T;
-    }
+            a.rt_out[c] = v.v[1] + dt_s * advection;
+            if (k < ke) a.mfz[c] = v.v[2] + w_k / ns_T;
+        });
 }
 template <class T, class TT>
 __global__ void __launch_bounds__(STRIP_THREADS) k_substep_strip(DevParams<T> p, SubArgs<T, TT> a, T dt_s, T ns_T,                                                                   double fact_tp64, int wc, const int* err) {
