@@ -1284,37 +1284,49 @@ __device__ __forceinline__ void b_thomas_strip(DevParams<T> p, const T* theta, c
     const int i = i0 + col;
     const T fact_tp = T(0.5) * (T(1.0) + p.beta);
     const T dt_tp2 = (dt_s * fact_tp) * (dt_s * fact_tp);
-    #pragma unroll 4
-    for (int j = r0; j < n && own; j += rs)
-        th_h[j * wc + col] = f2h(theta[MOIST_IDX(j, i)], theta[MOIST_IDX(j + 1, i)], dz[j], dz[j + 1]);
+    batched_loop<Vals<T, 2>>(
+        r0, own ? n : 0, rs, [&](int j) { return Vals<T, 2>{{theta[MOIST_IDX(j, i)], theta[MOIST_IDX(j + 1, i)]}}; },
+        [&](int j, const Vals<T, 2>& v) { th_h[j * wc + col] = f2h(v.v[0], v.v[1], dz[j], dz[j + 1]); });
     __syncthreads();
-    #pragma unroll 4
-    for (int j = r0; j < n && own; j += rs) {
-        const int k = j;
-        const T th_cur = th_h[j * wc + col];
-        const T th_prev = k > 0 ? th_h[(j - 1) * wc + col] : T(0);
-        const T th_next = (k + 1 <= ke - 1) ? th_h[(j + 1) * wc + col] : T(0);
-        const T r_k = rt2pres[MOIST_IDX(k, i)], r_kp = rt2pres[MOIST_IDX(k + 1, i)];
-        const T b = dt_tp2 * (r_k / dz[k] + r_kp / dz[k + 1]) * th_cur / (z[k + 1] - z[k]);
-        const T a = (k > 0) ? -dt_tp2 * (r_k * th_prev / ((z[k + 1] - z[k]) * dz[k]) - p.GRAV / (dz[k] + dz[k + 1])) : T(0);
-        const T c = (k < ke - 1) ? -dt_tp2 * (r_kp * th_next / ((z[k + 1] - z[k]) * dz[k + 1]) + p.GRAV / (dz[k] + dz[k + 1])) : T(0);
-        ta[MOIST_IDX(j, i)] = a;
-        tb[MOIST_IDX(j, i)] = b;
-        tc[MOIST_IDX(j, i)] = c;
-        sm.D[j * wc + col] = (TT)(b + T(1.0));
-        sm.a[j * wc + col] = a;
-        sm.cp[j * wc + col] = (TT)c;
-    }
+    batched_loop<Vals<T, 2>>(
+        r0, own ? n : 0, rs, [&](int j) { return Vals<T, 2>{{rt2pres[MOIST_IDX(j, i)], rt2pres[MOIST_IDX(j + 1, i)]}}; },
+        [&](int j, const Vals<T, 2>& v) {
+            const int k = j;
+            const T th_cur = th_h[j * wc + col];
+            const T th_prev = k > 0 ? th_h[(j - 1) * wc + col] : T(0);
+            const T th_next = (k + 1 <= ke - 1) ? th_h[(j + 1) * wc + col] : T(0);
+            const T r_k = v.v[0], r_kp = v.v[1];
+            const T b = dt_tp2 * (r_k / dz[k] + r_kp / dz[k + 1]) * th_cur / (z[k + 1] - z[k]);
+            const T a = (k > 0) ? -dt_tp2 * (r_k * th_prev / ((z[k + 1] - z[k]) * dz[k]) - p.GRAV / (dz[k] + dz[k + 1])) : T(0);
+            const T c = (k < ke - 1) ? -dt_tp2 * (r_kp * th_next / ((z[k + 1] - z[k]) * dz[k + 1]) + p.GRAV / (dz[k] + dz[k + 1])) : T(0);
+            ta[MOIST_IDX(j, i)] = a;
+            tb[MOIST_IDX(j, i)] = b;
+            tc[MOIST_IDX(j, i)] = c;
+            sm.D[j * wc + col] = (TT)(b + T(1.0));
+            sm.a[j * wc + col] = a;
+            sm.cp[j * wc + col] = (TT)c;
+        });
     __syncthreads();
     if (threadIdx.x < ncol) {
+        // the pivot recurrence, the next level's operands read one level ahead (index clamped)
         const int cc = threadIdx.x;
+        const TT* __restrict__ sD = sm.D;
+        const T* __restrict__ sa = sm.a;
+        TT* __restrict__ sc = sm.cp;
+        TT* __restrict__ sp = sm.piv;
         TT cp_prev = TT(0);
+        TT bn = sD[cc], an = (TT)sa[cc], cn = sc[cc];
+#pragma unroll 4
         for (int j = 0; j < n; j++) {
-            const TT bb = sm.D[j * wc + cc];
-            const TT piv = j == 0 ? bb : bb - (TT)sm.a[j * wc + cc] * cp_prev;
-            const TT cpj = sm.cp[j * wc + cc] / piv;
-            sm.piv[j * wc + cc] = piv;
-            sm.cp[j * wc + cc] = cpj;
+            const TT bb = bn, aj = an, cj = cn;
+            const int jn = j + 1 < n ? j + 1 : n - 1;
+            bn = sD[jn * wc + cc];
+            an = (TT)sa[jn * wc + cc];
+            cn = sc[jn * wc + cc];
+            const TT piv = j == 0 ? bb : bb - aj * cp_prev;
+            const TT cpj = cj / piv;
+            sp[j * wc + cc] = piv;
+            sc[j * wc + cc] = cpj;
             cp_prev = cpj;
         }
     }
