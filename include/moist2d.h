@@ -236,11 +236,10 @@ int moist_implicit_correction(const moist_params* p, int precision, int flags, v
  * MOIST_NOALLOC_SCRATCH_BYTES (e.g. 2048 columns of 128 levels with the FP64 elimination);
  * larger calls return MOIST_ERR_ARG before queuing anything and write the reason to err (if not
  * NULL). The first call on a device looks up the scratch array's device address with that
- * device current and keeps it for the life of the process: make that first call before any
- * stream capture, and make no call after a cudaDeviceReset of the device. All calls share the
- * array and keep the last call's contents; nothing in it needs to start at zero (every element
- * is written before it is read). Calls that overlap on the same GPU (for example on two
- * streams) race on it, so serialise them. */
+ * device current and keeps it for the life of the process, so make no call after a
+ * cudaDeviceReset of the device. All calls share the array and keep the last call's contents;
+ * nothing in it needs to start at zero (every element is written before it is read). Calls that
+ * overlap on the same GPU (for example on two streams) race on it, so serialise them. */
 #define MOIST_NOALLOC_MAX_NZ 1024
 #define MOIST_NOALLOC_SCRATCH_BYTES (4 * 1024 * 1024)
 int moist_implicit_correction_noalloc(const moist_params* p, int precision, int flags, int ncols,
