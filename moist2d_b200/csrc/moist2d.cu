@@ -278,9 +278,13 @@ struct Ctx : CtxBase {
     std::vector<int> ev_group;
     long long launches[MOIST_NGROUPS] = {0};
 
-    int mark(int group, int nkernels) {
+    // An event opens the interval of each group that follows a different one: consecutive
+    // launches of one group (the substeps of a stage) share one interval, because every timing
+    // event between kernels costs the stream several microseconds.
+    int mark(int group, int nkernels, bool close = false) {
         launches[group] += nkernels;
         if (!prof_on) return MOIST_OK;
+        if (!close && !ev_group.empty() && ev_group.back() == group) return MOIST_OK;
         const size_t j = ev_group.size();
         if (j >= ev_pool.size()) {
             cudaEvent_t e;
@@ -968,7 +972,7 @@ struct Ctx : CtxBase {
         prof_on = true;
         int r = MOIST_OK;
         for (int n = 0; n < nsteps && r == MOIST_OK; n++) r = launch_step();
-        if (r == MOIST_OK) r = mark(MOIST_KGROUP_OTHER, 0);
+        if (r == MOIST_OK) r = mark(MOIST_KGROUP_OTHER, 0, true);  // closes the last interval
         prof_on = false;
         if (r != MOIST_OK) return r;
         CK(cudaStreamSynchronize(st));
