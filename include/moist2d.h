@@ -471,10 +471,12 @@ enum {
     MOIST_KGROUP_OTHER = 5,     /* precipitation accumulation */
     MOIST_NGROUPS = 6
 };
-/* Run nsteps large steps with CUDA events recorded on the context stream before each kernel
- * group: *total_ms = device time from the first to the last event, group_ms[g] = time spent
- * in group g, group_launches[g] = kernels launched in group g (arrays of MOIST_NGROUPS; any
- * pointer may be NULL). */
+/* Run nsteps large steps with CUDA events recorded on the context stream wherever the kernel
+ * group changes (consecutive launches of one group, such as the substeps of a stage, share one
+ * interval): *total_ms = device time from the first to the last event, group_ms[g] = time
+ * spent in group g, group_launches[g] = kernels launched in group g (arrays of MOIST_NGROUPS;
+ * any pointer may be NULL). Every event between two kernels costs the stream a few
+ * microseconds, so *total_ms is somewhat above the time moist_time_steps gives. */
 int moist_step_profile(moist_ctx* ctx, int nsteps, float* total_ms, float* group_ms,
                        long long* group_launches);
 
